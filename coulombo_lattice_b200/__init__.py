@@ -1,0 +1,241 @@
+"""B200 implementation of Coulombo-Lattice's Coulomb-integral path.
+
+The product is ``libcoulombo_lattice.so`` (CUDA kernels for sm_100a behind the C ABI of
+``include/coulombo_lattice.h``) and the drop-in binaries ``bin/coulombo`` and
+``bin/potentials``.  This module is a ctypes mirror of the reference's compute seam,
+``CoulombCalculator`` (src/CoulombCalculator.hpp:28-94): ``initialize`` with a Coulomb or a
+custom kernel, ``prepare``/``calculate`` on grids, plus the integral pipeline
+(``set_states``/``compute``) and the host helpers.  Failures raise ``CoulomboError`` with
+the library's message, the way the reference throws ``std::runtime_error``.
+
+There is no fallback: if the shared library is missing, importing the calculator raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcoulombo_lattice.so")
+BIN_DIR = os.path.join(_HERE, "bin")
+
+MODE_FP64_PLAIN = 0
+MODE_FP32_FOURIER = 1
+
+_ERR_NAMES = {1: "argument", 2: "state", 3: "cuda", 4: "memory", 5: "unsupported", 6: "timeout"}
+
+_lib = None
+
+
+class CoulomboError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+        self.kind = _ERR_NAMES.get(code, "unknown")
+
+
+# (name, restype, argtypes) of every entry point declared in include/coulombo_lattice.h
+_P = ctypes.POINTER
+_d = ctypes.c_double
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_vp = ctypes.c_void_p
+SIGNATURES = [
+    ("cl_create", _i, [_P(_vp), _i, _i, _i, _d, _d, _d, _i]),
+    ("cl_destroy", None, [_vp]),
+    ("cl_last_error", ctypes.c_char_p, []),
+    ("cl_set_kernel_coulomb", _i, [_vp, _d, _d, _d]),
+    ("cl_set_kernel_grid", _i, [_vp, _P(_d)]),
+    ("cl_prepare_grid", _i, [_vp, _P(_d)]),
+    ("cl_calculate_grid", _i, [_vp, _P(_d), _P(_d)]),
+    ("cl_potential_grid", _i, [_vp, _P(_d)]),
+    ("cl_set_states", _i, [_vp, _i, _i, _i64, _i, _P(_d), _P(_i64)]),
+    ("cl_compute", _i, [_vp, _i64, _P(ctypes.c_int16), _P(_d)]),
+    ("cl_potentials", _i, [_vp, _P(_d)]),
+    ("cl_last_timings", _i, [_vp, _P(_d)]),
+    ("cl_fft3d", _i, [_i, _i, _i, _i, _i, _i, _P(_d)]),
+    ("cl_round_up_235", _i, [_i, _i]),
+    ("cl_detect_grid", _i, [_P(_d), _i64, _P(_i), _P(_i), _P(_d), _P(_d), _P(_i64)]),
+    ("cl_enumerate_integrals", _i, [ctypes.c_char_p, _i, _i, _P(_i64), _P(ctypes.c_int16), _i64]),
+    ("cl_vertex_cover", _i, [_i, _i64, _P(ctypes.c_int32), _P(ctypes.c_uint8)]),
+    ("cl_plan", _i, [_i, _i64, _P(ctypes.c_int16), _P(ctypes.c_int32)]),
+]
+
+
+def lib():
+    """Load libcoulombo_lattice.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libcoulombo_lattice.so is not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise CoulomboError(status, lib().cl_last_error().decode())
+
+
+def _ptr(a, ctype=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _cplx(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+# ----------------------------------------------------------------------------------------
+# Host helpers
+# ----------------------------------------------------------------------------------------
+
+def round_up_235(n, c=1):
+    r = lib().cl_round_up_235(int(n), int(c))
+    if r < 0:
+        _check(1)
+    return r
+
+
+def detect_grid(positions):
+    pos = np.ascontiguousarray(positions, dtype=np.float64)
+    n = pos.shape[0]
+    raw = (ctypes.c_int * 3)()
+    pad = (ctypes.c_int * 3)()
+    origin = (ctypes.c_double * 3)()
+    step = (ctypes.c_double * 3)()
+    cells = np.empty(n, dtype=np.int64)
+    _check(lib().cl_detect_grid(_ptr(pos), n, raw, pad, origin, step, _ptr(cells, ctypes.c_int64)))
+    return dict(raw=tuple(raw), pad=tuple(pad), origin=tuple(origin), step=tuple(step), cells=cells)
+
+
+def enumerate_integrals(pattern, n_inputs, n_holes):
+    count = ctypes.c_int64()
+    _check(lib().cl_enumerate_integrals(pattern.encode(), n_inputs, n_holes, ctypes.byref(count), None, 0))
+    specs = np.empty((count.value, 4), dtype=np.int16)
+    _check(lib().cl_enumerate_integrals(pattern.encode(), n_inputs, n_holes, ctypes.byref(count),
+                                        _ptr(specs, ctypes.c_int16), count.value))
+    return specs
+
+
+def vertex_cover(n_vertices, edges):
+    e = np.ascontiguousarray(np.asarray(edges, dtype=np.int32).reshape(-1, 2))
+    out = np.zeros(n_vertices, dtype=np.uint8)
+    _check(lib().cl_vertex_cover(n_vertices, e.shape[0], _ptr(e, ctypes.c_int32), _ptr(out, ctypes.c_uint8)))
+    return {int(v) for v in np.nonzero(out)[0]}
+
+
+def plan(n_inputs, specs):
+    s = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
+    steps = np.empty((s.shape[0], 5), dtype=np.int32)
+    _check(lib().cl_plan(n_inputs, s.shape[0], _ptr(s, ctypes.c_int16), _ptr(steps, ctypes.c_int32)))
+    return steps
+
+
+def fft3d(data, sign=-1, fp32=False):
+    """Unnormalised batched 3D FFT on the GPU; data [..., nz, ny, nx] complex."""
+    a = _cplx(data).copy()
+    nz, ny, nx = a.shape[-3:]
+    batch = int(np.prod(a.shape[:-3])) if a.ndim > 3 else 1
+    _check(lib().cl_fft3d(nx, ny, nz, batch, int(sign), int(bool(fp32)), _ptr(a.view(np.float64))))
+    return a
+
+
+# ----------------------------------------------------------------------------------------
+# Calculator
+# ----------------------------------------------------------------------------------------
+
+class CoulombCalculator:
+    """Mirror of the reference's CoulombCalculator on one GPU.
+
+    dims = (nx, ny, nz); step in Angstrom; grids are numpy arrays indexed [z, y, x]."""
+
+    def __init__(self, dims, step=(1.0, 1.0, 1.0), mode=MODE_FP64_PLAIN):
+        self.dims = tuple(int(d) for d in dims)
+        self.mode = mode
+        h = ctypes.c_void_p()
+        _check(lib().cl_create(ctypes.byref(h), *self.dims, *[float(s) for s in step], mode))
+        self._h = h
+        self.n_atoms = None
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().cl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def shape(self):
+        nx, ny, nz = self.dims
+        return (nz, ny, nx)
+
+    def initialize(self, dielectric=1.0, onsite=0.0, tf_lattice=0.0):
+        _check(lib().cl_set_kernel_coulomb(self._h, float(dielectric), float(onsite), float(tf_lattice or 0.0)))
+
+    def initialize_grid(self, G):
+        g = np.ascontiguousarray(G, dtype=np.float64)
+        nx, ny, nz = self.dims
+        if g.shape != (nz + 1, ny + 1, nx + 1):
+            raise ValueError("kernel grid must be (nz+1, ny+1, nx+1)")
+        _check(lib().cl_set_kernel_grid(self._h, _ptr(g)))
+
+    def prepare(self, rho):
+        r = _cplx(rho)
+        if r.shape != self.shape:
+            raise ValueError("density must be indexed [z, y, x]")
+        _check(lib().cl_prepare_grid(self._h, _ptr(r.view(np.float64))))
+
+    def calculate(self, rho2):
+        r = _cplx(rho2)
+        if r.shape != self.shape:
+            raise ValueError("density must be indexed [z, y, x]")
+        out = np.zeros(2)
+        _check(lib().cl_calculate_grid(self._h, _ptr(r.view(np.float64)), _ptr(out)))
+        return complex(out[0], out[1])
+
+    def potential(self):
+        v = np.empty(self.shape, dtype=np.complex128)
+        _check(lib().cl_potential_grid(self._h, _ptr(v.view(np.float64))))
+        return v
+
+    def set_states(self, states, cells, n_holes):
+        """states: [n_states, n_atoms, n_orb] complex (input order, holes first)."""
+        c = _cplx(states)
+        cl = np.ascontiguousarray(cells, dtype=np.int64)
+        n, a, o = c.shape
+        _check(lib().cl_set_states(self._h, n, int(n_holes), a, o, _ptr(c.view(np.float64)),
+                                   _ptr(cl, ctypes.c_int64)))
+        self.n_states, self.n_atoms = n, a
+
+    def compute(self, specs):
+        s = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
+        out = np.zeros(2 * s.shape[0])
+        _check(lib().cl_compute(self._h, s.shape[0], _ptr(s, ctypes.c_int16), _ptr(out)))
+        return out[0::2] + 1j * out[1::2]
+
+    def potentials(self):
+        out = np.zeros((self.n_states, self.n_atoms))
+        _check(lib().cl_potentials(self._h, _ptr(out)))
+        return out
+
+    def timings(self):
+        t = np.zeros(4)
+        _check(lib().cl_last_timings(self._h, _ptr(t)))
+        return dict(densities_ms=t[0], transforms_ms=t[1], reductions_ms=t[2], total_ms=t[3])

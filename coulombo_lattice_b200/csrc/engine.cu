@@ -1,0 +1,803 @@
+// Context, orchestration and the GPU half of the C ABI (include/coulombo_lattice.h).
+#include <algorithm>
+#include <array>
+#include <memory>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "coulombo_lattice.h"
+#include "host/host_logic.hpp"
+#include "host/status.hpp"
+#include "kernels.cuh"
+
+using clk::cx;
+using clk::FftPlan;
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// CUDA helpers
+// ---------------------------------------------------------------------------------------
+#define CL_CUDA(call)                                                                           \
+    do {                                                                                        \
+        cudaError_t err_ = (call);                                                              \
+        if (err_ != cudaSuccess)                                                                \
+            cl::fail(err_ == cudaErrorMemoryAllocation ? CL_ERR_MEMORY : CL_ERR_CUDA,           \
+                     "CUDA error %s at %s:%d: %s", cudaGetErrorName(err_), __FILE__, __LINE__,  \
+                     cudaGetErrorString(err_));                                                 \
+    } while (0)
+
+#define CL_LAUNCHED() CL_CUDA(cudaGetLastError())
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count == n && p) return;
+        release();
+        if (count == 0) return;
+        CL_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const T* host, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) CL_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+};
+
+int device_count() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+void require_gpu() {
+    if (device_count() == 0) cl::fail(CL_ERR_CUDA, "no CUDA device is available");
+}
+
+int grid_for(long long n, int threads = 256) {
+    long long b = (n + threads - 1) / threads;
+    return (int)std::max(1LL, std::min(b, 148LL * 32));
+}
+
+// ---------------------------------------------------------------------------------------
+// FFT plans and host-built tables
+// ---------------------------------------------------------------------------------------
+bool smooth235(int n) {
+    if (n < 1) return false;
+    for (int p : {2, 3, 5})
+        while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+FftPlan make_plan(int n) {
+    FftPlan p{};
+    p.n = n;
+    int m = n;
+    auto push = [&](int r) {
+        if (p.nst >= 16) cl::fail(CL_ERR_UNSUPPORTED, "FFT length %d needs too many stages", n);
+        p.radix[p.nst++] = r;
+        m /= r;
+    };
+    while (m % 8 == 0) push(8);
+    while (m % 4 == 0) push(4);
+    while (m % 2 == 0) push(2);
+    while (m % 3 == 0) push(3);
+    while (m % 5 == 0) push(5);
+    if (m != 1) cl::fail(CL_ERR_UNSUPPORTED, "FFT length %d is not a product of 2, 3 and 5", n);
+    return p;
+}
+
+// tw[t] = exp(-2 pi i t / n), built in extended precision and rounded once.
+std::vector<cx<double>> twiddles64(int n) {
+    std::vector<cx<double>> t(n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < n; ++i) {
+        long double ang = -2.0L * pi * (long double)i / (long double)n;
+        t[i].re = (double)std::cos(ang);
+        t[i].im = (double)std::sin(ang);
+    }
+    return t;
+}
+
+// phase(i) = exp(i pi i / n) (CoulombCalculator.cpp:45-54).
+std::vector<cx<double>> phases64(int n) {
+    std::vector<cx<double>> t(n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < n; ++i) {
+        long double ang = pi * (long double)i / (long double)n;
+        t[i].re = (double)std::cos(ang);
+        t[i].im = (double)std::sin(ang);
+    }
+    return t;
+}
+
+// Thomas-Fermi-Resta radius (Interaction.cpp:18-32, same Newton iteration and stop rule).
+void thomas_fermi(double dielectric, double lattice, double* r_tf, double* q_tf) {
+    const double eps = 1.0e-12;
+    const double q = 2.0 / std::sqrt(M_PI) * std::cbrt(96.0 * M_PI * M_PI) / lattice;
+    double x = std::sqrt(6.0 * (dielectric - 1.0)), dx;
+    int guard = 0;
+    do {
+        double F = std::sinh(x) - dielectric * x;
+        double dF = std::cosh(x) - dielectric;
+        dx = (std::fabs(F) < eps) ? 0 : F / dF;
+        x -= dx;
+        if (++guard > 10000) cl::fail(CL_ERR_ARGUMENT, "Thomas-Fermi radius did not converge");
+    } while (dx / q > eps);
+    *q_tf = q;
+    *r_tf = x / q;
+}
+
+struct Axis {
+    FftPlan plan;
+    DevBuf<cx<double>> tw64;
+    DevBuf<cx<float>> tw32;
+    DevBuf<cx<double>> phase;
+};
+
+// Per-launch geometry of the x passes and the y/z passes.
+struct XTile {
+    int rows, ld;
+    size_t smem;
+};
+struct LTile {
+    int W;
+    size_t smem;
+};
+
+template <typename T>
+XTile x_tile(int nx, int nrows) {
+    const int elems = sizeof(T) == 4 ? 4096 : 2048;
+    int rows = std::max(1, std::min(elems / std::max(nx, 1), 64));
+    rows = std::min(rows, nrows);
+    int ld = (rows % 2 == 0) ? rows + 1 : rows;
+    XTile t{rows, ld, sizeof(cx<T>) * ((size_t)nx + 2ull * nx * ld)};
+    return t;
+}
+
+template <typename T>
+LTile l_tile(int n, bool with_khat) {
+    int W = sizeof(T) == 4 ? 16 : 8;
+    auto bytes = [&](int w) {
+        return sizeof(cx<T>) * ((size_t)n + 2ull * n * w) + (with_khat ? sizeof(T) * (size_t)n * w : 0);
+    };
+    while (W > 1 && bytes(W) > 200 * 1024) W /= 2;
+    return LTile{W, bytes(W)};
+}
+
+template <typename K>
+void ensure_smem(K kernel, size_t bytes) {
+    if (bytes > 227 * 1024) cl::fail(CL_ERR_UNSUPPORTED, "tile needs %zu bytes of shared memory", bytes);
+    CL_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// The context
+// ---------------------------------------------------------------------------------------
+struct cl_ctx {
+    int device = 0;
+    int mode = CL_MODE_FP64_PLAIN;
+    int n[3] = {0, 0, 0};
+    long long M = 0;
+    double step[3] = {1, 1, 1};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[5] = {};
+    Axis ax[3];
+
+    bool kernel_ready = false;
+    DevBuf<double> ghat;
+    DevBuf<double> khat64[8];
+    DevBuf<float> khat32[8];
+
+    // grid API ("every cell is an atom")
+    DevBuf<int> grid_cell, grid_row_ptr;
+    DevBuf<cx<double>> grid_rho, grid_V, grid_rho2;
+    bool grid_prepared = false;
+
+    // states
+    int n_states = 0, n_holes = 0, n_orb = 0;
+    long long n_atoms = 0, n_sorted = 0;
+    DevBuf<cx<double>> coeff;
+    DevBuf<int> cell_sorted, orig_sorted, row_ptr;
+    std::vector<long long> atom_slot;  // input atom -> sorted (deduplicated) slot
+
+    // work buffers
+    DevBuf<unsigned char> work;
+    double timings[4] = {0, 0, 0, 0};
+
+    ~cl_ctx() {
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            for (auto& e : ev)
+                if (e) cudaEventDestroy(e);
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
+namespace {
+
+size_t free_device_bytes() {
+    size_t fr = 0, tot = 0;
+    CL_CUDA(cudaMemGetInfo(&fr, &tot));
+    return fr;
+}
+
+void build_khat(cl_ctx* c) {
+    const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+    const double denom = (double)((unsigned long long)c->M * 8ull);
+    for (int r = 0; r < 8; ++r) {
+        const int kx = r & 1, ky = (r >> 1) & 1, kz = (r >> 2) & 1;
+        if (c->mode == CL_MODE_FP64_PLAIN) {
+            c->khat64[r].alloc(c->M);
+            clk::k_khat<double><<<grid_for(c->M), 256, 0, c->stream>>>(c->ghat.p, nx, ny, nz, kx, ky, kz, denom,
+                                                                       c->khat64[r].p);
+        } else {
+            c->khat32[r].alloc(c->M);
+            clk::k_khat<float><<<grid_for(c->M), 256, 0, c->stream>>>(c->ghat.p, nx, ny, nz, kx, ky, kz, denom,
+                                                                      c->khat32[r].p);
+        }
+        CL_LAUNCHED();
+    }
+}
+
+// 3D DCT-I of the octant held in c->ghat (three separable passes), then Khat per round.
+void transform_kernel(cl_ctx* c) {
+    const int n1[3] = {c->n[0] + 1, c->n[1] + 1, c->n[2] + 1};
+    const long long total = (long long)n1[0] * n1[1] * n1[2];
+    DevBuf<double> tmp;
+    tmp.alloc(total);
+    double* src = c->ghat.p;
+    double* dst = tmp.p;
+    long long inner = 1;
+    for (int d = 0; d < 3; ++d) {
+        const int L = n1[d];
+        const int np = L - 1;
+        std::vector<double> ct(2 * (size_t)np);
+        const long double pi = 3.141592653589793238462643383279502884L;
+        for (int t = 0; t < 2 * np; ++t) ct[t] = (double)std::cos(pi * (long double)t / (long double)np);
+        DevBuf<double> dct;
+        dct.upload(ct.data(), ct.size(), c->stream);
+        const long long nlines = total / L;
+        int nl = 16;
+        while (nl > 1 && (size_t)(L * nl + 2 * np) * sizeof(double) > 160 * 1024) nl /= 2;
+        const size_t smem = (size_t)(L * nl + 2 * np) * sizeof(double);
+        ensure_smem(clk::k_dct1, smem);
+        const long long blocks = (nlines + nl - 1) / nl;
+        clk::k_dct1<<<(unsigned)blocks, 256, smem, c->stream>>>(src, dst, L, inner, nlines, nl, dct.p);
+        CL_LAUNCHED();
+        CL_CUDA(cudaStreamSynchronize(c->stream));  // dct table lifetime
+        std::swap(src, dst);
+        inner *= L;
+    }
+    if (src != c->ghat.p)
+        CL_CUDA(cudaMemcpyAsync(c->ghat.p, src, total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    build_khat(c);
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    c->kernel_ready = true;
+}
+
+// One request's transforms: for every density p in [0, np) (rho rows), V[p] += the 8-round
+// convolution at the atoms of the row CSR.  buf holds `chunk` grids of type T.
+template <typename T>
+void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, const int* row_ptr,
+                const int* cell, cx<double>* V, long long v_stride) {
+    const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+    const int nrows = ny * nz;
+    const long long nxy = (long long)nx * ny;
+    const size_t grid_bytes = sizeof(cx<T>) * (size_t)c->M;
+    // densities per chunk: keep the work buffer within 60% of the free memory
+    size_t budget = (size_t)(0.6 * (double)(free_device_bytes() + c->work.n));
+    int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)np, budget / grid_bytes));
+    c->work.alloc(std::max(c->work.n, (size_t)chunk * grid_bytes));
+    cx<T>* buf = reinterpret_cast<cx<T>*>(c->work.p);
+
+    const Axis& X = c->ax[0];
+    const Axis& Y = c->ax[1];
+    const Axis& Z = c->ax[2];
+    const cx<T>* twx = sizeof(T) == 4 ? (const cx<T>*)X.tw32.p : (const cx<T>*)X.tw64.p;
+    const cx<T>* twy = sizeof(T) == 4 ? (const cx<T>*)Y.tw32.p : (const cx<T>*)Y.tw64.p;
+    const cx<T>* twz = sizeof(T) == 4 ? (const cx<T>*)Z.tw32.p : (const cx<T>*)Z.tw64.p;
+
+    const XTile xt = x_tile<T>(nx, nrows);
+    const LTile yt = l_tile<T>(ny, false);
+    const LTile zt = l_tile<T>(nz, true);
+    ensure_smem(clk::k_xfwd<T>, xt.smem);
+    ensure_smem(clk::k_xinv<T>, xt.smem);
+    ensure_smem(clk::k_ypass<-1, T>, yt.smem);
+    ensure_smem(clk::k_ypass<+1, T>, yt.smem);
+    ensure_smem(clk::k_zpass<T>, zt.smem);
+    const int xblocks = (nrows + xt.rows - 1) / xt.rows;
+    const int ychunks = (nx + yt.W - 1) / yt.W;
+    const long long zblocks = (nxy + zt.W - 1) / zt.W;
+
+    for (int p0 = 0; p0 < np; p0 += chunk) {
+        const int cnt = std::min(chunk, np - p0);
+        const cx<double>* rho_c = rho + (long long)p0 * rho_stride;
+        cx<double>* V_c = V + (long long)p0 * v_stride;
+        for (int r = 0; r < 8; ++r) {
+            clk::RoundPhase rp{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, r & 1, (r >> 1) & 1,
+                               (r >> 2) & 1};
+            const T* kh = sizeof(T) == 4 ? (const T*)c->khat32[r].p : (const T*)c->khat64[r].p;
+            clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan,
+                                                                 twx, rp, nx, ny, nrows, xt.rows, xt.ld, cnt);
+            CL_LAUNCHED();
+            clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx, ny,
+                                                                                      yt.W, ychunks);
+            CL_LAUNCHED();
+            clk::k_zpass<T><<<(unsigned)zblocks, 256, zt.smem, c->stream>>>(buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W,
+                                                                             cnt, 0);
+            CL_LAUNCHED();
+            clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx, ny,
+                                                                                      yt.W, ychunks);
+            CL_LAUNCHED();
+            clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, rp, row_ptr, cell, V_c,
+                                                                 v_stride, nx, ny, nrows, xt.rows, xt.ld, cnt);
+            CL_LAUNCHED();
+        }
+    }
+}
+
+void run_rounds_mode(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, const int* row_ptr,
+                     const int* cell, cx<double>* V, long long v_stride) {
+    if (c->mode == CL_MODE_FP64_PLAIN)
+        run_rounds<double>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride);
+    else
+        run_rounds<float>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride);
+}
+
+// out4[l][r] = {sum ac, bd, ad, bc} over atoms (see k_gram).
+void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<double>* rho, long long r_stride,
+          const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
+    CL_CUDA(cudaMemsetAsync(out4_dev, 0, sizeof(double) * 4 * (size_t)nl * nr, c->stream));
+    const int tl = (nl + 63) / 64, tr = (nr + 63) / 64;
+    long long want = std::max(1LL, (148LL * 2) / std::max(1, tl * tr));
+    long long per = std::max(256LL, (n_atoms + want - 1) / want);
+    per = (per + 15) / 16 * 16;
+    long long splits = std::max(1LL, (n_atoms + per - 1) / per);
+    if (splits > 65535) {
+        splits = 65535;
+        per = ((n_atoms + splits - 1) / splits + 15) / 16 * 16;
+    }
+    clk::k_gram<<<dim3(tl, tr, (unsigned)splits), 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr,
+                                                                        n_atoms, per, out4_dev);
+    CL_LAUNCHED();
+}
+
+void check_ctx(cl_ctx* c) {
+    if (!c) cl::fail(CL_ERR_ARGUMENT, "null context");
+    CL_CUDA(cudaSetDevice(c->device));
+}
+
+void check_kernel(cl_ctx* c) {
+    if (!c->kernel_ready) cl::fail(CL_ERR_STATE, "the Coulomb kernel is not initialised (call cl_set_kernel_*)");
+}
+
+void identity_atoms(cl_ctx* c) {
+    if (c->grid_cell.p) return;
+    const int nrows = c->n[1] * c->n[2];
+    std::vector<int> cell((size_t)c->M), rp((size_t)nrows + 1);
+    std::iota(cell.begin(), cell.end(), 0);
+    for (int r = 0; r <= nrows; ++r) rp[r] = r * c->n[0];
+    c->grid_cell.upload(cell.data(), cell.size(), c->stream);
+    c->grid_row_ptr.upload(rp.data(), rp.size(), c->stream);
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+}  // namespace
+
+// =======================================================================================
+// C ABI
+// =======================================================================================
+extern "C" {
+
+int cl_create(cl_ctx** out, int nx, int ny, int nz, double sx, double sy, double sz, int mode) {
+    if (out) *out = nullptr;
+    cl_ctx* c = nullptr;
+    int st = cl::guarded([&] {
+        if (!out) cl::fail(CL_ERR_ARGUMENT, "null output pointer");
+        if (nx <= 0 || ny <= 0 || nz <= 0) cl::fail(CL_ERR_ARGUMENT, "dimensions must be positive");
+        if (mode != CL_MODE_FP64_PLAIN && mode != CL_MODE_FP32_FOURIER) cl::fail(CL_ERR_ARGUMENT, "unknown mode %d", mode);
+        const int dims[3] = {nx, ny, nz};
+        for (int d = 0; d < 3; ++d) {
+            if (!smooth235(dims[d]))
+                cl::fail(CL_ERR_UNSUPPORTED, "grid size %d is not a product of 2, 3 and 5", dims[d]);
+            if (dims[d] > 4096) cl::fail(CL_ERR_UNSUPPORTED, "grid size %d exceeds 4096", dims[d]);
+        }
+        const long long M = (long long)nx * ny * nz;
+        if (M >= (1LL << 31)) cl::fail(CL_ERR_UNSUPPORTED, "grid of %lld cells exceeds 2^31", M);
+        if (!(sx > 0 && sy > 0 && sz > 0)) cl::fail(CL_ERR_ARGUMENT, "step lengths must be positive");
+        require_gpu();
+        c = new cl_ctx();
+        CL_CUDA(cudaGetDevice(&c->device));
+        c->mode = mode;
+        c->n[0] = nx;
+        c->n[1] = ny;
+        c->n[2] = nz;
+        c->M = M;
+        c->step[0] = sx;
+        c->step[1] = sy;
+        c->step[2] = sz;
+        CL_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        for (auto& e : c->ev) CL_CUDA(cudaEventCreate(&e));
+        for (int d = 0; d < 3; ++d) {
+            Axis& A = c->ax[d];
+            A.plan = make_plan(dims[d]);
+            auto t64 = twiddles64(dims[d]);
+            std::vector<cx<float>> t32(t64.size());
+            for (size_t i = 0; i < t64.size(); ++i) {
+                t32[i].re = (float)t64[i].re;
+                t32[i].im = (float)t64[i].im;
+            }
+            A.tw64.upload(t64.data(), t64.size(), c->stream);
+            A.tw32.upload(t32.data(), t32.size(), c->stream);
+            auto ph = phases64(dims[d]);
+            A.phase.upload(ph.data(), ph.size(), c->stream);
+        }
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        *out = c;
+    });
+    if (st != CL_OK) delete c;
+    return st;
+}
+
+void cl_destroy(cl_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    delete ctx;
+}
+
+int cl_set_kernel_coulomb(cl_ctx* c, double dielectric, double onsite, double tf_lattice) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        clk::KernelModel km{dielectric, onsite, 0, 0.0, 0.0};
+        if (tf_lattice > 0) {
+            if (!(dielectric > 1.0)) cl::fail(CL_ERR_ARGUMENT, "dielectric constant must be >1 to use Thomas-Fermi model");
+            km.thomas_fermi = 1;
+            thomas_fermi(dielectric, tf_lattice, &km.r_tf, &km.q_tf);
+        }
+        const int n1x = c->n[0] + 1, n1y = c->n[1] + 1, n1z = c->n[2] + 1;
+        const long long total = (long long)n1x * n1y * n1z;
+        c->kernel_ready = false;
+        c->ghat.alloc(total);
+        clk::k_kernel_octant<<<grid_for(total), 256, 0, c->stream>>>(c->ghat.p, n1x, n1y, n1z, c->step[0], c->step[1],
+                                                                     c->step[2], km);
+        CL_LAUNCHED();
+        transform_kernel(c);
+    });
+}
+
+int cl_set_kernel_grid(cl_ctx* c, const double* G) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        if (!G) cl::fail(CL_ERR_ARGUMENT, "null kernel grid");
+        const long long total = (long long)(c->n[0] + 1) * (c->n[1] + 1) * (c->n[2] + 1);
+        c->kernel_ready = false;
+        c->ghat.upload(G, total, c->stream);
+        transform_kernel(c);
+    });
+}
+
+int cl_prepare_grid(cl_ctx* c, const double* rho) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        check_kernel(c);
+        if (!rho) cl::fail(CL_ERR_ARGUMENT, "null density");
+        identity_atoms(c);
+        c->grid_rho.upload(reinterpret_cast<const cx<double>*>(rho), c->M, c->stream);
+        c->grid_V.alloc(c->M);
+        CL_CUDA(cudaMemsetAsync(c->grid_V.p, 0, sizeof(cx<double>) * c->M, c->stream));
+        run_rounds_mode(c, c->grid_rho.p, c->M, 1, c->grid_row_ptr.p, c->grid_cell.p, c->grid_V.p, c->M);
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        c->grid_prepared = true;
+    });
+}
+
+int cl_calculate_grid(cl_ctx* c, const double* rho2, double out[2]) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        if (!c->grid_prepared) cl::fail(CL_ERR_STATE, "calculate() called before prepare()");
+        if (!rho2 || !out) cl::fail(CL_ERR_ARGUMENT, "null argument");
+        c->grid_rho2.upload(reinterpret_cast<const cx<double>*>(rho2), c->M, c->stream);
+        DevBuf<double> o4;
+        o4.alloc(4);
+        DevBuf<int> ridx;
+        int zero = 0;
+        ridx.upload(&zero, 1, c->stream);
+        gram(c, c->grid_V.p, c->M, 1, c->grid_rho2.p, c->M, ridx.p, 1, c->M, o4.p);
+        double h[4];
+        CL_CUDA(cudaMemcpyAsync(h, o4.p, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        out[0] = h[0] - h[1];
+        out[1] = h[2] + h[3];
+    });
+}
+
+int cl_potential_grid(cl_ctx* c, double* V) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        if (!c->grid_prepared) cl::fail(CL_ERR_STATE, "potential() called before prepare()");
+        if (!V) cl::fail(CL_ERR_ARGUMENT, "null argument");
+        CL_CUDA(cudaMemcpyAsync(V, c->grid_V.p, sizeof(cx<double>) * c->M, cudaMemcpyDeviceToHost, c->stream));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int cl_set_states(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_orb, const double* coeff,
+                  const int64_t* cells) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        if (n_states <= 0 || n_holes < 0 || n_holes > n_states || n_atoms <= 0 || n_orb <= 0 || !coeff || !cells)
+            cl::fail(CL_ERR_ARGUMENT, "invalid states description");
+        if (n_atoms >= (1LL << 31)) cl::fail(CL_ERR_UNSUPPORTED, "too many atoms");
+        // Sort atoms by cell; where several atoms share a cell the one listed last wins, as
+        // with F[cell] = value in atom order (Product.cpp:16-30).
+        std::vector<int> order((size_t)n_atoms);
+        std::iota(order.begin(), order.end(), 0);
+        for (int64_t a = 0; a < n_atoms; ++a)
+            if (cells[a] < 0 || cells[a] >= c->M) cl::fail(CL_ERR_ARGUMENT, "atom %lld lies outside the grid", (long long)a);
+        bool sorted = true;
+        for (int64_t a = 1; a < n_atoms && sorted; ++a) sorted = cells[a - 1] < cells[a];
+        if (!sorted)
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells[x] < cells[y]; });
+        std::vector<int> cell_s, orig_s;
+        cell_s.reserve((size_t)n_atoms);
+        orig_s.reserve((size_t)n_atoms);
+        c->atom_slot.assign((size_t)n_atoms, 0);
+        for (size_t i = 0; i < order.size(); ++i) {
+            const int a = order[i];
+            if (!cell_s.empty() && cell_s.back() == (int)cells[a]) {
+                orig_s.back() = a;  // later atom of the same cell replaces the earlier one
+            } else {
+                cell_s.push_back((int)cells[a]);
+                orig_s.push_back(a);
+            }
+            c->atom_slot[a] = (long long)cell_s.size() - 1;
+        }
+        const int nx = c->n[0];
+        const int nrows = c->n[1] * c->n[2];
+        std::vector<int> rp((size_t)nrows + 1, 0);
+        for (int cs : cell_s) rp[cs / nx + 1]++;
+        for (int r = 0; r < nrows; ++r) rp[r + 1] += rp[r];
+        c->n_states = n_states;
+        c->n_holes = n_holes;
+        c->n_orb = n_orb;
+        c->n_atoms = n_atoms;
+        c->n_sorted = (long long)cell_s.size();
+        c->cell_sorted.upload(cell_s.data(), cell_s.size(), c->stream);
+        c->orig_sorted.upload(orig_s.data(), orig_s.size(), c->stream);
+        c->row_ptr.upload(rp.data(), rp.size(), c->stream);
+        c->coeff.upload(reinterpret_cast<const cx<double>*>(coeff), (size_t)n_states * n_atoms * n_orb, c->stream);
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int cl_compute(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        check_kernel(c);
+        if (c->n_states == 0) cl::fail(CL_ERR_STATE, "no states loaded (call cl_set_states)");
+        if (n_int < 0 || (n_int && (!spec || !out))) cl::fail(CL_ERR_ARGUMENT, "invalid integral list");
+        std::memset(c->timings, 0, sizeof c->timings);
+        if (n_int == 0) return;
+        std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
+        for (int64_t i = 0; i < n_int; ++i)
+            for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
+        const auto plan = cl::compute_plan(c->n_states, specs);
+        // densities: prepared (left) products first, then right-only products
+        const int P = c->n_states * (c->n_states + 1) / 2;
+        std::vector<int> slot(P, -1), is_left(P, 0), is_right(P, 0);
+        for (const auto& s : plan) {
+            is_left[s.left.product] = 1;
+            is_right[s.right.product] = 1;
+        }
+        std::vector<int> prods;
+        for (int p = 0; p < P; ++p)
+            if (is_left[p]) { slot[p] = (int)prods.size(); prods.push_back(p); }
+        const int nl = (int)prods.size();
+        for (int p = 0; p < P; ++p)
+            if (is_right[p] && slot[p] < 0) { slot[p] = (int)prods.size(); prods.push_back(p); }
+        std::vector<int> rights, rcol(P, -1);
+        for (int p = 0; p < P; ++p)
+            if (is_right[p]) { rcol[p] = (int)rights.size(); rights.push_back(slot[p]); }
+        const int nu = (int)prods.size(), nr = (int)rights.size();
+        std::vector<int2> fl(nu);
+        for (int i = 0; i < nu; ++i) {
+            int a, b;
+            cl::product_states(prods[i], &a, &b);
+            fl[i] = make_int2(a - 1, b - 1);
+        }
+        const long long As = c->n_sorted;
+        DevBuf<int2> dprods;
+        dprods.upload(fl.data(), fl.size(), c->stream);
+        DevBuf<int> dr;
+        dr.upload(rights.data(), rights.size(), c->stream);
+        DevBuf<cx<double>> rho, V;
+        rho.alloc((size_t)nu * As);
+        V.alloc((size_t)nl * As);
+        DevBuf<double> o4;
+        o4.alloc((size_t)4 * nl * nr);
+        CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+        clk::k_pair_density<<<dim3(grid_for(As), nu), 256, 0, c->stream>>>(
+            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, As, dprods.p, rho.p);
+        CL_LAUNCHED();
+        CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)nl * As, c->stream));
+        CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
+        run_rounds_mode(c, rho.p, As, nl, c->row_ptr.p, c->cell_sorted.p, V.p, As);
+        CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
+        gram(c, V.p, As, nl, rho.p, As, dr.p, nr, As, o4.p);
+        CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
+        std::vector<double> h((size_t)4 * nl * nr);
+        CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        float t01, t12, t23, t03;
+        CL_CUDA(cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]));
+        CL_CUDA(cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]));
+        CL_CUDA(cudaEventElapsedTime(&t23, c->ev[2], c->ev[3]));
+        CL_CUDA(cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]));
+        c->timings[0] = t01;
+        c->timings[1] = t12;
+        c->timings[2] = t23;
+        c->timings[3] = t03;
+        // step values (coulombo.cpp:199-207)
+        for (const auto& s : plan) {
+            const int l = slot[s.left.product], r = rcol[s.right.product];
+            const double* q = &h[((size_t)l * nr + r) * 4];
+            const bool rconj = s.left.conjugate != s.right.conjugate;
+            double re, im;
+            if (rconj) {
+                re = q[0] + q[1];
+                im = q[3] - q[2];
+            } else {
+                re = q[0] - q[1];
+                im = q[2] + q[3];
+            }
+            if (s.left.conjugate) im = -im;
+            out[2 * s.id] = re;
+            out[2 * s.id + 1] = im;
+        }
+    });
+}
+
+int cl_potentials(cl_ctx* c, double* out) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        check_kernel(c);
+        if (c->n_states == 0) cl::fail(CL_ERR_STATE, "no states loaded (call cl_set_states)");
+        if (!out) cl::fail(CL_ERR_ARGUMENT, "null output");
+        const int n = c->n_states;
+        const long long As = c->n_sorted;
+        std::vector<int2> fl(n);
+        for (int s = 0; s < n; ++s) fl[s] = make_int2(s, s);
+        DevBuf<int2> dprods;
+        dprods.upload(fl.data(), fl.size(), c->stream);
+        DevBuf<cx<double>> rho, V;
+        rho.alloc((size_t)n * As);
+        V.alloc((size_t)n * As);
+        CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+        clk::k_pair_density<<<dim3(grid_for(As), n), 256, 0, c->stream>>>(c->coeff.p, c->n_atoms, c->n_orb,
+                                                                          c->orig_sorted.p, As, dprods.p, rho.p);
+        CL_LAUNCHED();
+        CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)n * As, c->stream));
+        CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
+        run_rounds_mode(c, rho.p, As, n, c->row_ptr.p, c->cell_sorted.p, V.p, As);
+        CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
+        std::vector<cx<double>> h((size_t)n * As);
+        CL_CUDA(cudaMemcpyAsync(h.data(), V.p, h.size() * sizeof(cx<double>), cudaMemcpyDeviceToHost, c->stream));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        for (int s = 0; s < n; ++s)
+            for (long long a = 0; a < c->n_atoms; ++a) out[(size_t)s * c->n_atoms + a] = h[(size_t)s * As + c->atom_slot[a]].re;
+        float t01, t12;
+        CL_CUDA(cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]));
+        CL_CUDA(cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]));
+        c->timings[0] = t01;
+        c->timings[1] = t12;
+        c->timings[2] = 0;
+        c->timings[3] = t01 + t12;
+    });
+}
+
+int cl_last_timings(cl_ctx* c, double t[4]) {
+    return cl::guarded([&] {
+        if (!c || !t) cl::fail(CL_ERR_ARGUMENT, "null argument");
+        for (int i = 0; i < 4; ++i) t[i] = c->timings[i];
+    });
+}
+
+int cl_fft3d(int nx, int ny, int nz, int batch, int sign, int fp32, double* data) {
+    return cl::guarded([&] {
+        if (nx <= 0 || ny <= 0 || nz <= 0 || batch <= 0 || !data || (sign != -1 && sign != 1))
+            cl::fail(CL_ERR_ARGUMENT, "invalid FFT arguments");
+        cl_ctx* raw = nullptr;
+        if (cl_create(&raw, nx, ny, nz, 1, 1, 1, fp32 ? CL_MODE_FP32_FOURIER : CL_MODE_FP64_PLAIN) != CL_OK)
+            cl::fail(CL_ERR_ARGUMENT, "%s", cl_last_error());
+        std::unique_ptr<cl_ctx> c(raw);
+        const long long M = c->M;
+        const size_t n = (size_t)M * batch;
+        DevBuf<cx<double>> d64;
+        d64.upload(reinterpret_cast<const cx<double>*>(data), n, c->stream);
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            DevBuf<cx<T>> dT;
+            cx<T>* buf;
+            if constexpr (sizeof(T) == 4) {
+                dT.alloc(n);
+                clk::k_narrow<float><<<grid_for((long long)n), 256, 0, c->stream>>>(d64.p, dT.p, (long long)n);
+                CL_LAUNCHED();
+                buf = dT.p;
+            } else {
+                buf = d64.p;
+            }
+            const Axis& X = c->ax[0];
+            const Axis& Y = c->ax[1];
+            const Axis& Z = c->ax[2];
+            const cx<T>* twx = sizeof(T) == 4 ? (const cx<T>*)X.tw32.p : (const cx<T>*)X.tw64.p;
+            const cx<T>* twy = sizeof(T) == 4 ? (const cx<T>*)Y.tw32.p : (const cx<T>*)Y.tw64.p;
+            const cx<T>* twz = sizeof(T) == 4 ? (const cx<T>*)Z.tw32.p : (const cx<T>*)Z.tw64.p;
+            const int nrows = ny * nz;
+            const XTile xt = x_tile<T>(nx, nrows);
+            const LTile yt = l_tile<T>(ny, false);
+            const LTile zt = l_tile<T>(nz, false);
+            const int xblocks = (nrows + xt.rows - 1) / xt.rows;
+            const int ychunks = (nx + yt.W - 1) / yt.W;
+            const long long nxy = (long long)nx * ny;
+            const long long zblocks = (nxy + zt.W - 1) / zt.W;
+            if (sign < 0) {
+                ensure_smem(clk::k_xpass<-1, T>, xt.smem);
+                ensure_smem(clk::k_ypass<-1, T>, yt.smem);
+                clk::k_xpass<-1, T><<<dim3(xblocks, batch), 256, xt.smem, c->stream>>>(buf, M, X.plan, twx, nx, nrows,
+                                                                                      xt.rows, xt.ld);
+                CL_LAUNCHED();
+                clk::k_ypass<-1, T><<<dim3(ychunks * nz, batch), 256, yt.smem, c->stream>>>(buf, M, Y.plan, twy, nx,
+                                                                                           ny, yt.W, ychunks);
+                CL_LAUNCHED();
+            } else {
+                ensure_smem(clk::k_xpass<+1, T>, xt.smem);
+                ensure_smem(clk::k_ypass<+1, T>, yt.smem);
+                clk::k_xpass<+1, T><<<dim3(xblocks, batch), 256, xt.smem, c->stream>>>(buf, M, X.plan, twx, nx, nrows,
+                                                                                      xt.rows, xt.ld);
+                CL_LAUNCHED();
+                clk::k_ypass<+1, T><<<dim3(ychunks * nz, batch), 256, yt.smem, c->stream>>>(buf, M, Y.plan, twy, nx,
+                                                                                           ny, yt.W, ychunks);
+                CL_LAUNCHED();
+            }
+            ensure_smem(clk::k_zpass<T>, zt.smem);
+            clk::k_zpass<T><<<(unsigned)zblocks, 256, zt.smem, c->stream>>>(buf, M, Z.plan, twz, nullptr, nxy, nz,
+                                                                             zt.W, batch, sign);
+            CL_LAUNCHED();
+            if constexpr (sizeof(T) == 4) {
+                clk::k_widen<float><<<grid_for((long long)n), 256, 0, c->stream>>>(dT.p, d64.p, (long long)n);
+                CL_LAUNCHED();
+            }
+            CL_CUDA(cudaMemcpyAsync(data, d64.p, n * sizeof(cx<double>), cudaMemcpyDeviceToHost, c->stream));
+            CL_CUDA(cudaStreamSynchronize(c->stream));
+        };
+        if (fp32)
+            run(float{});
+        else
+            run(double{});
+    });
+}
+
+}  // extern "C"

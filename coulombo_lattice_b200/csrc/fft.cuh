@@ -1,0 +1,196 @@
+// Shared-memory mixed-radix FFT for sm_100a.
+//
+// Lines of length n sit in shared memory in "column" layout: element idx of line l is at
+// buf[idx * ld + l], so consecutive threads touch consecutive lines and a warp never
+// serialises on a bank.  The transform is the Stockham autosort formulation (Govindaraju et
+// al., "High Performance Discrete Fourier Transforms on Graphics Processors", SC08): every
+// stage of radix R reads R inputs n/R apart, applies the twiddles of its position k within
+// the current sub-transform, does an R-point DFT in registers and writes the outputs Ns
+// apart, ping-ponging between two buffers.  Radices 2, 3, 4, 5 and 8 cover every 2*3*5-smooth
+// length.  Conventions are FFTW's: sign -1 forward, +1 backward, both unnormalised.
+//
+// Twiddles come from a table tw[t] = exp(-2 pi i t / n) built on the host in extended
+// precision and rounded once to the working type.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace clk {
+
+template <typename T>
+struct alignas(2 * sizeof(T)) cx {
+    T re, im;
+};
+
+template <typename T>
+__device__ __forceinline__ cx<T> mk(T r, T i) {
+    cx<T> c;
+    c.re = r;
+    c.im = i;
+    return c;
+}
+template <typename T>
+__device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) { return mk(a.re + b.re, a.im + b.im); }
+template <typename T>
+__device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) { return mk(a.re - b.re, a.im - b.im); }
+template <typename T>
+__device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b) {
+    return mk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+template <typename T>
+__device__ __forceinline__ cx<T> cmulc(cx<T> a, cx<T> b) {  // a * conj(b)
+    return mk(a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im);
+}
+template <typename T>
+__device__ __forceinline__ cx<T> scale(cx<T> a, T s) { return mk(a.re * s, a.im * s); }
+// i * s * a for s = +-1
+template <int S, typename T>
+__device__ __forceinline__ cx<T> mul_is(cx<T> a) {
+    return S > 0 ? mk(-a.im, a.re) : mk(a.im, -a.re);
+}
+
+// Decimal values of the DFT constants (exact mathematical constants rounded by the compiler).
+#define CLK_SQRT1_2 0.70710678118654752440084436210484903928
+#define CLK_SIN60 0.86602540378443864676372317075293618347      // sin(2 pi/3)
+#define CLK_C1_5 0.30901699437494742410229341718281905886       // cos(2 pi/5)
+#define CLK_C2_5 (-0.80901699437494742410229341718281905886)    // cos(4 pi/5)
+#define CLK_S1_5 0.95105651629515357211643933337938214340       // sin(2 pi/5)
+#define CLK_S2_5 0.58778525229247312916870595463907276860       // sin(4 pi/5)
+
+// R-point DFTs in registers: v[k] <- sum_j v[j] exp(S * 2 pi i j k / R).
+template <int S, typename T>
+__device__ __forceinline__ void dft2(cx<T>* v) {
+    cx<T> a = v[0], b = v[1];
+    v[0] = a + b;
+    v[1] = a - b;
+}
+
+template <int S, typename T>
+__device__ __forceinline__ void dft3(cx<T>* v) {
+    const T h = T(0.5), s60 = T(CLK_SIN60);
+    cx<T> t1 = v[1] + v[2];
+    cx<T> t2 = v[0] - scale(t1, h);
+    cx<T> t3 = mul_is<S>(scale(v[1] - v[2], s60));
+    v[0] = v[0] + t1;
+    v[1] = t2 + t3;
+    v[2] = t2 - t3;
+}
+
+template <int S, typename T>
+__device__ __forceinline__ void dft4(cx<T>* v) {
+    cx<T> a = v[0] + v[2], b = v[0] - v[2];
+    cx<T> c = v[1] + v[3], d = mul_is<S>(v[1] - v[3]);
+    v[0] = a + c;
+    v[2] = a - c;
+    v[1] = b + d;
+    v[3] = b - d;
+}
+
+template <int S, typename T>
+__device__ __forceinline__ void dft5(cx<T>* v) {
+    const T c1 = T(CLK_C1_5), c2 = T(CLK_C2_5), s1 = T(CLK_S1_5), s2 = T(CLK_S2_5);
+    cx<T> a1 = v[1] + v[4], a2 = v[2] + v[3];
+    cx<T> b1 = v[1] - v[4], b2 = v[2] - v[3];
+    cx<T> x0 = v[0];
+    cx<T> p1 = x0 + scale(a1, c1) + scale(a2, c2);
+    cx<T> p2 = x0 + scale(a1, c2) + scale(a2, c1);
+    cx<T> q1 = mul_is<S>(scale(b1, s1) + scale(b2, s2));
+    cx<T> q2 = mul_is<S>(scale(b1, s2) - scale(b2, s1));
+    v[0] = x0 + a1 + a2;
+    v[1] = p1 + q1;
+    v[4] = p1 - q1;
+    v[2] = p2 + q2;
+    v[3] = p2 - q2;
+}
+
+template <int S, typename T>
+__device__ __forceinline__ void dft8(cx<T>* v) {
+    cx<T> e[4] = {v[0], v[2], v[4], v[6]};
+    cx<T> o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<S>(e);
+    dft4<S>(o);
+    const T r = T(CLK_SQRT1_2);
+    // w8^k = exp(S i pi k / 4)
+    cx<T> o1 = mk((o[1].re - S * o[1].im) * r, (o[1].im + S * o[1].re) * r);
+    cx<T> o2 = mul_is<S>(o[2]);
+    cx<T> o3 = mk((-o[3].re - S * o[3].im) * r, (-o[3].im + S * o[3].re) * r);
+    v[0] = e[0] + o[0];
+    v[4] = e[0] - o[0];
+    v[1] = e[1] + o1;
+    v[5] = e[1] - o1;
+    v[2] = e[2] + o2;
+    v[6] = e[2] - o2;
+    v[3] = e[3] + o3;
+    v[7] = e[3] - o3;
+}
+
+template <int R, int S, typename T>
+__device__ __forceinline__ void dft(cx<T>* v) {
+    if constexpr (R == 2) dft2<S>(v);
+    else if constexpr (R == 3) dft3<S>(v);
+    else if constexpr (R == 4) dft4<S>(v);
+    else if constexpr (R == 5) dft5<S>(v);
+    else dft8<S>(v);
+}
+
+// Radix schedule of one axis.  Passed by value as a kernel parameter.
+struct FftPlan {
+    int n;
+    int nst;
+    int radix[16];
+};
+
+// One Stockham stage over `lines` lines in column layout.
+template <int R, int S, typename T>
+__device__ __forceinline__ void stage(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst,
+                                      const cx<T>* __restrict__ tw, int n, int ns, int lines, int ld) {
+    const int nb = n / R;
+    const int total = nb * lines;
+    const int twstep = n / (ns * R);
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        const int line = b % lines;
+        const int j = b / lines;
+        const int k = j % ns;
+        cx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * ld + line];
+        if (ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                cx<T> w = tw[r * k * twstep];
+                v[r] = S < 0 ? cmul(v[r], w) : cmulc(v[r], w);
+            }
+        }
+        dft<R, S>(v);
+        const int base = (j / ns) * ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[(base + r * ns) * ld + line] = v[r];
+    }
+}
+
+// Full transform of every line; returns the buffer (a or b) that holds the result.
+// Must be called by every thread of the block; ends with a __syncthreads().
+template <int S, typename T>
+__device__ cx<T>* fft_lines(cx<T>* a, cx<T>* b, const cx<T>* __restrict__ tw, const FftPlan& p,
+                            int lines, int ld) {
+    int ns = 1;
+    for (int s = 0; s < p.nst; ++s) {
+        const int R = p.radix[s];
+        switch (R) {
+            case 2: stage<2, S>(a, b, tw, p.n, ns, lines, ld); break;
+            case 3: stage<3, S>(a, b, tw, p.n, ns, lines, ld); break;
+            case 4: stage<4, S>(a, b, tw, p.n, ns, lines, ld); break;
+            case 5: stage<5, S>(a, b, tw, p.n, ns, lines, ld); break;
+            default: stage<8, S>(a, b, tw, p.n, ns, lines, ld); break;
+        }
+        __syncthreads();
+        cx<T>* t = a;
+        a = b;
+        b = t;
+        ns *= R;
+    }
+    return a;
+}
+
+}  // namespace clk

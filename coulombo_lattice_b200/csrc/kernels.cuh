@@ -1,0 +1,437 @@
+// Device kernels of the Coulomb-integral path (sm_100a).
+//
+// Data layout in HBM
+//   grid buffers   [density][z][y][x]   cx<T>, x fastest (T = double for the plain form,
+//                                        float for the FP32 form)
+//   pair densities [density][atom]      cx<double>, atoms sorted by grid cell
+//   potentials     [density][atom]      cx<double>, accumulated over the 8 rounds
+//   Ghat           [(nz+1)][(ny+1)][(nx+1)] double (DCT-I of the kernel octant)
+//   Khat_kappa     [z][y][x] T           Ghat folded for round kappa, divided by 8M
+//
+// One round kappa of the convolution for every density is five passes:
+//   k_xfwd   scatter atoms -> rows, x conj(phase_kappa), FFT along x     (reads atoms only)
+//   k_ypass  FFT along y
+//   k_zpass  FFT along z, x Khat_kappa, inverse FFT along z             (Khat tile reused
+//                                                                        for all densities)
+//   k_ypass  inverse FFT along y
+//   k_xinv   inverse FFT along x, x phase_kappa, accumulate V at atoms  (writes atoms only)
+#pragma once
+
+#include "fft.cuh"
+
+namespace clk {
+
+constexpr double kE2_4PE0 = 14.39963737103201;  // e^2/(4 pi eps0) in eV*A (src/base.hpp:28)
+
+struct RoundPhase {
+    const cx<double>* px;  // exp(i pi x / nx)
+    const cx<double>* py;
+    const cx<double>* pz;
+    int kx, ky, kz;
+};
+
+__device__ __forceinline__ cx<double> round_phase(const RoundPhase& rp, int x, int y, int z) {
+    cx<double> p = mk(1.0, 0.0);
+    if (rp.kz) p = rp.pz[z];
+    if (rp.ky) p = cmul(rp.py[y], p);
+    if (rp.kx) p = cmul(rp.px[x], p);
+    return p;
+}
+
+template <typename T>
+__device__ __forceinline__ cx<T> narrow(cx<double> v) {
+    return mk(static_cast<T>(v.re), static_cast<T>(v.im));
+}
+template <typename T>
+__device__ __forceinline__ cx<double> widen(cx<T> v) {
+    return mk(static_cast<double>(v.re), static_cast<double>(v.im));
+}
+template <typename T>
+__device__ __forceinline__ cx<T> czero() {
+    return mk(T(0), T(0));
+}
+
+// ---------------------------------------------------------------------------------------
+// Coulomb kernel on the octant: Interaction.hpp:32-51 with Interaction.cpp:8-39.
+// ---------------------------------------------------------------------------------------
+struct KernelModel {
+    double dielectric;
+    double onsite;
+    int thomas_fermi;
+    double r_tf, q_tf;
+};
+
+__global__ void k_kernel_octant(double* __restrict__ G, int n1x, int n1y, int n1z, double sx, double sy,
+                                double sz, KernelModel km) {
+    const long long total = (long long)n1x * n1y * n1z;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(idx % n1x);
+        const int iy = (int)((idx / n1x) % n1y);
+        const int iz = (int)(idx / ((long long)n1x * n1y));
+        // same association as the reference, with no contraction into FMA
+        const double z = __dmul_rn((double)iz, sz), z2 = __dmul_rn(z, z);
+        const double y = __dmul_rn((double)iy, sy), y2z2 = __dadd_rn(z2, __dmul_rn(y, y));
+        const double x = __dmul_rn((double)ix, sx);
+        const double r = sqrt(__dadd_rn(y2z2, __dmul_rn(x, x)));
+        double eps = km.dielectric;
+        if (km.thomas_fermi && r < km.r_tf)
+            eps = km.dielectric * (km.q_tf * km.r_tf / (sinh(km.q_tf * (km.r_tf - r)) + km.q_tf * r));
+        G[idx] = idx == 0 ? km.onsite : kE2_4PE0 / (eps * r);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// REDFT00 along one axis (FFTW's DCT-I definition):
+//   Y_k = X_0 + (-1)^k X_{L-1} + 2 sum_{j=1}^{L-2} X_j cos(pi j k / (L-1)),  L = points.
+// Line l = (o, i) has element j at (o*L + j)*inner + i.  A block handles `nl` consecutive
+// lines staged in shared memory; ctab[t] = cos(pi t / (L-1)), t < 2(L-1).
+// ---------------------------------------------------------------------------------------
+__global__ void k_dct1(const double* __restrict__ in, double* __restrict__ out, int L, long long inner,
+                       long long nlines, int nl, const double* __restrict__ ctab) {
+    extern __shared__ double dsm[];
+    const int np = L - 1;  // N'
+    double* ct = dsm;       // 2*np
+    double* s = dsm + 2 * np;  // [L][nl]
+    for (int t = threadIdx.x; t < 2 * np; t += blockDim.x) ct[t] = ctab[t];
+    const long long l0 = (long long)blockIdx.x * nl;
+    const int cnt = (int)min((long long)nl, nlines - l0);
+    const bool rows = (inner == 1);
+    for (int e = threadIdx.x; e < L * nl; e += blockDim.x) {
+        int j, l;
+        if (rows) { l = e / L; j = e - l * L; } else { j = e / nl; l = e - j * nl; }
+        double v = 0.0;
+        if (l < cnt) {
+            const long long line = l0 + l;
+            const long long o = line / inner, i = line - o * inner;
+            v = in[(o * L + j) * inner + i];
+        }
+        s[j * nl + l] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < L * nl; e += blockDim.x) {
+        int k, l;
+        if (rows) { l = e / L; k = e - l * L; } else { k = e / nl; l = e - k * nl; }
+        if (l >= cnt) continue;
+        double acc = 0.0;
+        int t = k % (2 * np);
+        int idx = t;
+        for (int j = 1; j < np; ++j) {
+            acc += s[j * nl + l] * ct[idx];
+            idx += t;
+            if (idx >= 2 * np) idx -= 2 * np;
+        }
+        double y = s[l] + ((k & 1) ? -s[np * nl + l] : s[np * nl + l]) + 2.0 * acc;
+        const long long line = l0 + l;
+        const long long o = line / inner, i = line - o * inner;
+        out[(o * L + k) * inner + i] = y;
+    }
+}
+
+// Khat_kappa(x,y,z) = Ghat(f(2x+kx), f(2y+ky), f(2z+kz)) / (8M), f(q) = min(q, 2n-q)
+// (CoulombCalculator.cpp:130-144 and :102).
+template <typename T>
+__global__ void k_khat(const double* __restrict__ ghat, int nx, int ny, int nz, int kx, int ky, int kz,
+                       double denom, T* __restrict__ out) {
+    const long long M = (long long)nx * ny * nz;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < M;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(idx % nx);
+        const int y = (int)((idx / nx) % ny);
+        const int z = (int)(idx / ((long long)nx * ny));
+        const int qx = 2 * x + kx, qy = 2 * y + ky, qz = 2 * z + kz;
+        const int fx = min(qx, 2 * nx - qx), fy = min(qy, 2 * ny - qy), fz = min(qz, 2 * nz - qz);
+        out[idx] = static_cast<T>(ghat[((long long)fz * (ny + 1) + fy) * (nx + 1) + fx] / denom);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Pair densities at atoms: rho_p(a) = sum_o conj(c_fl[a][o]) c_fr[a][o]  (Product.cpp:16-30).
+// coeff is [state][atom][orb] in input atom order; orig maps sorted -> input atom.
+// ---------------------------------------------------------------------------------------
+__global__ void k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb,
+                               const int* __restrict__ orig, long long n_sorted,
+                               const int2* __restrict__ prods, cx<double>* __restrict__ rho) {
+    const int p = blockIdx.y;
+    const int2 f = prods[p];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_sorted;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long a = orig[i];
+        const cx<double>* L = coeff + ((long long)f.x * n_atoms + a) * n_orb;
+        const cx<double>* R = coeff + ((long long)f.y * n_atoms + a) * n_orb;
+        cx<double> s = mk(0.0, 0.0);
+        for (int k = 0; k < n_orb; ++k) {
+            const cx<double> l = L[k], r = R[k];
+            s = s + mk(l.re * r.re + l.im * r.im, l.re * r.im - l.im * r.re);
+        }
+        rho[(long long)p * n_sorted + i] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Pass 1: scatter + conj(phase) + forward FFT along x.  A block owns `rows` consecutive
+// rows (row = z*ny + y); atoms of those rows are [row_ptr[r0], row_ptr[r0+rows]) in the
+// cell-sorted atom list.  Densities are processed one after another by the same block.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_xfwd(const cx<double>* __restrict__ rho, long long rho_stride,
+                                             const int* __restrict__ row_ptr, const int* __restrict__ cell,
+                                             cx<T>* __restrict__ out, long long out_stride, FftPlan plan,
+                                             const cx<T>* __restrict__ tw_g, RoundPhase rp, int nx, int ny,
+                                             int nrows, int rows, int ld, int np) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* a = tw + nx;
+    cx<T>* b = a + (size_t)nx * ld;
+    const int r0 = blockIdx.x * rows;
+    const int nr = min(rows, nrows - r0);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + nr];
+    for (int p = 0; p < np; ++p) {
+        for (int e = threadIdx.x; e < nx * ld; e += blockDim.x) a[e] = czero<T>();
+        __syncthreads();
+        const cx<double>* rp_ = rho + (long long)p * rho_stride;
+        for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+            const int c = cell[i];
+            const int row = c / nx, x = c - row * nx;
+            const int y = row % ny, z = row / ny;
+            a[x * ld + (row - r0)] = narrow<T>(cmulc(rp_[i], round_phase(rp, x, y, z)));
+        }
+        __syncthreads();
+        const cx<T>* res = fft_lines<-1>(a, b, tw, plan, rows, ld);
+        cx<T>* o = out + (long long)p * out_stride + (long long)r0 * nx;
+        for (int e = threadIdx.x; e < nr * nx; e += blockDim.x) {
+            const int lr = e / nx, x = e - lr * nx;
+            o[e] = res[x * ld + lr];
+        }
+        __syncthreads();
+    }
+}
+
+// Dense in-place FFT along x of whole rows (the standalone FFT entry point).
+template <int S, typename T>
+__global__ void __launch_bounds__(256) k_xpass(cx<T>* __restrict__ buf, long long stride, FftPlan plan,
+                                              const cx<T>* __restrict__ tw_g, int nx, int nrows, int rows,
+                                              int ld) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* a = tw + nx;
+    cx<T>* b = a + (size_t)nx * ld;
+    const int r0 = blockIdx.x * rows;
+    const int nr = min(rows, nrows - r0);
+    cx<T>* base = buf + (long long)blockIdx.y * stride + (long long)r0 * nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+    for (int e = threadIdx.x; e < rows * nx; e += blockDim.x) {
+        const int lr = e / nx, x = e - lr * nx;
+        a[x * ld + lr] = lr < nr ? base[e] : czero<T>();
+    }
+    __syncthreads();
+    const cx<T>* res = fft_lines<S>(a, b, tw, plan, rows, ld);
+    for (int e = threadIdx.x; e < nr * nx; e += blockDim.x) {
+        const int lr = e / nx, x = e - lr * nx;
+        base[e] = res[x * ld + lr];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Pass along y (or any axis with stride `step` between points and W adjacent lines):
+// block = (tile of W consecutive x, one z, one density).
+// ---------------------------------------------------------------------------------------
+template <int S, typename T>
+__global__ void __launch_bounds__(256) k_ypass(cx<T>* __restrict__ buf, long long stride, FftPlan plan,
+                                              const cx<T>* __restrict__ tw_g, int nx, int ny, int W,
+                                              int xchunks) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* a = tw + ny;
+    cx<T>* b = a + (size_t)ny * W;
+    const int xc = blockIdx.x % xchunks, z = blockIdx.x / xchunks;
+    const int x0 = xc * W, w = min(W, nx - x0);
+    cx<T>* base = buf + (long long)blockIdx.y * stride + (long long)z * nx * ny + x0;
+    for (int i = threadIdx.x; i < ny; i += blockDim.x) tw[i] = tw_g[i];
+    for (int e = threadIdx.x; e < ny * W; e += blockDim.x) {
+        const int y = e / W, l = e - y * W;
+        a[e] = l < w ? base[(long long)y * nx + l] : czero<T>();
+    }
+    __syncthreads();
+    const cx<T>* res = fft_lines<S>(a, b, tw, plan, W, W);
+    for (int e = threadIdx.x; e < ny * W; e += blockDim.x) {
+        const int y = e / W, l = e - y * W;
+        if (l < w) base[(long long)y * nx + l] = res[e];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Pass along z: forward FFT, x Khat_kappa (tile loaded once per block and reused for all
+// densities), inverse FFT.  With khat == nullptr only the forward (S<0) or backward
+// transform is done (standalone FFT).  Block = W consecutive xy positions, all z.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_zpass(cx<T>* __restrict__ buf, long long stride, FftPlan plan,
+                                              const cx<T>* __restrict__ tw_g, const T* __restrict__ khat,
+                                              long long nxy, int nz, int W, int np, int sign) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* a = tw + nz;
+    cx<T>* b = a + (size_t)nz * W;
+    T* kt = reinterpret_cast<T*>(b + (size_t)nz * W);
+    const long long c0 = (long long)blockIdx.x * W;
+    const int w = (int)min((long long)W, nxy - c0);
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) tw[i] = tw_g[i];
+    if (khat) {
+        for (int e = threadIdx.x; e < nz * W; e += blockDim.x) {
+            const int z = e / W, l = e - z * W;
+            kt[e] = l < w ? khat[(long long)z * nxy + c0 + l] : T(0);
+        }
+    }
+    for (int p = 0; p < np; ++p) {
+        cx<T>* base = buf + (long long)p * stride + c0;
+        for (int e = threadIdx.x; e < nz * W; e += blockDim.x) {
+            const int z = e / W, l = e - z * W;
+            a[e] = l < w ? base[(long long)z * nxy + l] : czero<T>();
+        }
+        __syncthreads();
+        cx<T>* res;
+        if (khat) {
+            res = fft_lines<-1>(a, b, tw, plan, W, W);
+            for (int e = threadIdx.x; e < nz * W; e += blockDim.x) {
+                const T k = kt[e];
+                res[e] = mk(res[e].re * k, res[e].im * k);
+            }
+            __syncthreads();
+            res = fft_lines<+1>(res, res == a ? b : a, tw, plan, W, W);
+        } else if (sign < 0) {
+            res = fft_lines<-1>(a, b, tw, plan, W, W);
+        } else {
+            res = fft_lines<+1>(a, b, tw, plan, W, W);
+        }
+        for (int e = threadIdx.x; e < nz * W; e += blockDim.x) {
+            const int z = e / W, l = e - z * W;
+            if (l < w) base[(long long)z * nxy + l] = res[e];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Last pass: inverse FFT along x, x phase_kappa, V(atom) += value (FP64).  Each atom's row
+// belongs to exactly one block, and rounds are ordered on the stream, so the accumulation
+// needs no atomics.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_xinv(const cx<T>* __restrict__ buf, long long stride, FftPlan plan,
+                                             const cx<T>* __restrict__ tw_g, RoundPhase rp,
+                                             const int* __restrict__ row_ptr, const int* __restrict__ cell,
+                                             cx<double>* __restrict__ V, long long v_stride, int nx, int ny,
+                                             int nrows, int rows, int ld, int np) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* a = tw + nx;
+    cx<T>* b = a + (size_t)nx * ld;
+    const int r0 = blockIdx.x * rows;
+    const int nr = min(rows, nrows - r0);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + nr];
+    for (int p = 0; p < np; ++p) {
+        const cx<T>* base = buf + (long long)p * stride + (long long)r0 * nx;
+        for (int e = threadIdx.x; e < rows * nx; e += blockDim.x) {
+            const int lr = e / nx, x = e - lr * nx;
+            a[x * ld + lr] = lr < nr ? base[e] : czero<T>();
+        }
+        __syncthreads();
+        const cx<T>* res = fft_lines<+1>(a, b, tw, plan, rows, ld);
+        cx<double>* vp = V + (long long)p * v_stride;
+        for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+            const int c = cell[i];
+            const int row = c / nx, x = c - row * nx;
+            const int y = row % ny, z = row / ny;
+            vp[i] = vp[i] + cmul(widen(res[x * ld + (row - r0)]), round_phase(rp, x, y, z));
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Real-space reductions in FP64 (CoulombCalculator.cpp:165-172 restricted to the atom
+// cells, where the right density is non-zero): for left l and right r with V = a+ib and
+// rho = c+id, out[l][r] += {sum ac, sum bd, sum ad, sum bc}; then
+//   sum V rho       = (ac - bd) + i (ad + bc)
+//   sum V conj(rho) = (ac + bd) + i (bc - ad).
+// 64x64 (l, r) tiles, 4x4 per thread, atoms staged 16 at a time; split over atoms with one
+// FP64 atomicAdd per result per block.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_gram(const cx<double>* __restrict__ V, long long v_stride, int nl,
+                                             const cx<double>* __restrict__ rho, long long r_stride,
+                                             const int* __restrict__ ridx, int nr, long long n_atoms,
+                                             long long atoms_per_split, double* __restrict__ out) {
+    __shared__ cx<double> vs[16][64];
+    __shared__ cx<double> rs[16][64];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int l0 = blockIdx.x * 64, r0 = blockIdx.y * 64;
+    const long long k_begin = (long long)blockIdx.z * atoms_per_split;
+    const long long k_end = min(n_atoms, k_begin + atoms_per_split);
+    double acc[4][4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+    for (long long k0 = k_begin; k0 < k_end; k0 += 16) {
+        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+            const int row = e >> 4, k = e & 15;
+            const long long atom = k0 + k;
+            const bool ok = atom < k_end;
+            const int l = l0 + row, r = r0 + row;
+            vs[k][row] = (ok && l < nl) ? V[(long long)l * v_stride + atom] : mk(0.0, 0.0);
+            rs[k][row] = (ok && r < nr) ? rho[(long long)ridx[r] * r_stride + atom] : mk(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k) {
+            cx<double> v[4], r[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) v[i] = vs[k][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) r[j] = rs[k][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    acc[i][j][0] += v[i].re * r[j].re;
+                    acc[i][j][1] += v[i].im * r[j].im;
+                    acc[i][j][2] += v[i].re * r[j].im;
+                    acc[i][j][3] += v[i].im * r[j].re;
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int l = l0 + ty + 16 * i, r = r0 + tx + 16 * j;
+            if (l < nl && r < nr) {
+                double* o = out + ((long long)l * nr + r) * 4;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) atomicAdd(o + q, acc[i][j][q]);
+            }
+        }
+}
+
+// Grid-API scatter of a dense density into the "every cell is an atom" list is the identity;
+// its dot product reuses k_gram with nl = nr = 1.
+
+// Widening / narrowing copies for the standalone FFT entry point.
+template <typename T>
+__global__ void k_narrow(const cx<double>* __restrict__ in, cx<T>* __restrict__ out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = narrow<T>(in[i]);
+}
+template <typename T>
+__global__ void k_widen(const cx<T>* __restrict__ in, cx<double>* __restrict__ out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = widen(in[i]);
+}
+
+}  // namespace clk

@@ -1,0 +1,160 @@
+/*
+ * coulombo_lattice.h -- C ABI of the B200 Coulomb-integral library (libcoulombo_lattice.so).
+ *
+ * The reference (Coulombo-Lattice, Rozanski & Zielinski, Comput. Phys. Commun. 287 (2023)
+ * 108693) has no plugin or FFI layer: its compute seam is the C++ class CoulombCalculator
+ * fed by Product::map and Interaction::map inside one executable.  Each entry point below
+ * names the reference interface it replaces (path:line within the reference project).
+ *
+ * Conventions
+ *   - Every call returns 0 on success and a non-zero CL_ERR_* code on failure; the message
+ *     is then available from cl_last_error() (thread-local).  No C++ exception crosses this
+ *     boundary and no call aborts the process.
+ *   - All array arguments are caller-owned HOST buffers; the library copies them to the GPU.
+ *   - Grids are x-fastest: cell index = (iz*ny + iy)*nx + ix (run-tests.cpp:169-175).
+ *   - Complex values are interleaved {re, im} doubles.
+ *   - One context per host thread; a context is bound to the CUDA device that was current
+ *     when it was created.
+ */
+#ifndef COULOMBO_LATTICE_H
+#define COULOMBO_LATTICE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CL_OK              0
+#define CL_ERR_ARGUMENT    1  /* invalid argument (reference: std::logic_error / runtime_error) */
+#define CL_ERR_STATE       2  /* call out of order, e.g. calculate() before prepare() */
+#define CL_ERR_CUDA        3  /* CUDA runtime failure or no usable GPU */
+#define CL_ERR_MEMORY      4  /* device or host allocation failed */
+#define CL_ERR_UNSUPPORTED 5  /* size outside what the kernels handle (e.g. not 2*3*5-smooth) */
+#define CL_ERR_TIMEOUT     6  /* a bounded device-side wait gave up */
+
+/* precision / algorithm forms */
+#define CL_MODE_FP64_PLAIN   0  /* all-FP64: 8 rounds of FFT -> x Ghat -> iFFT, real-space dot */
+#define CL_MODE_FP32_FOURIER 1  /* FP32 FFT stages, FP64 kernel/twiddles/reductions/round sum */
+
+typedef struct cl_ctx cl_ctx;
+
+/* ---------------------------------------------------------------------------------------
+ * Calculator life cycle
+ * ------------------------------------------------------------------------------------- */
+
+/* Create a calculator for an nx*ny*nz grid with step lengths (sx, sy, sz) in Angstrom.
+ * Replaces CoulombCalculator::CoulombCalculator(const Dimension&) (src/CoulombCalculator.cpp:11-55)
+ * together with the step argument of InteractionBase (src/Interaction.hpp:19-20).
+ * Sizes must be products of 2, 3 and 5 (what Broadcaster::round4FFT produces,
+ * src/Broadcaster.cpp:136-143). */
+int cl_create(cl_ctx** out, int nx, int ny, int nz, double sx, double sy, double sz, int mode);
+
+/* Release every device buffer of the context.  Safe on NULL. */
+void cl_destroy(cl_ctx* ctx);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* cl_last_error(void);
+
+/* ---------------------------------------------------------------------------------------
+ * Coulomb kernel: Interaction::map + CoulombCalculator::initialize
+ * ------------------------------------------------------------------------------------- */
+
+/* G(r) = e^2/(4 pi eps0) / (eps(r) r) on the (nx+1)(ny+1)(nz+1) octant, G(0) = onsite (eV),
+ * then Ghat = REDFT00 (3D DCT-I) / (8 nx ny nz).  tf_lattice <= 0 selects the simple model
+ * (InteractionSimple, src/Interaction.cpp:8-14); tf_lattice > 0 the Thomas-Fermi-Resta model
+ * (InteractionThomasFermi, src/Interaction.cpp:18-39), which requires dielectric > 1.
+ * Replaces src/Interaction.hpp:32-51 and src/CoulombCalculator.cpp:57-103. */
+int cl_set_kernel_coulomb(cl_ctx* ctx, double dielectric, double onsite, double tf_lattice);
+
+/* Same as above for a caller-supplied octant G[(nx+1)(ny+1)(nz+1)] (x fastest): the
+ * reference's custom-Interaction seam (run-tests.cpp:13-21 feeds one to CoulombCalculator). */
+int cl_set_kernel_grid(cl_ctx* ctx, const double* G);
+
+/* ---------------------------------------------------------------------------------------
+ * Grid-level calculator (the reference's prepare/calculate state machine)
+ * ------------------------------------------------------------------------------------- */
+
+/* input = rho (nx*ny*nz complex), then prepare(): V = aperiodic G * rho by 8 rounds.
+ * Replaces CoulombCalculator::input + prepare() (src/CoulombCalculator.hpp:48, .cpp:105-163). */
+int cl_prepare_grid(cl_ctx* ctx, const double* rho);
+
+/* input = rho2, then calculate(): out = sum_r V(r) rho2(r) (no conjugation), reusing the
+ * last prepare.  Replaces CoulombCalculator::calculate() (src/CoulombCalculator.cpp:165-172). */
+int cl_calculate_grid(cl_ctx* ctx, const double* rho2, double out[2]);
+
+/* Copy the quasi-potential V of the last cl_prepare_grid (nx*ny*nz complex) to the host.
+ * Replaces CoulombCalculator::potential() (src/CoulombCalculator.hpp:90-93). */
+int cl_potential_grid(cl_ctx* ctx, double* V);
+
+/* ---------------------------------------------------------------------------------------
+ * Integral pipeline (FunctionCollection + Planner + the coulombo main loop)
+ * ------------------------------------------------------------------------------------- */
+
+/* Upload n_states LCAO states of n_atoms atoms x n_orb orbitals, coeff laid out
+ * [state][atom][orbital]{re,im} (the file order of src/FunctionCollection.cpp:56-84), and
+ * the grid cell of every atom (src/Broadcaster.cpp:76-87).  States are in input order,
+ * holes first (coulombo.cpp:96-117).  Replaces FunctionCollection::appendFile and the
+ * Broadcaster's coefficient scatter (src/FunctionCollection.cpp:86-89, src/Broadcaster.cpp:96-103). */
+int cl_set_states(cl_ctx* ctx, int n_states, int n_holes, int64_t n_atoms, int n_orb,
+                  const double* coeff, const int64_t* cells);
+
+/* Compute n_int integrals spec[i] = (i1,i2,i3,i4), 1-based input indices, into
+ * out[i] = {re, im} in eV.  Product indexing, conjugation flags, plan orientation and the
+ * result conjugation follow the reference (src/Planner.hpp:71-144, src/Graph.hpp:49-91,
+ * coulombo.cpp:186-209).  Replaces the whole "Computing requested integrals" phase. */
+int cl_compute(cl_ctx* ctx, int64_t n_int, const int16_t* spec, double* out);
+
+/* V of every state's own density |psi_s|^2 (real part) at every atom, out[state][atom].
+ * Replaces the loop of potentials.cpp:137-158 (createSelfProducts, prepare,
+ * extractAtomCellValues at src/FunctionCollection.cpp:122-131). */
+int cl_potentials(cl_ctx* ctx, double* out);
+
+/* Device time in milliseconds of the phases of the last cl_compute / cl_potentials:
+ * t[0] pair densities, t[1] transforms (all rounds), t[2] reductions, t[3] total. */
+int cl_last_timings(cl_ctx* ctx, double t[4]);
+
+/* ---------------------------------------------------------------------------------------
+ * FFT engine (FourierPlan seam, src/FourierPlan.hpp:17-39)
+ * ------------------------------------------------------------------------------------- */
+
+/* In-place batched 3D complex FFT of `batch` grids nx*ny*nz (x fastest), sign -1 forward or
+ * +1 backward, unnormalised (FFTW's convention).  fp32 != 0 runs the FP32 stages (data are
+ * rounded to float on upload and widened back).  Replaces fftw_execute on the plans of
+ * src/CoulombCalculator.cpp:17-32. */
+int cl_fft3d(int nx, int ny, int nz, int batch, int sign, int fp32, double* data);
+
+/* ---------------------------------------------------------------------------------------
+ * Host-side helpers (no GPU needed)
+ * ------------------------------------------------------------------------------------- */
+
+/* Smallest c * 2^i 3^j 5^k >= n.  Replaces Round::up<2,3,5> (src/Round.hpp:20-49). */
+int cl_round_up_235(int n, int c);
+
+/* Lattice-grid detection: per-axis float-GCD step, origin, raw size, 2*3*5 padding, and the
+ * cell index of every atom.  pos is [atom][3] in Angstrom; cells may be NULL.
+ * Replaces gcd/computeGrid/round4FFT and the cell loop of src/Broadcaster.cpp:8-87, 136-143.
+ * Fails with "could not find common grid step" like the reference. */
+int cl_detect_grid(const double* pos, int64_t n_atoms, int raw[3], int pad[3],
+                   double origin[3], double step[3], int64_t* cells);
+
+/* Number of 1-based (i1..i4) in [1,n_inputs]^4 matching the comma-separated pattern list,
+ * and (if specs != NULL and capacity suffices) the matches in lexicographic order as
+ * int16[4] each.  Replaces Pattern (src/Pattern.hpp:15-100) and coulombo.cpp:135-148. */
+int cl_enumerate_integrals(const char* pattern, int n_inputs, int n_holes, int64_t* count,
+                           int16_t* specs, int64_t capacity);
+
+/* Greedy vertex cover of an undirected graph with self-loops (edges as int pairs);
+ * in_cover[v] = 0/1.  Replaces Graph::computeVertexCover (src/Graph.hpp:49-91). */
+int cl_vertex_cover(int n_vertices, int64_t n_edges, const int32_t* edges, uint8_t* in_cover);
+
+/* The reference's execution plan for a list of integrals: steps[i] = {id, left, lconj,
+ * right, rconj} in execution order.  Replaces MasterPlanner (src/Planner.hpp:71-117). */
+int cl_plan(int n_inputs, int64_t n_int, const int16_t* spec, int32_t* steps /* [n_int][5] */);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COULOMBO_LATTICE_H */

@@ -1,0 +1,134 @@
+"""The integral pipeline (cl_set_states + cl_compute, cl_potentials) against the oracle
+and the reference's example golden."""
+import numpy as np
+import pytest
+
+import coulombo_lattice_b200 as cl
+from coulombo_lattice_b200 import synth
+from oracle import coulomb as C
+from oracle import host as H
+
+pytestmark = pytest.mark.gpu
+
+
+def gate(got, want, mode):
+    """FP64 plain path: 1e-10 relative.  FP32 form: max(1e-6 |I|, 1e-9 eV)."""
+    got = np.asarray(got)
+    want = np.asarray(want)
+    err = np.abs(got - want)
+    if mode == cl.MODE_FP64_PLAIN:
+        lim = 1e-10 * np.maximum(np.abs(want), 1e-300) + 1e-16
+    else:
+        lim = np.maximum(1e-6 * np.abs(want), 1e-9)
+    return err, lim
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_example_golden(mode):
+    import make_example_fixture as fx
+    d = fx.load()
+    g = cl.detect_grid(d["pos"])
+    with cl.CoulombCalculator(g["pad"], g["step"], mode) as cc:
+        cc.initialize(dielectric=11.4)
+        cc.set_states(d["coeff"][None], g["cells"], 0)
+        v = cc.compute([(1, 1, 1, 1)])[0]
+    text = H.format_outputs([(1, 1, 1, 1)], [v], 0, 1)["eeee"]
+    if mode == cl.MODE_FP64_PLAIN:
+        assert text[:29] == d["golden"]
+    assert abs(v - 0.09034007197751963) <= 1e-6 * 0.0903
+
+
+def _oracle_values(d, specs, dielectric=10.89, onsite=0.0, tf=None):
+    step = (synth.A_ZB / 4,) * 3
+    return np.array(H.compute_integrals(list(d["states"]), d["cells_idx"], d["dims"], step, specs,
+                                        dielectric=dielectric, onsite=onsite, tf_lattice=tf))
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("pattern", ["****", "eeee,hhhh,ehhe,eheh", "ijji,1*2*"])
+def test_c1_all_patterns(mode, pattern):
+    d = synth.build("c1")
+    n = d["states"].shape[0]
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals(pattern, n, d["holes"])]
+    want = _oracle_values(d, specs)
+    step = (synth.A_ZB / 4,) * 3
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], d["holes"])
+        got = cc.compute(specs)
+    err, lim = gate(got, want, mode)
+    assert np.all(err <= lim), (err / lim).max()
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_medium_structure_eight_states(mode):
+    """64^3 grid, 8 states (36 densities), the default four classes."""
+    d = synth.build("c3", cells=(16, 16, 16))
+    d["states"] = d["states"][:, :, :6]
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals(d["integrals"], 8, 4)]
+    want = _oracle_values(d, specs)
+    step = (synth.A_ZB / 4,) * 3
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], 4)
+        got = cc.compute(specs)
+    err, lim = gate(got, want, mode)
+    assert np.all(err <= lim), (err / lim).max()
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_unsorted_atoms_duplicates_onsite_tf(mode):
+    """Atom order does not matter; a later atom in the same cell replaces an earlier one
+    (F[cell] = value in atom order, Product.cpp:16-30); onsite and Thomas-Fermi kernel."""
+    d = synth.build("c1", cells=(3, 2, 2))
+    rng = np.random.default_rng(4)
+    perm = rng.permutation(d["states"].shape[1])
+    states = d["states"][:, perm]
+    cells = d["cells_idx"][perm]
+    # duplicate a few atoms into already occupied cells
+    dup = rng.choice(len(cells), 5, replace=False)
+    cells = np.concatenate([cells, cells[dup]])
+    extra = rng.normal(size=(states.shape[0], 5, states.shape[2])) * 0.05
+    states = np.concatenate([states, extra + 0j], axis=1)
+    d2 = dict(d, states=states, cells_idx=cells)
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    want = _oracle_values(d2, specs, onsite=1.7, tf=5.65)
+    step = (synth.A_ZB / 4,) * 3
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89, onsite=1.7, tf_lattice=5.65)
+        cc.set_states(states, cells, 2)
+        got = cc.compute(specs)
+    err, lim = gate(got, want, mode)
+    assert np.all(err <= lim), (err / lim).max()
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_potentials_match_oracle(mode):
+    d = synth.build("c1", cells=(3, 3, 2))
+    step = (synth.A_ZB / 4,) * 3
+    ghat = C.kernel_spectrum(C.kernel_octant(d["dims"], step, 10.89), d["dims"])
+    want = []
+    for s in range(d["states"].shape[0]):
+        rho = C.pair_density_atoms(d["states"][s], d["states"][s])
+        V = C.prepare(C.scatter_density(rho, d["cells_idx"], d["dims"]), ghat).ravel()
+        want.append(V[d["cells_idx"]].real)
+    want = np.array(want)
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], 0)
+        got = cc.potentials()
+    tol = 1e-10 if mode == cl.MODE_FP64_PLAIN else 1e-6
+    assert np.abs(got - want).max() <= tol * np.abs(want).max()
+
+
+def test_compute_requires_states_and_kernel():
+    with cl.CoulombCalculator((8, 8, 8)) as cc:
+        with pytest.raises(cl.CoulomboError) as e:
+            cc.compute([(1, 1, 1, 1)])
+        assert e.value.kind == "state"
+        cc.initialize(1.0)
+        with pytest.raises(cl.CoulomboError) as e:
+            cc.compute([(1, 1, 1, 1)])
+        assert e.value.kind == "state"
+        with pytest.raises(cl.CoulomboError, match="outside the grid"):
+            cc.set_states(np.ones((1, 2, 1), complex), np.array([0, 512]), 0)
