@@ -24,6 +24,9 @@ BIN_DIR = os.path.join(_HERE, "bin")
 MODE_FP64_PLAIN = 0
 MODE_FP32_FOURIER = 1
 
+# kernel classes of cl_kernel_profile (include/coulombo_lattice.h CL_KCLASS_*)
+KERNEL_CLASSES = ["pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram", "kernel_build", "spare"]
+
 _ERR_NAMES = {1: "argument", 2: "state", 3: "cuda", 4: "memory", 5: "unsupported", 6: "timeout"}
 
 _lib = None
@@ -55,6 +58,9 @@ SIGNATURES = [
     ("cl_compute", _i, [_vp, _i64, _P(ctypes.c_int16), _P(_d)]),
     ("cl_potentials", _i, [_vp, _P(_d)]),
     ("cl_last_timings", _i, [_vp, _P(_d)]),
+    ("cl_compute_rounds", _i, [_vp, _i64, _P(ctypes.c_int16), _i, _P(_d)]),
+    ("cl_set_profiling", _i, [_vp, _i]),
+    ("cl_kernel_profile", _i, [_vp, _P(_d), _P(_i64), _P(_d)]),
     ("cl_fft3d", _i, [_i, _i, _i, _i, _i, _i, _P(_d)]),
     ("cl_round_up_235", _i, [_i, _i]),
     ("cl_detect_grid", _i, [_P(_d), _i64, _P(_i), _P(_i), _P(_d), _P(_d), _P(_i64)]),
@@ -229,6 +235,35 @@ class CoulombCalculator:
         out = np.zeros(2 * s.shape[0])
         _check(lib().cl_compute(self._h, s.shape[0], _ptr(s, ctypes.c_int16), _ptr(out)))
         return out[0::2] + 1j * out[1::2]
+
+    def compute_rounds(self, specs, round_mask):
+        """Partial integrals over the rounds in round_mask (bit k = round kappa k)."""
+        s = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
+        out = np.zeros(2 * s.shape[0])
+        _check(lib().cl_compute_rounds(self._h, s.shape[0], _ptr(s, ctypes.c_int16), int(round_mask), _ptr(out)))
+        return out[0::2] + 1j * out[1::2]
+
+    def set_profiling(self, on=True):
+        _check(lib().cl_set_profiling(self._h, int(bool(on))))
+
+    def kernel_profile(self):
+        """{class: (ms, launches, algorithmic bytes)} since profiling was switched on."""
+        ms = np.zeros(8)
+        n = np.zeros(8, dtype=np.int64)
+        b = np.zeros(8)
+        _check(lib().cl_kernel_profile(self._h, _ptr(ms), _ptr(n, ctypes.c_int64), _ptr(b)))
+        return {KERNEL_CLASSES[k]: (float(ms[k]), int(n[k]), float(b[k])) for k in range(8) if n[k]}
+
+    def set_states_raw(self, n_states, n_holes, n_atoms, n_orb, coeff_ptr, cells_ptr):
+        """cl_set_states on raw host addresses (e.g. pinned buffers)."""
+        _check(lib().cl_set_states(self._h, int(n_states), int(n_holes), int(n_atoms), int(n_orb),
+                                   ctypes.cast(coeff_ptr, ctypes.POINTER(ctypes.c_double)),
+                                   ctypes.cast(cells_ptr, ctypes.POINTER(ctypes.c_int64))))
+        self.n_states, self.n_atoms = n_states, n_atoms
+
+    def compute_raw(self, n_int, spec_ptr, out_ptr):
+        _check(lib().cl_compute(self._h, int(n_int), ctypes.cast(spec_ptr, ctypes.POINTER(ctypes.c_int16)),
+                                ctypes.cast(out_ptr, ctypes.POINTER(ctypes.c_double))))
 
     def potentials(self):
         out = np.zeros((self.n_states, self.n_atoms))

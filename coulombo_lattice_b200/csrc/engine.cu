@@ -226,11 +226,26 @@ struct cl_ctx {
     DevBuf<unsigned char> work;
     double timings[4] = {0, 0, 0, 0};
 
+    // per-kernel profiling (events recorded around launches on `stream`)
+    struct ProfEntry {
+        int cls;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<ProfEntry> prof_pending;
+    double prof_ms[CL_NUM_KCLASS] = {};
+    double prof_bytes[CL_NUM_KCLASS] = {};
+    int64_t prof_launches[CL_NUM_KCLASS] = {};
+
     ~cl_ctx() {
         if (stream) {
             cudaStreamSynchronize(stream);
             for (auto& e : ev)
                 if (e) cudaEventDestroy(e);
+            for (auto& e : ev_pool) cudaEventDestroy(e);
             cudaStreamDestroy(stream);
         }
     }
@@ -242,6 +257,43 @@ size_t free_device_bytes() {
     size_t fr = 0, tot = 0;
     CL_CUDA(cudaMemGetInfo(&fr, &tot));
     return fr;
+}
+
+cudaEvent_t prof_event(cl_ctx* c) {
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t e;
+        CL_CUDA(cudaEventCreate(&e));
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+
+// Marks the start of a launch of class `cls`; returns the start event (or nullptr).
+cudaEvent_t prof_begin(cl_ctx* c) {
+    if (!c->profiling) return nullptr;
+    cudaEvent_t a = prof_event(c);
+    CL_CUDA(cudaEventRecord(a, c->stream));
+    return a;
+}
+
+void prof_end(cl_ctx* c, cudaEvent_t a, int cls, double bytes) {
+    if (!a) return;
+    cudaEvent_t b = prof_event(c);
+    CL_CUDA(cudaEventRecord(b, c->stream));
+    c->prof_pending.push_back({cls, a, b, bytes});
+}
+
+// After the stream has been synchronised: fold the pending pairs into the totals.
+void prof_collect(cl_ctx* c) {
+    for (const auto& e : c->prof_pending) {
+        float ms = 0;
+        CL_CUDA(cudaEventElapsedTime(&ms, e.a, e.b));
+        c->prof_ms[e.cls] += ms;
+        c->prof_bytes[e.cls] += e.bytes;
+        c->prof_launches[e.cls] += 1;
+    }
+    c->prof_pending.clear();
+    c->ev_used = 0;
 }
 
 void build_khat(cl_ctx* c) {
@@ -298,11 +350,16 @@ void transform_kernel(cl_ctx* c) {
     c->kernel_ready = true;
 }
 
+// Number of atoms listed by a row CSR (host-side copy kept with the CSR).
+long long row_ptr_count(cl_ctx* c, const int* row_ptr) {
+    return row_ptr == c->row_ptr.p ? c->n_sorted : c->M;
+}
+
 // One request's transforms: for every density p in [0, np) (rho rows), V[p] += the 8-round
 // convolution at the atoms of the row CSR.  buf holds `chunk` grids of type T.
 template <typename T>
 void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, const int* row_ptr,
-                const int* cell, cx<double>* V, long long v_stride) {
+                const int* cell, cx<double>* V, long long v_stride, int round_mask) {
     const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
     const int nrows = ny * nz;
     const long long nxy = (long long)nx * ny;
@@ -332,39 +389,53 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     const int ychunks = (nx + yt.W - 1) / yt.W;
     const long long zblocks = (nxy + zt.W - 1) / zt.W;
 
+    // algorithmic bytes per density of each pass (minimum HBM traffic of its work)
+    const double gbytes = (double)grid_bytes;
+    const double atoms = (double)(row_ptr_count(c, row_ptr));
     for (int p0 = 0; p0 < np; p0 += chunk) {
         const int cnt = std::min(chunk, np - p0);
         const cx<double>* rho_c = rho + (long long)p0 * rho_stride;
         cx<double>* V_c = V + (long long)p0 * v_stride;
         for (int r = 0; r < 8; ++r) {
+            if (!((round_mask >> r) & 1)) continue;
             clk::RoundPhase rp{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, r & 1, (r >> 1) & 1,
                                (r >> 2) & 1};
             const T* kh = sizeof(T) == 4 ? (const T*)c->khat32[r].p : (const T*)c->khat64[r].p;
+            cudaEvent_t e = prof_begin(c);
             clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan,
                                                                  twx, rp, nx, ny, nrows, xt.rows, xt.ld, cnt);
             CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * 16.0 + gbytes) + atoms * 4.0);
+            e = prof_begin(c);
             clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx, ny,
                                                                                       yt.W, ychunks);
             CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
+            e = prof_begin(c);
             clk::k_zpass<T><<<(unsigned)zblocks, 256, zt.smem, c->stream>>>(buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W,
                                                                              cnt, 0);
             CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
+            e = prof_begin(c);
             clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx, ny,
                                                                                       yt.W, ychunks);
             CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
+            e = prof_begin(c);
             clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, rp, row_ptr, cell, V_c,
                                                                  v_stride, nx, ny, nrows, xt.rows, xt.ld, cnt);
             CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_XINV, cnt * (gbytes + atoms * 32.0) + atoms * 4.0);
         }
     }
 }
 
 void run_rounds_mode(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, const int* row_ptr,
-                     const int* cell, cx<double>* V, long long v_stride) {
+                     const int* cell, cx<double>* V, long long v_stride, int round_mask = 0xFF) {
     if (c->mode == CL_MODE_FP64_PLAIN)
-        run_rounds<double>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride);
+        run_rounds<double>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride, round_mask);
     else
-        run_rounds<float>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride);
+        run_rounds<float>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride, round_mask);
 }
 
 // out4[l][r] = {sum ac, bd, ad, bc} over atoms (see k_gram).
@@ -380,9 +451,11 @@ void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<d
         splits = 65535;
         per = ((n_atoms + splits - 1) / splits + 15) / 16 * 16;
     }
+    cudaEvent_t e = prof_begin(c);
     clk::k_gram<<<dim3(tl, tr, (unsigned)splits), 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr,
                                                                         n_atoms, per, out4_dev);
     CL_LAUNCHED();
+    prof_end(c, e, CL_KCLASS_GRAM, (double)(nl + nr) * n_atoms * 16.0);
 }
 
 void check_ctx(cl_ctx* c) {
@@ -481,10 +554,14 @@ int cl_set_kernel_coulomb(cl_ctx* c, double dielectric, double onsite, double tf
         const long long total = (long long)n1x * n1y * n1z;
         c->kernel_ready = false;
         c->ghat.alloc(total);
+        cudaEvent_t pe = prof_begin(c);
         clk::k_kernel_octant<<<grid_for(total), 256, 0, c->stream>>>(c->ghat.p, n1x, n1y, n1z, c->step[0], c->step[1],
                                                                      c->step[2], km);
         CL_LAUNCHED();
         transform_kernel(c);
+        prof_end(c, pe, CL_KCLASS_KERNEL, (double)total * 8.0 * 7.0 + (double)c->M * 8.0 * (c->mode ? 4.0 : 8.0));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        prof_collect(c);
     });
 }
 
@@ -593,8 +670,11 @@ int cl_set_states(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_o
     });
 }
 
-int cl_compute(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out) {
-    return cl::guarded([&] {
+}  // extern "C"
+
+namespace {
+void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, int round_mask) {
+    {
         check_ctx(c);
         check_kernel(c);
         if (c->n_states == 0) cl::fail(CL_ERR_STATE, "no states loaded (call cl_set_states)");
@@ -639,12 +719,14 @@ int cl_compute(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out) {
         DevBuf<double> o4;
         o4.alloc((size_t)4 * nl * nr);
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+        cudaEvent_t pe = prof_begin(c);
         clk::k_pair_density<<<dim3(grid_for(As), nu), 256, 0, c->stream>>>(
             c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, As, dprods.p, rho.p);
         CL_LAUNCHED();
+        prof_end(c, pe, CL_KCLASS_DENSITY, (double)c->n_states * c->n_atoms * c->n_orb * 16.0 + (double)nu * As * 16.0);
         CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)nl * As, c->stream));
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
-        run_rounds_mode(c, rho.p, As, nl, c->row_ptr.p, c->cell_sorted.p, V.p, As);
+        run_rounds_mode(c, rho.p, As, nl, c->row_ptr.p, c->cell_sorted.p, V.p, As, round_mask);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
         gram(c, V.p, As, nl, rho.p, As, dr.p, nr, As, o4.p);
         CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
@@ -660,6 +742,7 @@ int cl_compute(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out) {
         c->timings[1] = t12;
         c->timings[2] = t23;
         c->timings[3] = t03;
+        prof_collect(c);
         // step values (coulombo.cpp:199-207)
         for (const auto& s : plan) {
             const int l = slot[s.left.product], r = rcol[s.right.product];
@@ -676,6 +759,48 @@ int cl_compute(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out) {
             if (s.left.conjugate) im = -im;
             out[2 * s.id] = re;
             out[2 * s.id + 1] = im;
+        }
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int cl_compute(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out) {
+    return cl::guarded([&] { compute_impl(c, n_int, spec, out, 0xFF); });
+}
+
+int cl_compute_rounds(cl_ctx* c, int64_t n_int, const int16_t* spec, int round_mask, double* out) {
+    return cl::guarded([&] {
+        if (round_mask < 0 || round_mask > 0xFF) cl::fail(CL_ERR_ARGUMENT, "round mask must be within 0..255");
+        compute_impl(c, n_int, spec, out, round_mask);
+    });
+}
+
+int cl_set_profiling(cl_ctx* c, int enable) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        prof_collect(c);
+        c->profiling = enable != 0;
+        if (c->profiling) {
+            std::fill(std::begin(c->prof_ms), std::end(c->prof_ms), 0.0);
+            std::fill(std::begin(c->prof_bytes), std::end(c->prof_bytes), 0.0);
+            std::fill(std::begin(c->prof_launches), std::end(c->prof_launches), (int64_t)0);
+        }
+    });
+}
+
+int cl_kernel_profile(cl_ctx* c, double ms[CL_NUM_KCLASS], int64_t launches[CL_NUM_KCLASS],
+                      double bytes[CL_NUM_KCLASS]) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        prof_collect(c);
+        for (int k = 0; k < CL_NUM_KCLASS; ++k) {
+            if (ms) ms[k] = c->prof_ms[k];
+            if (launches) launches[k] = c->prof_launches[k];
+            if (bytes) bytes[k] = c->prof_bytes[k];
         }
     });
 }
@@ -711,6 +836,7 @@ int cl_potentials(cl_ctx* c, double* out) {
         float t01, t12;
         CL_CUDA(cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]));
         CL_CUDA(cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]));
+        prof_collect(c);
         c->timings[0] = t01;
         c->timings[1] = t12;
         c->timings[2] = 0;

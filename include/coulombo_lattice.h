@@ -111,9 +111,34 @@ int cl_compute(cl_ctx* ctx, int64_t n_int, const int16_t* spec, double* out);
  * extractAtomCellValues at src/FunctionCollection.cpp:122-131). */
 int cl_potentials(cl_ctx* ctx, double* out);
 
+/* Same as cl_compute restricted to the rounds kappa whose bit is set in round_mask
+ * (bit 0 = kappa 0 ... bit 7 = kappa 7).  The integrals are sums over rounds
+ * (CoulombCalculator.cpp:105-163 accumulates V_ += Ftemp per round), so partial results
+ * of disjoint masks add up to cl_compute's: the unit of work a multi-GPU split hands each
+ * rank before one all-reduce.  No reference counterpart (single-process decomposition of
+ * the reference's prepare()). */
+int cl_compute_rounds(cl_ctx* ctx, int64_t n_int, const int16_t* spec, int round_mask, double* out);
+
 /* Device time in milliseconds of the phases of the last cl_compute / cl_potentials:
  * t[0] pair densities, t[1] transforms (all rounds), t[2] reductions, t[3] total. */
 int cl_last_timings(cl_ctx* ctx, double t[4]);
+
+/* Per-kernel timing with CUDA events recorded on the context's stream around every launch.
+ * Classes: */
+#define CL_KCLASS_DENSITY   0  /* pair densities at atoms */
+#define CL_KCLASS_XFWD      1  /* scatter + phase + FFT along x */
+#define CL_KCLASS_YPASS     2  /* FFT along y (both directions) */
+#define CL_KCLASS_ZPASS     3  /* FFT along z, x Khat, inverse FFT along z */
+#define CL_KCLASS_XINV      4  /* inverse FFT along x + phase + accumulate V at atoms */
+#define CL_KCLASS_GRAM      5  /* FP64 real-space reductions */
+#define CL_KCLASS_KERNEL    6  /* Coulomb kernel octant, DCT-I, folded kernels */
+#define CL_NUM_KCLASS       8
+/* enable != 0 starts recording (and clears the counters); 0 stops. */
+int cl_set_profiling(cl_ctx* ctx, int enable);
+/* Accumulated device milliseconds, launches and algorithmic bytes (the minimum HBM
+ * traffic of each launch's work, see the kernel notes) per class since profiling started. */
+int cl_kernel_profile(cl_ctx* ctx, double ms[CL_NUM_KCLASS], int64_t launches[CL_NUM_KCLASS],
+                      double bytes[CL_NUM_KCLASS]);
 
 /* ---------------------------------------------------------------------------------------
  * FFT engine (FourierPlan seam, src/FourierPlan.hpp:17-39)
