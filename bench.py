@@ -317,10 +317,11 @@ def run_ours(args):
     traffic = profiled_traffic(args.config, dom)
     fft_ms = sum(v[0] for v in fft_classes.values())
     # FFT HBM-roofline %: sum of 2*M*s bytes over every 3D transform (8 forward + 8 inverse
-    # per prepared density) / time of all transform passes / peak.  Each request runs 16
-    # y passes of cnt*2*M*s algorithmic bytes, i.e. exactly that sum.
-    fft_bytes = fft_classes["y_pass"][2]
-    buf_mb = fft_classes["y_pass"][2] / fft_classes["y_pass"][1] / 2 / 1e6
+    # per prepared density) / time of all transform passes / peak.
+    M = int(np.prod(d["dims"]))
+    n_prepared = len({int(s[1]) for s in cl.plan(n, specs)})
+    fft_bytes = args.steps * 16 * n_prepared * 2.0 * M * 8
+    buf_mb = n_prepared * M * 8 / 1e6
     total_launches = sum(v[1] for v in prof.values())
 
     line = {
@@ -329,7 +330,8 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.config], "integrals_per_step": int(n_int),
                    "form": "FP32 transforms, FP64 kernel/twiddles/reductions/round sum",
-                   "l2": "inputs larger than L2 (126 MB): every pass streams the %.0f MB transform buffer" % buf_mb,
+                   "l2": "inputs larger than L2 (126 MB): %.0f MB of transformed grids per request, "
+                         "streamed in chunks" % buf_mb, "prepared_densities": n_prepared,
                    "init_ms_kernel_build": init_ms, "wall_ms_per_step": wall_ms / args.steps},
         "accuracy": accuracy,
         "plain_fp64": {"value": world * n_int / (plain_ms / 1e3), "ms_per_step": plain_ms,

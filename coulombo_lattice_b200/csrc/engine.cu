@@ -3,6 +3,7 @@
 #include <array>
 #include <memory>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -97,12 +98,33 @@ FftPlan make_plan(int n) {
         p.radix[p.nst++] = r;
         m /= r;
     };
-    while (m % 8 == 0) push(8);
-    while (m % 4 == 0) push(4);
-    while (m % 2 == 0) push(2);
-    while (m % 3 == 0) push(3);
-    while (m % 5 == 0) push(5);
+    // fewest shared-memory round trips: radix 16 first, then 8/4, a lone 2 joined with a
+    // 3 (-> 6) or 5 (-> 10), a lone 4 with a 3 (-> 12), then 3s and 5s
+    int twos = 0, threes = 0, fives = 0;
+    for (; m % 2 == 0; m /= 2) ++twos;
+    for (; m % 3 == 0; m /= 3) ++threes;
+    for (; m % 5 == 0; m /= 5) ++fives;
     if (m != 1) cl::fail(CL_ERR_UNSUPPORTED, "FFT length %d is not a product of 2, 3 and 5", n);
+    m = n;
+    while (twos >= 4) { push(16); twos -= 4; }
+    if (twos == 3) { push(8); twos = 0; }
+    if (twos == 2) {
+        if (threes > 0) { push(12); --threes; } else push(4);
+        twos = 0;
+    }
+    if (twos == 1) {
+        if (threes > 0) { push(6); --threes; }
+        else if (fives > 0) { push(10); --fives; }
+        else push(2);
+        twos = 0;
+    }
+    while (threes-- > 0) push(3);
+    while (fives-- > 0) push(5);
+    int ns = 1;
+    for (int s = 0; s < p.nst; ++s) {
+        p.ns_magic[s] = clk::fdiv_magic(ns);
+        ns *= p.radix[s];
+    }
     return p;
 }
 
@@ -182,6 +204,28 @@ LTile l_tile(int n, bool with_khat) {
     };
     while (W > 1 && bytes(W) > 200 * 1024) W /= 2;
     return LTile{W, bytes(W)};
+}
+
+// Whole xy-plane in shared memory ([y][ld], ld odd) plus both twiddle tables.
+struct PlaneTile {
+    bool fits;
+    int ld;
+    size_t smem;
+};
+template <typename T>
+PlaneTile plane_tile(int nx, int ny) {
+    const int ld = (nx % 2 == 0) ? nx + 1 : nx;
+    const size_t smem = sizeof(cx<T>) * ((size_t)nx + ny + (size_t)ny * ld);
+    const bool fits = smem <= 220 * 1024 && clk::plane_size_supported(nx) && clk::plane_size_supported(ny) &&
+                      !std::getenv("CL_NO_XY_FUSION");
+    return PlaneTile{fits, ld, smem};
+}
+
+// Bytes of grids a chunk may hold so that consecutive passes meet in L2 (CL_L2_CHUNK_MB).
+size_t l2_chunk_bytes() {
+    const char* e = std::getenv("CL_L2_CHUNK_MB");
+    double mb = e ? std::atof(e) : 48.0;
+    return (size_t)(std::max(0.0, mb) * 1024 * 1024);
 }
 
 template <typename K>
@@ -364,9 +408,14 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     const int nrows = ny * nz;
     const long long nxy = (long long)nx * ny;
     const size_t grid_bytes = sizeof(cx<T>) * (size_t)c->M;
-    // densities per chunk: keep the work buffer within 60% of the free memory
+    // Densities per chunk.  When a few grids fit in L2, chunks are sized so that the passes of
+    // one round hand their output to the next pass through L2; otherwise chunks are as large
+    // as 60% of the free memory allows (fewer, larger launches and Khat reuse in the z pass).
+    const size_t l2_budget = l2_chunk_bytes();
     size_t budget = (size_t)(0.6 * (double)(free_device_bytes() + c->work.n));
-    int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)np, budget / grid_bytes));
+    size_t by_mem = std::max<size_t>(1, budget / grid_bytes);
+    size_t by_l2 = l2_budget / grid_bytes;
+    int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)np, by_l2 >= 2 ? by_l2 : by_mem));
     c->work.alloc(std::max(c->work.n, (size_t)chunk * grid_bytes));
     cx<T>* buf = reinterpret_cast<cx<T>*>(c->work.p);
 
@@ -380,10 +429,17 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     const XTile xt = x_tile<T>(nx, nrows);
     const LTile yt = l_tile<T>(ny, false);
     const LTile zt = l_tile<T>(nz, true);
-    ensure_smem(clk::k_xfwd<T>, xt.smem);
-    ensure_smem(clk::k_xinv<T>, xt.smem);
-    ensure_smem(clk::k_ypass<-1, T>, yt.smem);
-    ensure_smem(clk::k_ypass<+1, T>, yt.smem);
+    const PlaneTile pt = plane_tile<T>(nx, ny);
+    constexpr int VALS = sizeof(T) == 4 ? 8 : 4;
+    if (pt.fits) {
+        ensure_smem(clk::k_xyfwd<T, VALS>, pt.smem);
+        ensure_smem(clk::k_xyinv<T, VALS>, pt.smem);
+    } else {
+        ensure_smem(clk::k_xfwd<T>, xt.smem);
+        ensure_smem(clk::k_xinv<T>, xt.smem);
+        ensure_smem(clk::k_ypass<-1, T>, yt.smem);
+        ensure_smem(clk::k_ypass<+1, T>, yt.smem);
+    }
     ensure_smem(clk::k_zpass<T>, zt.smem);
     const int xblocks = (nrows + xt.rows - 1) / xt.rows;
     const int ychunks = (nx + yt.W - 1) / yt.W;
@@ -402,28 +458,43 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
                                (r >> 2) & 1};
             const T* kh = sizeof(T) == 4 ? (const T*)c->khat32[r].p : (const T*)c->khat64[r].p;
             cudaEvent_t e = prof_begin(c);
-            clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan,
-                                                                 twx, rp, nx, ny, nrows, xt.rows, xt.ld, cnt);
+            if (pt.fits) {
+                clk::k_xyfwd<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
+                    rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan, Y.plan, twx, twy, rp, nx, ny, pt.ld);
+            } else {
+                clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, c->M,
+                                                                     X.plan, twx, rp, nx, ny, nrows, xt.rows, xt.ld,
+                                                                     cnt);
+            }
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * 16.0 + gbytes) + atoms * 4.0);
-            e = prof_begin(c);
-            clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx, ny,
-                                                                                      yt.W, ychunks);
-            CL_LAUNCHED();
-            prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
+            if (!pt.fits) {
+                e = prof_begin(c);
+                clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx,
+                                                                                          ny, yt.W, ychunks);
+                CL_LAUNCHED();
+                prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
+            }
             e = prof_begin(c);
             clk::k_zpass<T><<<(unsigned)zblocks, 256, zt.smem, c->stream>>>(buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W,
                                                                              cnt, 0);
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
+            if (!pt.fits) {
+                e = prof_begin(c);
+                clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx,
+                                                                                          ny, yt.W, ychunks);
+                CL_LAUNCHED();
+                prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
+            }
             e = prof_begin(c);
-            clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx, ny,
-                                                                                      yt.W, ychunks);
-            CL_LAUNCHED();
-            prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
-            e = prof_begin(c);
-            clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, rp, row_ptr, cell, V_c,
-                                                                 v_stride, nx, ny, nrows, xt.rows, xt.ld, cnt);
+            if (pt.fits) {
+                clk::k_xyinv<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
+                    buf, c->M, X.plan, Y.plan, twx, twy, rp, row_ptr, cell, V_c, v_stride, nx, ny, pt.ld);
+            } else {
+                clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, rp, row_ptr, cell, V_c,
+                                                                     v_stride, nx, ny, nrows, xt.rows, xt.ld, cnt);
+            }
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_XINV, cnt * (gbytes + atoms * 32.0) + atoms * 4.0);
         }

@@ -6,8 +6,8 @@
 // al., "High Performance Discrete Fourier Transforms on Graphics Processors", SC08): every
 // stage of radix R reads R inputs n/R apart, applies the twiddles of its position k within
 // the current sub-transform, does an R-point DFT in registers and writes the outputs Ns
-// apart, ping-ponging between two buffers.  Radices 2, 3, 4, 5 and 8 cover every 2*3*5-smooth
-// length.  Conventions are FFTW's: sign -1 forward, +1 backward, both unnormalised.
+// apart, ping-ponging between two buffers.  Radices 2, 3, 4, 5, 8 and the composite register
+// codelets 6, 10, 12, 16 cover every 2*3*5-smooth length.  Conventions are FFTW's: sign -1 forward, +1 backward, both unnormalised.
 //
 // Twiddles come from a table tw[t] = exp(-2 pi i t / n) built on the host in extended
 // precision and rounded once to the working type.
@@ -125,33 +125,223 @@ __device__ __forceinline__ void dft8(cx<T>* v) {
     v[7] = e[3] - o3;
 }
 
+template <int N>
+struct WConst;
+// Twiddle constants exp(2 pi i m / N) of the composite register codelets, evaluated to
+// 40 digits from the Taylor series of cos and sin (generated once; values are exact
+// mathematical constants, not taken from any library).
+template <> struct WConst<6> {
+    static __device__ __forceinline__ double c(int m) {
+        switch (m) {
+            case 0: return 1.0000000000000000000000000000000000000000;
+            case 1: return 0.5000000000000000000000000000000000000000;
+            case 2: return -0.5000000000000000000000000000000000000000;
+            case 3: return -1.0000000000000000000000000000000000000000;
+            case 4: return -0.5000000000000000000000000000000000000000;
+            case 5: return 0.5000000000000000000000000000000000000000;
+        }
+        return 0.0;
+    }
+    static __device__ __forceinline__ double s(int m) {
+        switch (m) {
+            case 0: return 0.0000000000000000000000000000000000000000;
+            case 1: return 0.8660254037844386467637231707529361834714;
+            case 2: return 0.8660254037844386467637231707529361834714;
+            case 3: return 0.0000000000000000000000000000000000000000;
+            case 4: return -0.8660254037844386467637231707529361834714;
+            case 5: return -0.8660254037844386467637231707529361834714;
+        }
+        return 0.0;
+    }
+};
+template <> struct WConst<10> {
+    static __device__ __forceinline__ double c(int m) {
+        switch (m) {
+            case 0: return 1.0000000000000000000000000000000000000000;
+            case 1: return 0.8090169943749474241022934171828190588602;
+            case 2: return 0.3090169943749474241022934171828190588602;
+            case 3: return -0.3090169943749474241022934171828190588602;
+            case 4: return -0.8090169943749474241022934171828190588602;
+            case 5: return -1.0000000000000000000000000000000000000000;
+            case 6: return -0.8090169943749474241022934171828190588602;
+            case 7: return -0.3090169943749474241022934171828190588602;
+            case 8: return 0.3090169943749474241022934171828190588602;
+            case 9: return 0.8090169943749474241022934171828190588602;
+        }
+        return 0.0;
+    }
+    static __device__ __forceinline__ double s(int m) {
+        switch (m) {
+            case 0: return 0.0000000000000000000000000000000000000000;
+            case 1: return 0.5877852522924731291687059546390727685977;
+            case 2: return 0.9510565162951535721164393333793821434057;
+            case 3: return 0.9510565162951535721164393333793821434057;
+            case 4: return 0.5877852522924731291687059546390727685977;
+            case 5: return 0.0000000000000000000000000000000000000000;
+            case 6: return -0.5877852522924731291687059546390727685977;
+            case 7: return -0.9510565162951535721164393333793821434057;
+            case 8: return -0.9510565162951535721164393333793821434057;
+            case 9: return -0.5877852522924731291687059546390727685977;
+        }
+        return 0.0;
+    }
+};
+template <> struct WConst<12> {
+    static __device__ __forceinline__ double c(int m) {
+        switch (m) {
+            case 0: return 1.0000000000000000000000000000000000000000;
+            case 1: return 0.8660254037844386467637231707529361834714;
+            case 2: return 0.5000000000000000000000000000000000000000;
+            case 3: return -0.0000000000000000000000000000000000000000;
+            case 4: return -0.5000000000000000000000000000000000000000;
+            case 5: return -0.8660254037844386467637231707529361834714;
+            case 6: return -1.0000000000000000000000000000000000000000;
+            case 7: return -0.8660254037844386467637231707529361834714;
+            case 8: return -0.5000000000000000000000000000000000000000;
+            case 9: return -0.0000000000000000000000000000000000000000;
+            case 10: return 0.5000000000000000000000000000000000000000;
+            case 11: return 0.8660254037844386467637231707529361834714;
+        }
+        return 0.0;
+    }
+    static __device__ __forceinline__ double s(int m) {
+        switch (m) {
+            case 0: return 0.0000000000000000000000000000000000000000;
+            case 1: return 0.5000000000000000000000000000000000000000;
+            case 2: return 0.8660254037844386467637231707529361834714;
+            case 3: return 1.0000000000000000000000000000000000000000;
+            case 4: return 0.8660254037844386467637231707529361834714;
+            case 5: return 0.5000000000000000000000000000000000000000;
+            case 6: return 0.0000000000000000000000000000000000000000;
+            case 7: return -0.5000000000000000000000000000000000000000;
+            case 8: return -0.8660254037844386467637231707529361834714;
+            case 9: return -1.0000000000000000000000000000000000000000;
+            case 10: return -0.8660254037844386467637231707529361834714;
+            case 11: return -0.5000000000000000000000000000000000000000;
+        }
+        return 0.0;
+    }
+};
+template <> struct WConst<16> {
+    static __device__ __forceinline__ double c(int m) {
+        switch (m) {
+            case 0: return 1.0000000000000000000000000000000000000000;
+            case 1: return 0.9238795325112867561281831893967882868224;
+            case 2: return 0.7071067811865475244008443621048490392848;
+            case 3: return 0.3826834323650897717284599840303988667613;
+            case 4: return -0.0000000000000000000000000000000000000000;
+            case 5: return -0.3826834323650897717284599840303988667613;
+            case 6: return -0.7071067811865475244008443621048490392848;
+            case 7: return -0.9238795325112867561281831893967882868224;
+            case 8: return -1.0000000000000000000000000000000000000000;
+            case 9: return -0.9238795325112867561281831893967882868224;
+            case 10: return -0.7071067811865475244008443621048490392848;
+            case 11: return -0.3826834323650897717284599840303988667613;
+            case 12: return -0.0000000000000000000000000000000000000000;
+            case 13: return 0.3826834323650897717284599840303988667613;
+            case 14: return 0.7071067811865475244008443621048490392848;
+            case 15: return 0.9238795325112867561281831893967882868224;
+        }
+        return 0.0;
+    }
+    static __device__ __forceinline__ double s(int m) {
+        switch (m) {
+            case 0: return 0.0000000000000000000000000000000000000000;
+            case 1: return 0.3826834323650897717284599840303988667613;
+            case 2: return 0.7071067811865475244008443621048490392848;
+            case 3: return 0.9238795325112867561281831893967882868224;
+            case 4: return 1.0000000000000000000000000000000000000000;
+            case 5: return 0.9238795325112867561281831893967882868224;
+            case 6: return 0.7071067811865475244008443621048490392848;
+            case 7: return 0.3826834323650897717284599840303988667613;
+            case 8: return 0.0000000000000000000000000000000000000000;
+            case 9: return -0.3826834323650897717284599840303988667613;
+            case 10: return -0.7071067811865475244008443621048490392848;
+            case 11: return -0.9238795325112867561281831893967882868224;
+            case 12: return -1.0000000000000000000000000000000000000000;
+            case 13: return -0.9238795325112867561281831893967882868224;
+            case 14: return -0.7071067811865475244008443621048490392848;
+            case 15: return -0.3826834323650897717284599840303988667613;
+        }
+        return 0.0;
+    }
+};
+
+template <int R, int S, typename T>
+__device__ __forceinline__ void dft(cx<T>* v);
+
+// Composite N = N1*N2 codelet in registers (decimation in time):
+//   X[k1 + N1 k2] = sum_t W_N2^(t k2) [ W_N^(t k1) sum_j1 x[t + N2 j1] W_N1^(j1 k1) ].
+template <int N1, int N2, int S, typename T>
+__device__ __forceinline__ void dft_2f(cx<T>* v) {
+    constexpr int N = N1 * N2;
+    cx<T> y[N];
+#pragma unroll
+    for (int t = 0; t < N2; ++t) {
+        cx<T> u[N1];
+#pragma unroll
+        for (int j = 0; j < N1; ++j) u[j] = v[t + N2 * j];
+        dft<N1, S>(u);
+#pragma unroll
+        for (int k = 0; k < N1; ++k) {
+            const int m = (t * k) % N;
+            if (m == 0) {
+                y[k * N2 + t] = u[k];
+            } else {
+                const cx<T> w = mk(T(WConst<N>::c(m)), T(S * WConst<N>::s(m)));
+                y[k * N2 + t] = cmul(u[k], w);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < N1; ++k) {
+        cx<T> w2[N2];
+#pragma unroll
+        for (int t = 0; t < N2; ++t) w2[t] = y[k * N2 + t];
+        dft<N2, S>(w2);
+#pragma unroll
+        for (int q = 0; q < N2; ++q) v[k + N1 * q] = w2[q];
+    }
+}
+
 template <int R, int S, typename T>
 __device__ __forceinline__ void dft(cx<T>* v) {
     if constexpr (R == 2) dft2<S>(v);
     else if constexpr (R == 3) dft3<S>(v);
     else if constexpr (R == 4) dft4<S>(v);
     else if constexpr (R == 5) dft5<S>(v);
+    else if constexpr (R == 6) dft_2f<2, 3, S>(v);
+    else if constexpr (R == 10) dft_2f<2, 5, S>(v);
+    else if constexpr (R == 12) dft_2f<4, 3, S>(v);
+    else if constexpr (R == 16) dft_2f<4, 4, S>(v);
     else dft8<S>(v);
 }
+
+// Exact quotient j / d for j, d < 2^16 from m = floor(2^32 / d) + 1; d = 1 wraps m to 0,
+// which is taken to mean the identity.
+__device__ __forceinline__ int fdiv(int j, unsigned m) { return m ? (int)__umulhi((unsigned)j, m) : j; }
+__host__ __device__ inline unsigned fdiv_magic(int d) { return (unsigned)(0xFFFFFFFFu / (unsigned)d) + 1u; }
 
 // Radix schedule of one axis.  Passed by value as a kernel parameter.
 struct FftPlan {
     int n;
     int nst;
     int radix[16];
+    unsigned ns_magic[16];  // fdiv_magic(product of the radices before stage s)
 };
 
 // One Stockham stage over `lines` lines in column layout.
 template <int R, int S, typename T>
 __device__ __forceinline__ void stage(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst,
-                                      const cx<T>* __restrict__ tw, int n, int ns, int lines, int ld) {
+                                      const cx<T>* __restrict__ tw, int n, int ns, unsigned ns_m, int lines,
+                                      unsigned lines_m, int ld) {
     const int nb = n / R;
     const int total = nb * lines;
     const int twstep = n / (ns * R);
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
-        const int line = b % lines;
-        const int j = b / lines;
-        const int k = j % ns;
+        const int j = fdiv(b, lines_m);
+        const int line = b - j * lines;
+        const int k = j - fdiv(j, ns_m) * ns;
         cx<T> v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * ld + line];
@@ -163,7 +353,7 @@ __device__ __forceinline__ void stage(const cx<T>* __restrict__ src, cx<T>* __re
             }
         }
         dft<R, S>(v);
-        const int base = (j / ns) * ns * R + k;
+        const int base = (j - k) * R + k;
 #pragma unroll
         for (int r = 0; r < R; ++r) dst[(base + r * ns) * ld + line] = v[r];
     }
@@ -175,14 +365,20 @@ template <int S, typename T>
 __device__ cx<T>* fft_lines(cx<T>* a, cx<T>* b, const cx<T>* __restrict__ tw, const FftPlan& p,
                             int lines, int ld) {
     int ns = 1;
+    const unsigned lm = fdiv_magic(lines);
     for (int s = 0; s < p.nst; ++s) {
         const int R = p.radix[s];
+        const unsigned nm = p.ns_magic[s];
         switch (R) {
-            case 2: stage<2, S>(a, b, tw, p.n, ns, lines, ld); break;
-            case 3: stage<3, S>(a, b, tw, p.n, ns, lines, ld); break;
-            case 4: stage<4, S>(a, b, tw, p.n, ns, lines, ld); break;
-            case 5: stage<5, S>(a, b, tw, p.n, ns, lines, ld); break;
-            default: stage<8, S>(a, b, tw, p.n, ns, lines, ld); break;
+            case 2: stage<2, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            case 3: stage<3, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            case 4: stage<4, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            case 5: stage<5, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            case 6: stage<6, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            case 10: stage<10, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            case 12: stage<12, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            case 16: stage<16, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
+            default: stage<8, S>(a, b, tw, p.n, ns, nm, lines, lm, ld); break;
         }
         __syncthreads();
         cx<T>* t = a;
@@ -191,6 +387,156 @@ __device__ cx<T>* fft_lines(cx<T>* a, cx<T>* b, const cx<T>* __restrict__ tw, co
         ns *= R;
     }
     return a;
+}
+
+// ---------------------------------------------------------------------------------------
+// In-place variant: element (line, idx) at buf[line*ls + idx*is].  Within a stage every
+// thread first loads all of its butterflies' inputs into registers, the block synchronises,
+// and only then are outputs written, so a single buffer serves as both source and
+// destination.  Lines are processed in groups small enough that a group's elements fit in
+// VALS registers per thread.
+// ---------------------------------------------------------------------------------------
+template <int R, int S, int VALS, typename T>
+__device__ __forceinline__ void stage_ip(cx<T>* buf, const cx<T>* __restrict__ tw, int n, int ns, unsigned ns_m,
+                                         int l0, int lines, unsigned lines_m, int ls, int is) {
+    constexpr int B = (VALS + R - 1) / R;
+    const int nb = n / R;
+    const int total = nb * lines;
+    const int twstep = n / (ns * R);
+    cx<T> v[B][R];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int b = threadIdx.x + i * blockDim.x;
+        if (b < total) {
+            const int j = fdiv(b, lines_m);
+            const int line = b - j * lines;
+            const int k = j - fdiv(j, ns_m) * ns;
+            const cx<T>* base = buf + (l0 + line) * ls;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[i][r] = base[(j + r * nb) * is];
+            if (ns > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    cx<T> w = tw[r * k * twstep];
+                    v[i][r] = S < 0 ? cmul(v[i][r], w) : cmulc(v[i][r], w);
+                }
+            }
+            dft<R, S>(v[i]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int b = threadIdx.x + i * blockDim.x;
+        if (b < total) {
+            const int j = fdiv(b, lines_m);
+            const int line = b - j * lines;
+            const int k = j - fdiv(j, ns_m) * ns;
+            cx<T>* base = buf + (l0 + line) * ls;
+            const int o = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) base[(o + r * ns) * is] = v[i][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Transforms `lines` lines in place.  Requires blockDim.x * VALS >= n (one line per group
+// at least); the caller synchronises before the call.  Ends synchronised.
+template <int S, int VALS, typename T>
+__device__ __forceinline__ void fft_lines_ip(cx<T>* buf, const cx<T>* __restrict__ tw, const FftPlan& p,
+                                             int lines, int ls, int is) {
+    const int group = max(1, min(lines, (int)(blockDim.x * VALS) / p.n));
+    for (int l0 = 0; l0 < lines; l0 += group) {
+        const int cnt = min(group, lines - l0);
+        const unsigned lm = fdiv_magic(cnt);
+        int ns = 1;
+        for (int s = 0; s < p.nst; ++s) {
+            const int R = p.radix[s];
+            const unsigned nm = p.ns_magic[s];
+            switch (R) {
+                case 2: stage_ip<2, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                case 3: stage_ip<3, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                case 4: stage_ip<4, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                case 5: stage_ip<5, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                case 6: stage_ip<6, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                case 10: stage_ip<10, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                case 12: stage_ip<12, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                case 16: stage_ip<16, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+                default: stage_ip<8, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
+            }
+            ns *= R;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Compile-time stage chains for the in-place plane transforms: with the length N and every
+// radix known at compile time, each stage is straight-line code (divisions by constants),
+// and the kernel's register allocation is that of its largest single stage.
+// ---------------------------------------------------------------------------------------
+template <int R, int S, int VALS, int N, int NS, typename T>
+__device__ __forceinline__ void stage_ct(cx<T>* buf, const cx<T>* __restrict__ tw, int l0, int lines,
+                                         unsigned lines_m, int ls, int is) {
+    constexpr int B = (VALS + R - 1) / R;
+    constexpr int NB = N / R;
+    constexpr int TWSTEP = N / (NS * R);
+    const int total = NB * lines;
+    cx<T> v[B][R];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int b = threadIdx.x + i * blockDim.x;
+        if (b < total) {
+            const int j = fdiv(b, lines_m);
+            const int line = b - j * lines;
+            const int k = j % NS;
+            const cx<T>* base = buf + (l0 + line) * ls;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[i][r] = base[(j + r * NB) * is];
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    cx<T> w = tw[r * k * TWSTEP];
+                    v[i][r] = S < 0 ? cmul(v[i][r], w) : cmulc(v[i][r], w);
+                }
+            }
+            dft<R, S>(v[i]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int b = threadIdx.x + i * blockDim.x;
+        if (b < total) {
+            const int j = fdiv(b, lines_m);
+            const int line = b - j * lines;
+            const int k = j % NS;
+            cx<T>* base = buf + (l0 + line) * ls;
+            const int o = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) base[(o + r * NS) * is] = v[i][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int S, int VALS, int N, int NS, typename T, int R, int... Rest>
+__device__ __forceinline__ void chain_ct(cx<T>* buf, const cx<T>* __restrict__ tw, int l0, int lines,
+                                         unsigned lines_m, int ls, int is) {
+    stage_ct<R, S, VALS, N, NS>(buf, tw, l0, lines, lines_m, ls, is);
+    if constexpr (sizeof...(Rest) > 0) chain_ct<S, VALS, N, NS * R, T, Rest...>(buf, tw, l0, lines, lines_m, ls, is);
+}
+
+// All `lines` lines of length N = product(Rs), in place, in groups that fit VALS registers
+// per thread.  Caller synchronises before; ends synchronised.
+template <int S, int VALS, typename T, int... Rs>
+__device__ __forceinline__ void axis_ct(cx<T>* buf, const cx<T>* __restrict__ tw, int lines, int ls, int is) {
+    constexpr int N = (Rs * ...);
+    const int group = max(1, min(lines, (int)(blockDim.x * VALS) / N));
+    for (int l0 = 0; l0 < lines; l0 += group) {
+        const int cnt = min(group, lines - l0);
+        chain_ct<S, VALS, N, 1, T, Rs...>(buf, tw, l0, cnt, fdiv_magic(cnt), ls, is);
+    }
 }
 
 }  // namespace clk

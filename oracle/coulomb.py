@@ -122,13 +122,14 @@ def folded_kernel(ghat, dims, round_index):
     return ghat[np.ix_(fz, fy, fx)]
 
 
-def prepare(F, ghat):
+def prepare(F, ghat, rounds=range(8)):
     """V = aperiodic (G * F) on the N^3 grid by 8 phase-shifted rounds of N-point FFTs
-    -- CoulombCalculator.cpp:105-163.  F is a complex [z,y,x] array."""
+    -- CoulombCalculator.cpp:105-163.  F is a complex [z,y,x] array.  `rounds` restricts the
+    sum to some rounds kappa (the partial potentials of a multi-GPU split add up)."""
     nz, ny, nx = F.shape
     dims = (nx, ny, nz)
     V = np.zeros_like(F, dtype=np.complex128)
-    for rnd in range(8):
+    for rnd in rounds:
         ph = round_phase(dims, rnd)
         T = F * np.conj(ph)
         T = sfft.fftn(T, workers=-1)

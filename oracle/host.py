@@ -269,7 +269,7 @@ def load_state(path, n_atoms, n_orb, skip_lines):
 # --------------------------------------------------------------------------------------
 
 def compute_integrals(states, cells, dims, step, specs, dielectric=1.0, onsite=0.0,
-                      tf_lattice=None):
+                      tf_lattice=None, rounds=range(8)):
     """Runs the reference's plan loop (coulombo.cpp:186-209) with the FP64 real-space
     convolution.  states: list of [atom, orb] arrays in input order (holes first)."""
     n = len(states)
@@ -291,7 +291,7 @@ def compute_integrals(states, cells, dims, step, specs, dielectric=1.0, onsite=0
 
     for (sid, left, right) in plan:
         if left[0] != last_left:
-            V = C.prepare(density(left[0], False), ghat)
+            V = C.prepare(density(left[0], False), ghat, rounds)
             last_left = left[0]
         rconj = left[1] != right[1]
         if right[0] != last_right or rconj != last_rconj:

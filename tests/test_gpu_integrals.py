@@ -132,3 +132,47 @@ def test_compute_requires_states_and_kernel():
         assert e.value.kind == "state"
         with pytest.raises(cl.CoulomboError, match="outside the grid"):
             cc.set_states(np.ones((1, 2, 1), complex), np.array([0, 512]), 0)
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("env", [{"CL_NO_XY_FUSION": "1"}, {"CL_L2_CHUNK_MB": "0"}, {"CL_L2_CHUNK_MB": "4"}])
+def test_pass_variants_agree(mode, env, monkeypatch):
+    """The fused xy-plane passes, the separate x/y passes and every chunking of the densities
+    compute the same integrals."""
+    d = synth.build("c1", cells=(8, 8, 6))
+    step = (synth.A_ZB / 4,) * 3
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+
+    def run():
+        with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+            cc.initialize(dielectric=10.89)
+            cc.set_states(d["states"], d["cells_idx"], 2)
+            return cc.compute(specs)
+
+    base = run()
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    other = run()
+    tol = 1e-12 if mode == cl.MODE_FP64_PLAIN else 1e-6
+    assert np.abs(other - base).max() <= tol * np.abs(base).max()
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_round_split_adds_up(mode):
+    """cl_compute_rounds over disjoint round masks (the multi-GPU split) sums to cl_compute,
+    and matches the oracle's partial sums over the same rounds."""
+    from coulombo_lattice_b200 import multi
+    d = synth.build("c1", cells=(4, 4, 4))
+    step = (synth.A_ZB / 4,) * 3
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("eeee,hhhh,ehhe,eheh", 4, 2)]
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], 2)
+        full = cc.compute(specs)
+        parts = [cc.compute_rounds(specs, multi.round_mask(r, 3)) for r in range(3)]
+    tol = 1e-12 if mode == cl.MODE_FP64_PLAIN else 1e-6
+    assert np.abs(sum(parts) - full).max() <= tol * np.abs(full).max()
+    want0 = np.array(H.compute_integrals(list(d["states"]), d["cells_idx"], d["dims"], step, specs,
+                                         dielectric=10.89, rounds=[0, 3, 6]))
+    err, lim = gate(parts[0], want0, mode)
+    assert np.all(err <= np.maximum(lim, 1e-9 * np.abs(full).max()))
