@@ -221,10 +221,19 @@ PlaneTile plane_tile(int nx, int ny) {
     return PlaneTile{fits, ld, smem};
 }
 
-// Bytes of grids a chunk may hold so that consecutive passes meet in L2 (CL_L2_CHUNK_MB).
+// Density groups of the z pass: enough blocks to fill every SM several times over, while
+// each block still reuses its Khat tile for a run of densities.
+unsigned zgroups(long long zblocks, int cnt) {
+    const long long target = 148LL * 16;
+    long long g = (target + zblocks - 1) / zblocks;
+    return (unsigned)std::max(1LL, std::min<long long>(g, cnt));
+}
+
+// Bytes of grids a chunk may hold so that consecutive passes meet in L2 (CL_L2_CHUNK_MB;
+// off by default: measured on B200 it gave no gain at 96^3 over whole-request chunks).
 size_t l2_chunk_bytes() {
     const char* e = std::getenv("CL_L2_CHUNK_MB");
-    double mb = e ? std::atof(e) : 48.0;
+    double mb = e ? std::atof(e) : 0.0;
     return (size_t)(std::max(0.0, mb) * 1024 * 1024);
 }
 
@@ -476,8 +485,8 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
                 prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
             }
             e = prof_begin(c);
-            clk::k_zpass<T><<<(unsigned)zblocks, 256, zt.smem, c->stream>>>(buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W,
-                                                                             cnt, 0);
+            clk::k_zpass<T><<<dim3((unsigned)zblocks, zgroups(zblocks, cnt)), 256, zt.smem, c->stream>>>(
+                buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W, cnt, 0);
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
             if (!pt.fits) {

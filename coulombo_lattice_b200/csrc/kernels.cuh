@@ -62,7 +62,7 @@ struct KernelModel {
     double r_tf, q_tf;
 };
 
-__global__ void k_kernel_octant(double* __restrict__ G, int n1x, int n1y, int n1z, double sx, double sy,
+static __global__ void k_kernel_octant(double* __restrict__ G, int n1x, int n1y, int n1z, double sx, double sy,
                                 double sz, KernelModel km) {
     const long long total = (long long)n1x * n1y * n1z;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
@@ -88,7 +88,7 @@ __global__ void k_kernel_octant(double* __restrict__ G, int n1x, int n1y, int n1
 // Line l = (o, i) has element j at (o*L + j)*inner + i.  A block handles `nl` consecutive
 // lines staged in shared memory; ctab[t] = cos(pi t / (L-1)), t < 2(L-1).
 // ---------------------------------------------------------------------------------------
-__global__ void k_dct1(const double* __restrict__ in, double* __restrict__ out, int L, long long inner,
+static __global__ void k_dct1(const double* __restrict__ in, double* __restrict__ out, int L, long long inner,
                        long long nlines, int nl, const double* __restrict__ ctab) {
     extern __shared__ double dsm[];
     const int np = L - 1;  // N'
@@ -150,7 +150,7 @@ __global__ void k_khat(const double* __restrict__ ghat, int nx, int ny, int nz, 
 // Pair densities at atoms: rho_p(a) = sum_o conj(c_fl[a][o]) c_fr[a][o]  (Product.cpp:16-30).
 // coeff is [state][atom][orb] in input atom order; orig maps sorted -> input atom.
 // ---------------------------------------------------------------------------------------
-__global__ void k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb,
+static __global__ void k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb,
                                const int* __restrict__ orig, long long n_sorted,
                                const int2* __restrict__ prods, cx<double>* __restrict__ rho) {
     const int p = blockIdx.y;
@@ -285,7 +285,10 @@ __global__ void __launch_bounds__(256) k_zpass(cx<T>* __restrict__ buf, long lon
             kt[e] = l < w ? khat[(long long)z * nxy + c0 + l] : T(0);
         }
     }
-    for (int p = 0; p < np; ++p) {
+    // densities of this block: gridDim.y groups share the np densities
+    const int per = (np + gridDim.y - 1) / gridDim.y;
+    const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
+    for (int p = p_begin; p < p_end; ++p) {
         cx<T>* base = buf + (long long)p * stride + c0;
         for (int e = threadIdx.x; e < nz * W; e += blockDim.x) {
             const int z = e / W, l = e - z * W;
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(512, 1) k_xyinv(const cx<T>* __restrict__ buf,
 // 64x64 (l, r) tiles, 4x4 per thread, atoms staged 16 at a time; split over atoms with one
 // FP64 atomicAdd per result per block.
 // ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_gram(const cx<double>* __restrict__ V, long long v_stride, int nl,
+static __global__ void __launch_bounds__(256) k_gram(const cx<double>* __restrict__ V, long long v_stride, int nl,
                                              const cx<double>* __restrict__ rho, long long r_stride,
                                              const int* __restrict__ ridx, int nr, long long n_atoms,
                                              long long atoms_per_split, double* __restrict__ out) {
