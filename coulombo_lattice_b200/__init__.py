@@ -62,6 +62,7 @@ SIGNATURES = [
     ("cl_set_profiling", _i, [_vp, _i]),
     ("cl_kernel_profile", _i, [_vp, _P(_d), _P(_i64), _P(_d)]),
     ("cl_fft3d", _i, [_i, _i, _i, _i, _i, _i, _P(_d)]),
+    ("cl_fft3d_noalloc", _i, [_i, _i, _i, _i, _i, _vp]),
     ("cl_round_up_235", _i, [_i, _i]),
     ("cl_detect_grid", _i, [_P(_d), _i64, _P(_i), _P(_i), _P(_d), _P(_d), _P(_i64)]),
     ("cl_enumerate_integrals", _i, [ctypes.c_char_p, _i, _i, _P(_i64), _P(ctypes.c_int16), _i64]),
@@ -151,6 +152,13 @@ def fft3d(data, sign=-1, fp32=False):
     batch = int(np.prod(a.shape[:-3])) if a.ndim > 3 else 1
     _check(lib().cl_fft3d(nx, ny, nz, batch, int(sign), int(bool(fp32)), _ptr(a.view(np.float64))))
     return a
+
+
+def fft3d_noalloc_device(ptr, dims, batch=1, sign=-1):
+    """cl_fft3d_noalloc on a caller-owned device buffer at address `ptr` (complex128,
+    [batch, nz, ny, nx]), in place; the library allocates no device memory for it."""
+    nx, ny, nz = dims
+    _check(lib().cl_fft3d_noalloc(int(nx), int(ny), int(nz), int(batch), int(sign), ctypes.c_void_p(int(ptr))))
 
 
 # ----------------------------------------------------------------------------------------

@@ -150,6 +150,18 @@ int cl_kernel_profile(cl_ctx* ctx, double ms[CL_NUM_KCLASS], int64_t launches[CL
  * src/CoulombCalculator.cpp:17-32. */
 int cl_fft3d(int nx, int ny, int nz, int batch, int sign, int fp32, double* data);
 
+/* Allocation-free variant of cl_fft3d for callers that cannot call cudaMalloc (those whose
+ * pool or arena owns all device memory, or whose latency-critical path must not let an
+ * allocation synchronise the device).  No counterpart in the reference: it exists for this
+ * library's callers.  `data` is a DEVICE pointer to batch*nx*ny*nz complex doubles,
+ * 16-byte aligned, transformed in place on the legacy default stream; the call returns
+ * after the transform has finished.  It allocates nothing: the twiddle tables live in a
+ * fixed 192 KiB array inside the library (held by every GPU that loads it until exit), so
+ * each axis is limited to 4096 points and longer axes are rejected.  The first call on a
+ * device looks up that array's device address; make it before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race. */
+int cl_fft3d_noalloc(int nx, int ny, int nz, int batch, int sign, double* data);
+
 /* ---------------------------------------------------------------------------------------
  * Host-side helpers (no GPU needed)
  * ------------------------------------------------------------------------------------- */
