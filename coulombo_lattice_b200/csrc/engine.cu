@@ -15,6 +15,7 @@
 #include "host/host_logic.hpp"
 #include "host/status.hpp"
 #include "kernels.cuh"
+#include "rfft.cuh"
 
 using clk::cx;
 using clk::FftPlan;
@@ -403,6 +404,42 @@ void transform_kernel(cl_ctx* c) {
     c->kernel_ready = true;
 }
 
+// Register two-factor column passes (rfft.cuh) where the length has a compiled split; these
+// return false (nothing launched) otherwise.  CL_NO_REGISTER_FFT forces the generic passes.
+template <typename T>
+bool launch_zconv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const T* kh, long long nxy, int nz, int cnt) {
+    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
+    constexpr int L = sizeof(T) == 4 ? 16 : 8;
+    return clk::with_split2(nz, [&](auto tag) {
+        using Tag = decltype(tag);
+        constexpr int N = Tag::r1 * Tag::r2;
+        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
+        auto kern = clk::k_zconv_rf<T, Tag::r1, Tag::r2, L>;
+        const size_t smem = sizeof(cx<T>) * ((size_t)N + 2ull * N * L);
+        ensure_smem(kern, smem);
+        const long long blocks = (nxy + L - 1) / L;
+        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), L * Q, smem, c->stream>>>(buf, c->M, tw, kh, nxy, cnt);
+    });
+}
+
+template <int S, typename T>
+bool launch_ycol_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, int nx, int ny, int nz, int cnt) {
+    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
+    constexpr int L = sizeof(T) == 4 ? 16 : 8;
+    return clk::with_split2(ny, [&](auto tag) {
+        using Tag = decltype(tag);
+        constexpr int N = Tag::r1 * Tag::r2;
+        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
+        auto kern = clk::k_ycol_rf<S, T, Tag::r1, Tag::r2, L>;
+        const size_t smem = sizeof(cx<T>) * ((size_t)N + (size_t)N * L);
+        ensure_smem(kern, smem);
+        const int xchunks = (nx + L - 1) / L;
+        const long long blocks = (long long)xchunks * nz;
+        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), L * Q, smem, c->stream>>>(buf, c->M, tw, nx, ny, xchunks,
+                                                                                        cnt);
+    });
+}
+
 // Number of atoms listed by a row CSR (host-side copy kept with the CSR).
 long long row_ptr_count(cl_ctx* c, const int* row_ptr) {
     return row_ptr == c->row_ptr.p ? c->n_sorted : c->M;
@@ -479,20 +516,23 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
             prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * 16.0 + gbytes) + atoms * 4.0);
             if (!pt.fits) {
                 e = prof_begin(c);
-                clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx,
-                                                                                          ny, yt.W, ychunks);
+                if (!launch_ycol_rf<-1, T>(c, buf, twy, nx, ny, nz, cnt))
+                    clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy,
+                                                                                              nx, ny, yt.W, ychunks);
                 CL_LAUNCHED();
                 prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
             }
             e = prof_begin(c);
-            clk::k_zpass<T><<<dim3((unsigned)zblocks, zgroups(zblocks, cnt)), 256, zt.smem, c->stream>>>(
-                buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W, cnt, 0);
+            if (!launch_zconv_rf<T>(c, buf, twz, kh, nxy, nz, cnt))
+                clk::k_zpass<T><<<dim3((unsigned)zblocks, zgroups(zblocks, cnt)), 256, zt.smem, c->stream>>>(
+                    buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W, cnt, 0);
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
             if (!pt.fits) {
                 e = prof_begin(c);
-                clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy, nx,
-                                                                                          ny, yt.W, ychunks);
+                if (!launch_ycol_rf<+1, T>(c, buf, twy, nx, ny, nz, cnt))
+                    clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy,
+                                                                                              nx, ny, yt.W, ychunks);
                 CL_LAUNCHED();
                 prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
             }

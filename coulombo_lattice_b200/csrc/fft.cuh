@@ -267,6 +267,78 @@ template <> struct WConst<16> {
     }
 };
 
+template <> struct WConst<9> {
+    static __device__ __forceinline__ double c(int m) {
+        switch (m) {
+            case 0: return 1.0000000000000000000000000000000000000000;
+            case 1: return 0.7660444431189780352023926505554166739358;
+            case 2: return 0.1736481776669303488517166267693147960004;
+            case 3: return -0.5000000000000000000000000000000000000000;
+            case 4: return -0.9396926207859083840541092773247314699362;
+            case 5: return -0.9396926207859083840541092773247314699362;
+            case 6: return -0.5000000000000000000000000000000000000000;
+            case 7: return 0.1736481776669303488517166267693147960004;
+            case 8: return 0.7660444431189780352023926505554166739358;
+        }
+        return 0.0;
+    }
+    static __device__ __forceinline__ double s(int m) {
+        switch (m) {
+            case 0: return 0.0000000000000000000000000000000000000000;
+            case 1: return 0.6427876096865393263226434099072634329076;
+            case 2: return 0.9848077530122080593667430245895230136706;
+            case 3: return 0.8660254037844386467637231707529361834714;
+            case 4: return 0.3420201433256687330440996146822595807631;
+            case 5: return -0.3420201433256687330440996146822595807631;
+            case 6: return -0.8660254037844386467637231707529361834714;
+            case 7: return -0.9848077530122080593667430245895230136706;
+            case 8: return -0.6427876096865393263226434099072634329076;
+        }
+        return 0.0;
+    }
+};
+template <> struct WConst<15> {
+    static __device__ __forceinline__ double c(int m) {
+        switch (m) {
+            case 0: return 1.0000000000000000000000000000000000000000;
+            case 1: return 0.9135454576426008955021275719853171779408;
+            case 2: return 0.6691306063588582138262733306867804735996;
+            case 3: return 0.3090169943749474241022934171828190588602;
+            case 4: return -0.1045284632676534713998341548024981190807;
+            case 5: return -0.5000000000000000000000000000000000000000;
+            case 6: return -0.8090169943749474241022934171828190588602;
+            case 7: return -0.9781476007338056379285667478695995324597;
+            case 8: return -0.9781476007338056379285667478695995324597;
+            case 9: return -0.8090169943749474241022934171828190588602;
+            case 10: return -0.5000000000000000000000000000000000000000;
+            case 11: return -0.1045284632676534713998341548024981190807;
+            case 12: return 0.3090169943749474241022934171828190588602;
+            case 13: return 0.6691306063588582138262733306867804735996;
+            case 14: return 0.9135454576426008955021275719853171779408;
+        }
+        return 0.0;
+    }
+    static __device__ __forceinline__ double s(int m) {
+        switch (m) {
+            case 0: return 0.0000000000000000000000000000000000000000;
+            case 1: return 0.4067366430758002077539859903414976129231;
+            case 2: return 0.7431448254773942350146970489742569771891;
+            case 3: return 0.9510565162951535721164393333793821434057;
+            case 4: return 0.9945218953682733369226919449805703815208;
+            case 5: return 0.8660254037844386467637231707529361834714;
+            case 6: return 0.5877852522924731291687059546390727685977;
+            case 7: return 0.2079116908177593371017422844051251662166;
+            case 8: return -0.2079116908177593371017422844051251662166;
+            case 9: return -0.5877852522924731291687059546390727685977;
+            case 10: return -0.8660254037844386467637231707529361834714;
+            case 11: return -0.9945218953682733369226919449805703815208;
+            case 12: return -0.9510565162951535721164393333793821434057;
+            case 13: return -0.7431448254773942350146970489742569771891;
+            case 14: return -0.4067366430758002077539859903414976129231;
+        }
+        return 0.0;
+    }
+};
 template <int R, int S, typename T>
 __device__ __forceinline__ void dft(cx<T>* v);
 
@@ -311,6 +383,8 @@ __device__ __forceinline__ void dft(cx<T>* v) {
     else if constexpr (R == 4) dft4<S>(v);
     else if constexpr (R == 5) dft5<S>(v);
     else if constexpr (R == 6) dft_2f<2, 3, S>(v);
+    else if constexpr (R == 9) dft_2f<3, 3, S>(v);
+    else if constexpr (R == 15) dft_2f<3, 5, S>(v);
     else if constexpr (R == 10) dft_2f<2, 5, S>(v);
     else if constexpr (R == 12) dft_2f<4, 3, S>(v);
     else if constexpr (R == 16) dft_2f<4, 4, S>(v);

@@ -81,3 +81,26 @@ def test_state_errors():
         assert e.value.kind == "state"
         with pytest.raises(cl.CoulomboError, match="Thomas-Fermi"):
             cc.initialize(1.0, tf_lattice=5.0)
+
+
+# y and z lengths covering the compiled two-factor splits of the register column passes
+# (x kept small); the generic passes handle the rest.
+SPLIT_SHAPES = [(8, 256, 8), (8, 8, 256), (6, 96, 128), (4, 160, 144), (4, 240, 180), (2, 225, 135),
+                (4, 192, 150), (4, 120, 108), (4, 100, 90), (8, 81, 75), (8, 72, 64), (8, 60, 54),
+                (8, 50, 48), (8, 45, 40), (8, 36, 32), (8, 30, 27), (8, 25, 24), (8, 20, 16)]
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("dims", SPLIT_SHAPES)
+def test_register_column_passes_match_oracle(mode, dims):
+    nx, ny, nz = dims
+    rng = np.random.default_rng(nx + 7 * ny + 13 * nz)
+    F = rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx))
+    step = (1.4, 1.1, 0.8)
+    ghat = C.kernel_spectrum(C.kernel_octant(dims, step, dielectric=3.0), dims)
+    V = C.prepare(F, ghat)
+    with cl.CoulombCalculator(dims, step, mode) as cc:
+        cc.initialize(dielectric=3.0)
+        cc.prepare(F)
+        Vg = cc.potential()
+    assert np.abs(Vg - V).max() <= TOL[mode] * 10 * np.abs(V).max()
