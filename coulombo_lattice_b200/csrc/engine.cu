@@ -217,8 +217,10 @@ template <typename T>
 PlaneTile plane_tile(int nx, int ny) {
     const int ld = (nx % 2 == 0) ? nx + 1 : nx;
     const size_t smem = sizeof(cx<T>) * ((size_t)nx + ny + (size_t)ny * ld);
+    // Off unless CL_XY_FUSION is set: measured on B200 at 96^3, the register row/column passes
+    // (two HBM sweeps more) run 1.5x faster than this whole-plane kernel.
     const bool fits = smem <= 220 * 1024 && clk::plane_size_supported(nx) && clk::plane_size_supported(ny) &&
-                      !std::getenv("CL_NO_XY_FUSION");
+                      std::getenv("CL_XY_FUSION") != nullptr;
     return PlaneTile{fits, ld, smem};
 }
 
@@ -274,6 +276,7 @@ struct cl_ctx {
     long long n_atoms = 0, n_sorted = 0;
     DevBuf<cx<double>> coeff;
     DevBuf<int> cell_sorted, orig_sorted, row_ptr;
+    long long live_rows = 0;           // rows (y, z) holding at least one atom
     std::vector<long long> atom_slot;  // input atom -> sorted (deduplicated) slot
 
     // work buffers
@@ -423,7 +426,7 @@ bool launch_zconv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const T* kh, long l
 }
 
 template <int S, typename T>
-bool launch_ycol_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, int nx, int ny, int nz, int cnt) {
+bool launch_ycol_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, int nx, int ny, int nz, int cnt, const int* row_ptr) {
     if (std::getenv("CL_NO_REGISTER_FFT")) return false;
     constexpr int L = sizeof(T) == 4 ? 16 : 8;
     return clk::with_split2(ny, [&](auto tag) {
@@ -436,7 +439,44 @@ bool launch_ycol_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, int nx, int ny, int 
         const int xchunks = (nx + L - 1) / L;
         const long long blocks = (long long)xchunks * nz;
         kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), L * Q, smem, c->stream>>>(buf, c->M, tw, nx, ny, xchunks,
-                                                                                        cnt);
+                                                                                        cnt, row_ptr);
+    });
+}
+
+template <typename T>
+bool launch_xfwd_rf(cl_ctx* c, const cx<double>* rho, long long rho_stride, const int* row_ptr, const int* cell,
+                    cx<T>* buf, const cx<T>* tw, const clk::RoundPhase& rp, int nx, int ny, int nrows, int cnt,
+                    int skip_empty) {
+    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
+    constexpr int LR = sizeof(T) == 4 ? 16 : 8;
+    return clk::with_split2(nx, [&](auto tag) {
+        using Tag = decltype(tag);
+        constexpr int N = Tag::r1 * Tag::r2;
+        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
+        auto kern = clk::k_xfwd_rf<T, Tag::r1, Tag::r2, LR>;
+        const size_t smem = sizeof(cx<T>) * ((size_t)N + 2ull * N * (LR + 1));
+        ensure_smem(kern, smem);
+        const long long blocks = (nrows + LR - 1) / LR;
+        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), LR * Q, smem, c->stream>>>(
+            rho, rho_stride, row_ptr, cell, buf, c->M, tw, rp, ny, nrows, cnt, skip_empty);
+    });
+}
+
+template <typename T>
+bool launch_xinv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const clk::RoundPhase& rp, const int* row_ptr,
+                    const int* cell, cx<double>* V, long long v_stride, int nx, int ny, int nrows, int cnt) {
+    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
+    constexpr int LR = sizeof(T) == 4 ? 16 : 8;
+    return clk::with_split2(nx, [&](auto tag) {
+        using Tag = decltype(tag);
+        constexpr int N = Tag::r1 * Tag::r2;
+        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
+        auto kern = clk::k_xinv_rf<T, Tag::r1, Tag::r2, LR>;
+        const size_t smem = sizeof(cx<T>) * ((size_t)N + 3ull * N * (LR + 1));
+        ensure_smem(kern, smem);
+        const long long blocks = (nrows + LR - 1) / LR;
+        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), LR * Q, smem, c->stream>>>(
+            buf, c->M, tw, rp, row_ptr, cell, V, v_stride, ny, nrows, cnt);
     });
 }
 
@@ -490,10 +530,18 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     const int xblocks = (nrows + xt.rows - 1) / xt.rows;
     const int ychunks = (nx + yt.W - 1) / yt.W;
     const long long zblocks = (nxy + zt.W - 1) / zt.W;
+    // Rows without atoms are skipped (not stored / not loaded) when the x and y passes are both
+    // the register ones, which agree on it; CL_NO_ROW_SKIP turns it off.
+    const bool reg_x = !std::getenv("CL_NO_REGISTER_FFT") && clk::with_split2(nx, [](auto) {});
+    const bool reg_y = !std::getenv("CL_NO_REGISTER_FFT") && clk::with_split2(ny, [](auto) {});
+    const int skip_empty = (!pt.fits && reg_x && reg_y && !std::getenv("CL_NO_ROW_SKIP")) ? 1 : 0;
 
-    // algorithmic bytes per density of each pass (minimum HBM traffic of its work)
+    // algorithmic bytes per density of each pass (minimum HBM traffic of its work); with
+    // skipped rows only the live fraction of a row-side sweep counts
     const double gbytes = (double)grid_bytes;
     const double atoms = (double)(row_ptr_count(c, row_ptr));
+    const double live = (skip_empty && row_ptr == c->row_ptr.p) ? (double)c->live_rows / nrows : 1.0;
+    const double row_side = (row_ptr == c->row_ptr.p) ? (double)c->live_rows / nrows : 1.0;
     for (int p0 = 0; p0 < np; p0 += chunk) {
         const int cnt = std::min(chunk, np - p0);
         const cx<double>* rho_c = rho + (long long)p0 * rho_stride;
@@ -507,20 +555,21 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
             if (pt.fits) {
                 clk::k_xyfwd<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
                     rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan, Y.plan, twx, twy, rp, nx, ny, pt.ld);
-            } else {
+            } else if (!launch_xfwd_rf<T>(c, rho_c, rho_stride, row_ptr, cell, buf, twx, rp, nx, ny, nrows, cnt,
+                                          skip_empty)) {
                 clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, c->M,
                                                                      X.plan, twx, rp, nx, ny, nrows, xt.rows, xt.ld,
                                                                      cnt);
             }
             CL_LAUNCHED();
-            prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * 16.0 + gbytes) + atoms * 4.0);
+            prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * 16.0 + live * gbytes) + atoms * 4.0);
             if (!pt.fits) {
                 e = prof_begin(c);
-                if (!launch_ycol_rf<-1, T>(c, buf, twy, nx, ny, nz, cnt))
+                if (!launch_ycol_rf<-1, T>(c, buf, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr))
                     clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy,
                                                                                               nx, ny, yt.W, ychunks);
                 CL_LAUNCHED();
-                prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
+                prof_end(c, e, CL_KCLASS_YPASS, cnt * (1.0 + live) * gbytes);
             }
             e = prof_begin(c);
             if (!launch_zconv_rf<T>(c, buf, twz, kh, nxy, nz, cnt))
@@ -530,22 +579,22 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
             prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
             if (!pt.fits) {
                 e = prof_begin(c);
-                if (!launch_ycol_rf<+1, T>(c, buf, twy, nx, ny, nz, cnt))
+                if (!launch_ycol_rf<+1, T>(c, buf, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr))
                     clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy,
                                                                                               nx, ny, yt.W, ychunks);
                 CL_LAUNCHED();
-                prof_end(c, e, CL_KCLASS_YPASS, cnt * 2.0 * gbytes);
+                prof_end(c, e, CL_KCLASS_YPASS, cnt * (1.0 + live) * gbytes);
             }
             e = prof_begin(c);
             if (pt.fits) {
                 clk::k_xyinv<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
                     buf, c->M, X.plan, Y.plan, twx, twy, rp, row_ptr, cell, V_c, v_stride, nx, ny, pt.ld);
-            } else {
+            } else if (!launch_xinv_rf<T>(c, buf, twx, rp, row_ptr, cell, V_c, v_stride, nx, ny, nrows, cnt)) {
                 clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, rp, row_ptr, cell, V_c,
                                                                      v_stride, nx, ny, nrows, xt.rows, xt.ld, cnt);
             }
             CL_LAUNCHED();
-            prof_end(c, e, CL_KCLASS_XINV, cnt * (gbytes + atoms * 32.0) + atoms * 4.0);
+            prof_end(c, e, CL_KCLASS_XINV, cnt * (row_side * gbytes + atoms * 32.0) + atoms * 4.0);
         }
     }
 }
@@ -558,12 +607,21 @@ void run_rounds_mode(cl_ctx* c, const cx<double>* rho, long long rho_stride, int
         run_rounds<float>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride, round_mask);
 }
 
-// out4[l][r] = {sum ac, bd, ad, bc} over atoms (see k_gram).
+// out4[l][r] = {sum ac, bd, ad, bc} over atoms (see k_gram).  The register block IB (tile
+// 16*IB) is the one that pads max(nl, nr) least, preferring larger blocks.
 void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<double>* rho, long long r_stride,
           const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
     CL_CUDA(cudaMemsetAsync(out4_dev, 0, sizeof(double) * 4 * (size_t)nl * nr, c->stream));
-    const int tl = (nl + 63) / 64, tr = (nr + 63) / 64;
-    long long want = std::max(1LL, (148LL * 2) / std::max(1, tl * tr));
+    const int pmax = std::max(nl, nr);
+    int ib = 4;
+    long long best = -1;
+    for (int cand = 4; cand >= 1; --cand) {
+        const long long ts = 16 * cand, padded = (pmax + ts - 1) / ts * ts;
+        if (best < 0 || padded < best) { best = padded; ib = cand; }
+    }
+    const int ts = 16 * ib;
+    const int tl = (nl + ts - 1) / ts, tr = (nr + ts - 1) / ts;
+    long long want = std::max(1LL, (148LL * 4) / std::max(1, tl * tr));
     long long per = std::max(256LL, (n_atoms + want - 1) / want);
     per = (per + 15) / 16 * 16;
     long long splits = std::max(1LL, (n_atoms + per - 1) / per);
@@ -572,10 +630,46 @@ void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<d
         per = ((n_atoms + splits - 1) / splits + 15) / 16 * 16;
     }
     cudaEvent_t e = prof_begin(c);
-    clk::k_gram<<<dim3(tl, tr, (unsigned)splits), 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr,
-                                                                        n_atoms, per, out4_dev);
+    const dim3 grid(tl, tr, (unsigned)splits);
+    switch (ib) {
+        case 1: clk::k_gram<1><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+        case 2: clk::k_gram<2><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+        case 3: clk::k_gram<3><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+        default: clk::k_gram<4><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+    }
     CL_LAUNCHED();
     prof_end(c, e, CL_KCLASS_GRAM, (double)(nl + nr) * n_atoms * 16.0);
+}
+
+// Pair densities rho[p][atom] for products (fl[p], fr[p]) (0-based state indices).
+void pair_densities(cl_ctx* c, const std::vector<int2>& fl, cx<double>* rho) {
+    const int np = (int)fl.size();
+    std::vector<int> used;
+    std::vector<int> where(c->n_states, -1);
+    for (const auto& f : fl)
+        for (int s : {f.x, f.y})
+            if (where[s] < 0) { where[s] = (int)used.size(); used.push_back(s); }
+    std::vector<int2> local(np);
+    for (int p = 0; p < np; ++p) local[p] = make_int2(where[fl[p].x], where[fl[p].y]);
+    DevBuf<int2> dprods;
+    dprods.upload(local.data(), local.size(), c->stream);
+    DevBuf<int> dstates;
+    dstates.upload(used.data(), used.size(), c->stream);
+    const int os = c->n_orb | 1;
+    const size_t per_atom = sizeof(cx<double>) * (size_t)used.size() * os;
+    int chunk = (int)std::max<size_t>(1, std::min<size_t>(64, (96 * 1024) / per_atom));
+    const size_t smem = per_atom * chunk;
+    ensure_smem(clk::k_pair_density, smem);
+    const long long chunks = (c->n_sorted + chunk - 1) / chunk;
+    const int blocks = (int)std::min<long long>(chunks, 148LL * 8);
+    cudaEvent_t e = prof_begin(c);
+    clk::k_pair_density<<<blocks, 256, smem, c->stream>>>(c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p,
+                                                         c->n_sorted, dprods.p, np, dstates.p, (int)used.size(),
+                                                         chunk, rho);
+    CL_LAUNCHED();
+    prof_end(c, e, CL_KCLASS_DENSITY,
+             (double)used.size() * c->n_atoms * c->n_orb * 16.0 + (double)np * c->n_sorted * 16.0);
+    CL_CUDA(cudaStreamSynchronize(c->stream));  // device lists go out of scope
 }
 
 void check_ctx(cl_ctx* c) {
@@ -777,6 +871,9 @@ int cl_set_states(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_o
         std::vector<int> rp((size_t)nrows + 1, 0);
         for (int cs : cell_s) rp[cs / nx + 1]++;
         for (int r = 0; r < nrows; ++r) rp[r + 1] += rp[r];
+        long long live = 0;
+        for (int r = 0; r < nrows; ++r) live += rp[r + 1] > rp[r];
+        c->live_rows = live;
         c->n_states = n_states;
         c->n_holes = n_holes;
         c->n_orb = n_orb;
@@ -829,8 +926,6 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
             fl[i] = make_int2(a - 1, b - 1);
         }
         const long long As = c->n_sorted;
-        DevBuf<int2> dprods;
-        dprods.upload(fl.data(), fl.size(), c->stream);
         DevBuf<int> dr;
         dr.upload(rights.data(), rights.size(), c->stream);
         DevBuf<cx<double>> rho, V;
@@ -839,11 +934,7 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         DevBuf<double> o4;
         o4.alloc((size_t)4 * nl * nr);
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
-        cudaEvent_t pe = prof_begin(c);
-        clk::k_pair_density<<<dim3(grid_for(As), nu), 256, 0, c->stream>>>(
-            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, As, dprods.p, rho.p);
-        CL_LAUNCHED();
-        prof_end(c, pe, CL_KCLASS_DENSITY, (double)c->n_states * c->n_atoms * c->n_orb * 16.0 + (double)nu * As * 16.0);
+        pair_densities(c, fl, rho.p);
         CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)nl * As, c->stream));
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
         run_rounds_mode(c, rho.p, As, nl, c->row_ptr.p, c->cell_sorted.p, V.p, As, round_mask);
@@ -935,15 +1026,11 @@ int cl_potentials(cl_ctx* c, double* out) {
         const long long As = c->n_sorted;
         std::vector<int2> fl(n);
         for (int s = 0; s < n; ++s) fl[s] = make_int2(s, s);
-        DevBuf<int2> dprods;
-        dprods.upload(fl.data(), fl.size(), c->stream);
         DevBuf<cx<double>> rho, V;
         rho.alloc((size_t)n * As);
         V.alloc((size_t)n * As);
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
-        clk::k_pair_density<<<dim3(grid_for(As), n), 256, 0, c->stream>>>(c->coeff.p, c->n_atoms, c->n_orb,
-                                                                          c->orig_sorted.p, As, dprods.p, rho.p);
-        CL_LAUNCHED();
+        pair_densities(c, fl, rho.p);
         CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)n * As, c->stream));
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
         run_rounds_mode(c, rho.p, As, n, c->row_ptr.p, c->cell_sorted.p, V.p, As);

@@ -150,22 +150,40 @@ __global__ void k_khat(const double* __restrict__ ghat, int nx, int ny, int nz, 
 // Pair densities at atoms: rho_p(a) = sum_o conj(c_fl[a][o]) c_fr[a][o]  (Product.cpp:16-30).
 // coeff is [state][atom][orb] in input atom order; orig maps sorted -> input atom.
 // ---------------------------------------------------------------------------------------
-static __global__ void k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb,
-                               const int* __restrict__ orig, long long n_sorted,
-                               const int2* __restrict__ prods, cx<double>* __restrict__ rho) {
-    const int p = blockIdx.y;
-    const int2 f = prods[p];
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_sorted;
-         i += (long long)gridDim.x * blockDim.x) {
-        const long long a = orig[i];
-        const cx<double>* L = coeff + ((long long)f.x * n_atoms + a) * n_orb;
-        const cx<double>* R = coeff + ((long long)f.y * n_atoms + a) * n_orb;
-        cx<double> s = mk(0.0, 0.0);
-        for (int k = 0; k < n_orb; ++k) {
-            const cx<double> l = L[k], r = R[k];
-            s = s + mk(l.re * r.re + l.im * r.im, l.re * r.im - l.im * r.re);
+static __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms,
+                                                           int n_orb, const int* __restrict__ orig, long long n_sorted,
+                                                           const int2* __restrict__ prods, int n_prods,
+                                                           const int* __restrict__ states, int n_used, int chunk,
+                                                           cx<double>* __restrict__ rho) {
+    // A block stages the coefficients of `chunk` consecutive (cell-sorted) atoms for every
+    // used state in shared memory -- each coefficient is read from HBM once -- then forms every
+    // product of the chunk.  Atom pitch `os` is odd (in 16-byte units), so threads on
+    // consecutive atoms hit distinct banks.
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<double>* sc = reinterpret_cast<cx<double>*>(smem_raw);
+    const int os = n_orb | 1;
+    for (long long i0 = (long long)blockIdx.x * chunk; i0 < n_sorted; i0 += (long long)gridDim.x * chunk) {
+        const int ca = (int)min((long long)chunk, n_sorted - i0);
+        const int per_state = ca * n_orb;
+        for (int e = threadIdx.x; e < n_used * per_state; e += blockDim.x) {
+            const int su = e / per_state, rem = e - su * per_state;
+            const int a = rem / n_orb, k = rem - a * n_orb;
+            sc[(su * chunk + a) * os + k] = coeff[((long long)states[su] * n_atoms + orig[i0 + a]) * n_orb + k];
         }
-        rho[(long long)p * n_sorted + i] = s;
+        __syncthreads();
+        for (int e = threadIdx.x; e < n_prods * ca; e += blockDim.x) {
+            const int p = e / ca, a = e - p * ca;
+            const int2 f = prods[p];  // indices into the used-state list
+            const cx<double>* L = sc + (f.x * chunk + a) * os;
+            const cx<double>* R = sc + (f.y * chunk + a) * os;
+            cx<double> acc = mk(0.0, 0.0);
+            for (int k = 0; k < n_orb; ++k) {
+                const cx<double> l = L[k], r = R[k];
+                acc = acc + mk(l.re * r.re + l.im * r.im, l.re * r.im - l.im * r.re);
+            }
+            rho[(long long)p * n_sorted + i0 + a] = acc;
+        }
+        __syncthreads();
     }
 }
 
@@ -440,25 +458,29 @@ __global__ void __launch_bounds__(512, 1) k_xyinv(const cx<T>* __restrict__ buf,
 // 64x64 (l, r) tiles, 4x4 per thread, atoms staged 16 at a time; split over atoms with one
 // FP64 atomicAdd per result per block.
 // ---------------------------------------------------------------------------------------
-static __global__ void __launch_bounds__(256) k_gram(const cx<double>* __restrict__ V, long long v_stride, int nl,
+template <int IB>
+__global__ void __launch_bounds__(256) k_gram(const cx<double>* __restrict__ V, long long v_stride, int nl,
                                              const cx<double>* __restrict__ rho, long long r_stride,
                                              const int* __restrict__ ridx, int nr, long long n_atoms,
                                              long long atoms_per_split, double* __restrict__ out) {
-    __shared__ cx<double> vs[16][64];
-    __shared__ cx<double> rs[16][64];
+    // (16*IB) x (16*IB) tile of (left, right) pairs, IB x IB per thread; IB is chosen on the host
+    // so the tiles waste little of a small density count.
+    constexpr int TS = 16 * IB;
+    __shared__ cx<double> vs[16][TS];
+    __shared__ cx<double> rs[16][TS];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int l0 = blockIdx.x * 64, r0 = blockIdx.y * 64;
+    const int l0 = blockIdx.x * TS, r0 = blockIdx.y * TS;
     const long long k_begin = (long long)blockIdx.z * atoms_per_split;
     const long long k_end = min(n_atoms, k_begin + atoms_per_split);
-    double acc[4][4][4];
+    double acc[IB][IB][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < IB; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < IB; ++j)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
     for (long long k0 = k_begin; k0 < k_end; k0 += 16) {
-        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+        for (int e = threadIdx.x; e < 16 * TS; e += 256) {
             const int row = e >> 4, k = e & 15;
             const long long atom = k0 + k;
             const bool ok = atom < k_end;
@@ -469,15 +491,15 @@ static __global__ void __launch_bounds__(256) k_gram(const cx<double>* __restric
         __syncthreads();
 #pragma unroll 4
         for (int k = 0; k < 16; ++k) {
-            cx<double> v[4], r[4];
+            cx<double> v[IB], r[IB];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) v[i] = vs[k][ty + 16 * i];
+            for (int i = 0; i < IB; ++i) v[i] = vs[k][ty + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) r[j] = rs[k][tx + 16 * j];
+            for (int j = 0; j < IB; ++j) r[j] = rs[k][tx + 16 * j];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < IB; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
+                for (int j = 0; j < IB; ++j) {
                     acc[i][j][0] += v[i].re * r[j].re;
                     acc[i][j][1] += v[i].im * r[j].im;
                     acc[i][j][2] += v[i].re * r[j].im;
@@ -487,9 +509,9 @@ static __global__ void __launch_bounds__(256) k_gram(const cx<double>* __restric
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < IB; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < IB; ++j) {
             const int l = l0 + ty + 16 * i, r = r0 + tx + 16 * j;
             if (l < nl && r < nr) {
                 double* o = out + ((long long)l * nr + r) * 4;

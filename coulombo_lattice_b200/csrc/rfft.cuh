@@ -17,6 +17,7 @@
 #pragma once
 
 #include "fft.cuh"
+#include "kernels.cuh"
 
 namespace clk {
 
@@ -25,12 +26,20 @@ struct cmax {
     static constexpr int value = A > B ? A : B;
 };
 
+// Minimum resident blocks asked of the compiler: with a radix-16 factor two (<= 128 registers
+// for 256 threads; left alone those passes grow past it, one block per SM); otherwise none
+// (0: the compiler's own choice, measured lower than with any explicit minimum).
+template <int A, int B, int THREADS>
+struct col_min_blocks {
+    static constexpr int value = (A >= 16 || B >= 16) ? 2 : 0;
+};
+
 // ---------------------------------------------------------------------------------------
 // z pass: forward FFT along z, x Khat, inverse FFT along z; block = L adjacent xy columns,
 // densities [blockIdx.y * per, ...).
 // ---------------------------------------------------------------------------------------
 template <typename T, int R1, int R2, int L>
-__global__ void __launch_bounds__(L * cmax<R1, R2>::value)
+__global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2, L * cmax<R1, R2>::value>::value)
     k_zconv_rf(cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g,
                const T* __restrict__ khat, long long nxy, int np) {
     constexpr int N = R1 * R2;
@@ -94,9 +103,9 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value)
 // [blockIdx.y * per, ...).
 // ---------------------------------------------------------------------------------------
 template <int S, typename T, int R1, int R2, int L>
-__global__ void __launch_bounds__(L * cmax<R1, R2>::value)
+__global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2, L * cmax<R1, R2>::value>::value)
     k_ycol_rf(cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g, int nx, int ny,
-              int xchunks, int np) {
+              int xchunks, int np, const int* __restrict__ row_ptr) {
     constexpr int N = R1 * R2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
@@ -107,6 +116,23 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value)
     const int x = xc * L + line;
     const bool valid = x < nx;
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
+    // Rows (y, z) without atoms: after the forward x pass they are zero and were not stored;
+    // after the inverse y pass nothing reads them.  row_ptr == nullptr: every row is live.
+    unsigned live_in = 0, live_out = 0;
+    if (q < R2) {
+#pragma unroll
+        for (int j = 0; j < R1; ++j) {
+            const int r = z * ny + q + R2 * j;
+            if (!row_ptr || row_ptr[r + 1] > row_ptr[r]) live_in |= 1u << j;
+        }
+    }
+    if (q < R1) {
+#pragma unroll
+        for (int j = 0; j < R2; ++j) {
+            const int r = z * ny + q + j * R1;
+            if (!row_ptr || row_ptr[r + 1] > row_ptr[r]) live_out |= 1u << j;
+        }
+    }
     __syncthreads();
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
@@ -115,7 +141,10 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value)
         if (q < R2) {
             cx<T> v[R1];
 #pragma unroll
-            for (int j = 0; j < R1; ++j) v[j] = valid ? base[(long long)(q + R2 * j) * nx] : mk(T(0), T(0));
+            for (int j = 0; j < R1; ++j) {
+                const bool load = valid && (S > 0 || ((live_in >> j) & 1u));
+                v[j] = load ? base[(long long)(q + R2 * j) * nx] : mk(T(0), T(0));
+            }
             dft<R1, S>(v);
 #pragma unroll
             for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * L + line] = v[r];
@@ -130,7 +159,225 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value)
             dft<R2, S>(u);
             if (valid) {
 #pragma unroll
-                for (int r = 0; r < R2; ++r) base[(long long)(q + r * R1) * nx] = u[r];
+                for (int r = 0; r < R2; ++r)
+                    if (S < 0 || ((live_out >> r) & 1u)) base[(long long)(q + r * R1) * nx] = u[r];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+
+// ---------------------------------------------------------------------------------------
+// Row passes (x) with the same two-factor register FFT.  A block owns LR consecutive rows
+// (row = z*ny + y) held transposed in shared memory, T[x*(LR+1) + row]: phase A maps
+// consecutive threads to consecutive rows and phase B to consecutive x, both free of bank
+// conflicts thanks to the odd row pitch.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Forward: scatter the rows' atoms x conj(phase_kappa), FFT along x, store whole rows.
+template <typename T, int R1, int R2, int LR>
+__global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R2, LR * cmax<R1, R2>::value>::value)
+    k_xfwd_rf(const cx<double>* __restrict__ rho, long long rho_stride, const int* __restrict__ row_ptr,
+              const int* __restrict__ cell, cx<T>* __restrict__ out, long long out_stride,
+              const cx<T>* __restrict__ tw_g, RoundPhase rp, int ny, int nrows, int np, int skip_empty) {
+    constexpr int N = R1 * R2;
+    constexpr int LP = LR + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* tile = tw + N;
+    cx<T>* ex = tile + N * LP;
+    const int r0 = blockIdx.x * LR;
+    const int nr = min(LR, nrows - r0);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
+    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + nr];
+    const int per = (np + gridDim.y - 1) / gridDim.y;
+    const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
+    // a row without atoms transforms to zero; with skip_empty the consumer (the forward y
+    // pass) reads zero for it instead of loading it, so it is not stored
+    bool store_row;
+    {
+        const int lr = threadIdx.x / R1;
+        store_row = lr < nr && (!skip_empty || row_ptr[r0 + lr + 1] > row_ptr[r0 + lr]);
+    }
+    // the block's atoms (at most KA per thread): shared-memory slot and phase, computed once
+    // for all densities
+    constexpr int KA = 4;
+    const bool pre = (a1 - a0) <= KA * (int)blockDim.x;
+    int slot[KA];
+    cx<double> ph[KA];
+    if (pre) {
+#pragma unroll
+        for (int k = 0; k < KA; ++k) {
+            const int i = a0 + threadIdx.x + k * blockDim.x;
+            slot[k] = -1;
+            if (i < a1) {
+                const int c = cell[i];
+                const int row = c / N, x = c - row * N;
+                slot[k] = x * LP + (row - r0);
+                ph[k] = round_phase(rp, x, row % ny, row / ny);
+            }
+        }
+    }
+    for (int p = p_begin; p < p_end; ++p) {
+        for (int e = threadIdx.x; e < N * LP; e += blockDim.x) tile[e] = mk(T(0), T(0));
+        __syncthreads();
+        const cx<double>* rp_ = rho + (long long)p * rho_stride;
+        if (pre) {
+#pragma unroll
+            for (int k = 0; k < KA; ++k)
+                if (slot[k] >= 0) tile[slot[k]] = narrow<T>(cmulc(rp_[a0 + threadIdx.x + k * blockDim.x], ph[k]));
+        } else {
+            for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+                const int c = cell[i];
+                const int row = c / N, x = c - row * N;
+                const int y = row % ny, z = row / ny;
+                tile[x * LP + (row - r0)] = narrow<T>(cmulc(rp_[i], round_phase(rp, x, y, z)));
+            }
+        }
+        __syncthreads();
+        {
+            const int lr = threadIdx.x % LR, t = threadIdx.x / LR;
+            if (t < R2) {
+                cx<T> v[R1];
+#pragma unroll
+                for (int j = 0; j < R1; ++j) v[j] = tile[(t + R2 * j) * LP + lr];
+                dft<R1, -1>(v);
+#pragma unroll
+                for (int r = 0; r < R1; ++r) ex[(t * R1 + r) * LP + lr] = v[r];
+            }
+        }
+        __syncthreads();
+        {
+            const int j = threadIdx.x % R1, lr = threadIdx.x / R1;
+            if (store_row) {
+                cx<T> u[R2];
+#pragma unroll
+                for (int r = 0; r < R2; ++r) u[r] = ex[(j + r * R1) * LP + lr];
+#pragma unroll
+                for (int r = 1; r < R2; ++r) u[r] = cmul(u[r], tw[r * j]);
+                dft<R2, -1>(u);
+                cx<T>* o = out + (long long)p * out_stride + (long long)(r0 + lr) * N + j;
+#pragma unroll
+                for (int r = 0; r < R2; ++r) o[r * R1] = u[r];
+            }
+        }
+    }
+}
+
+// Inverse: rows of the next density are prefetched with cp.async while the current one is
+// transformed; then x phase_kappa is accumulated into V at the rows' atoms (FP64).
+template <typename T, int R1, int R2, int LR>
+__global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R2, LR * cmax<R1, R2>::value>::value)
+    k_xinv_rf(const cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g, RoundPhase rp,
+              const int* __restrict__ row_ptr, const int* __restrict__ cell, cx<double>* __restrict__ V,
+              long long v_stride, int ny, int nrows, int np) {
+    constexpr int N = R1 * R2;
+    constexpr int LP = LR + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* tb[2] = {tw + N, tw + N + N * LP};
+    cx<T>* ex = tw + N + 2 * N * LP;
+    __shared__ unsigned char live[LR];
+    const int r0 = blockIdx.x * LR;
+    const int nr = min(LR, nrows - r0);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
+    if (threadIdx.x < LR) {
+        const int r = r0 + threadIdx.x;
+        live[threadIdx.x] = (threadIdx.x < nr && row_ptr[r + 1] > row_ptr[r]) ? 1 : 0;
+    }
+    __syncthreads();
+    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + nr];
+    const int per = (np + gridDim.y - 1) / gridDim.y;
+    const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
+    // rows without atoms are never gathered, so they are not loaded (their slots keep
+    // whatever the buffer held; each row's transform is independent)
+    auto load = [&](int p, cx<T>* dst) {
+        const cx<T>* src = buf + (long long)p * stride + (long long)r0 * N;
+        for (int e = threadIdx.x; e < nr * N; e += blockDim.x) {
+            const int lr = e / N, x = e - lr * N;
+            if (live[lr]) cp_async<sizeof(cx<T>)>(dst + x * LP + lr, src + e);
+        }
+        cp_async_commit();
+    };
+    constexpr int KA = 4;
+    const bool pre = (a1 - a0) <= KA * (int)blockDim.x;
+    int slot[KA];
+    cx<double> ph[KA];
+    if (pre) {
+#pragma unroll
+        for (int k = 0; k < KA; ++k) {
+            const int i = a0 + threadIdx.x + k * blockDim.x;
+            slot[k] = -1;
+            if (i < a1) {
+                const int c = cell[i];
+                const int row = c / N, x = c - row * N;
+                slot[k] = x * LP + (row - r0);
+                ph[k] = round_phase(rp, x, row % ny, row / ny);
+            }
+        }
+    }
+    if (p_begin < p_end) load(p_begin, tb[0]);
+    for (int p = p_begin; p < p_end; ++p) {
+        cx<T>* cur = tb[(p - p_begin) & 1];
+        if (p + 1 < p_end) {
+            load(p + 1, tb[(p + 1 - p_begin) & 1]);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        {
+            const int lr = threadIdx.x % LR, t = threadIdx.x / LR;
+            if (t < R2) {
+                cx<T> v[R1];
+#pragma unroll
+                for (int j = 0; j < R1; ++j) v[j] = cur[(t + R2 * j) * LP + lr];
+                dft<R1, +1>(v);
+#pragma unroll
+                for (int r = 0; r < R1; ++r) ex[(t * R1 + r) * LP + lr] = v[r];
+            }
+        }
+        __syncthreads();
+        {
+            const int j = threadIdx.x % R1, lr = threadIdx.x / R1;
+            if (lr < LR) {
+                cx<T> u[R2];
+#pragma unroll
+                for (int r = 0; r < R2; ++r) u[r] = ex[(j + r * R1) * LP + lr];
+#pragma unroll
+                for (int r = 1; r < R2; ++r) u[r] = cmulc(u[r], tw[r * j]);
+                dft<R2, +1>(u);
+#pragma unroll
+                for (int r = 0; r < R2; ++r) cur[(j + r * R1) * LP + lr] = u[r];
+            }
+        }
+        __syncthreads();
+        cx<double>* vp = V + (long long)p * v_stride;
+        if (pre) {
+#pragma unroll
+            for (int k = 0; k < KA; ++k)
+                if (slot[k] >= 0) {
+                    const int i = a0 + threadIdx.x + k * blockDim.x;
+                    vp[i] = vp[i] + cmul(widen(cur[slot[k]]), ph[k]);
+                }
+        } else {
+            for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+                const int c = cell[i];
+                const int row = c / N, x = c - row * N;
+                const int y = row % ny, z = row / ny;
+                vp[i] = vp[i] + cmul(widen(cur[x * LP + (row - r0)]), round_phase(rp, x, y, z));
             }
         }
         __syncthreads();

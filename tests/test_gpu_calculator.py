@@ -104,3 +104,29 @@ def test_register_column_passes_match_oracle(mode, dims):
         cc.prepare(F)
         Vg = cc.potential()
     assert np.abs(Vg - V).max() <= TOL[mode] * 10 * np.abs(V).max()
+
+
+# long x axes with y outside the whole-plane sizes: the register row passes (scatter + FFT
+# along x, FFT along x + gather) are exercised
+ROW_SHAPES = [(256, 8, 6), (96, 12, 10), (160, 6, 5), (45, 12, 6), (128, 6, 8), (240, 4, 6), (225, 4, 4),
+              (20, 6, 6), (192, 10, 4), (100, 12, 3)]
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("dims", ROW_SHAPES)
+def test_register_row_passes_match_oracle(mode, dims):
+    nx, ny, nz = dims
+    rng = np.random.default_rng(3 * nx + ny + 11 * nz)
+    F = rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx))
+    F2 = rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx))
+    step = (0.9, 1.3, 1.2)
+    ghat = C.kernel_spectrum(C.kernel_octant(dims, step, dielectric=4.0, onsite=0.2), dims)
+    V = C.prepare(F, ghat)
+    want = C.calculate(V, F2)
+    with cl.CoulombCalculator(dims, step, mode) as cc:
+        cc.initialize(dielectric=4.0, onsite=0.2)
+        cc.prepare(F)
+        Vg = cc.potential()
+        got = cc.calculate(F2)
+    assert np.abs(Vg - V).max() <= TOL[mode] * 10 * np.abs(V).max()
+    assert abs(got - want) <= TOL[mode] * 10 * np.sqrt(np.sum(np.abs(V) ** 2) * np.sum(np.abs(F2) ** 2))
