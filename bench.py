@@ -33,6 +33,8 @@ WORKLOADS = {
     "c2": "zinc-blende 24x24x24 cells (lens-dot states), 96^3 grid, 110592 atoms, 20 orbitals, 6e+6h, "
           "eeee,hhhh,ehhe,eheh",
     "c3": "zinc-blende 64x64x64 cells, 256^3 grid, 2097152 atoms, 20 orbitals, 4e+4h, eeee,hhhh,ehhe,eheh",
+    "c4": "zinc-blende 32x32x32 cells (lens-dot Hermite-Gaussian states), 128^3 grid, 262144 atoms, 20 orbitals, "
+          "20e+20h, ijkl (all 2,560,000 integrals, 820 pair densities)",
 }
 DIELECTRIC = 10.89
 
@@ -186,7 +188,7 @@ def run_reference(args):
         return
     d = build_workload(args.config)
     threads = os.cpu_count() or 1
-    n_left = {"c1": 2, "c2": 2, "c3": 1}[args.config]
+    n_left = {"c1": 2, "c2": 2, "c3": 1, "c4": 1}[args.config]
     for _ in range(args.warmup):
         cpu_sample(d, n_left, threads)
     vals, secs = [], []
@@ -352,7 +354,7 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        n_left = {"c1": 2, "c2": 4, "c3": 1}[args.config]
+        n_left = {"c1": 2, "c2": 4, "c3": 1, "c4": 1}[args.config]
         line["cpu_baseline"] = cpu_baseline_entry(d, n_left, threads)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -901,7 +901,7 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
         for (int64_t i = 0; i < n_int; ++i)
             for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
-        const auto plan = cl::compute_plan(c->n_states, specs);
+        const auto plan = cl::orient_steps(c->n_states, specs);
         // densities: prepared (left) products first, then right-only products
         const int P = c->n_states * (c->n_states + 1) / 2;
         std::vector<int> slot(P, -1), is_left(P, 0), is_right(P, 0);

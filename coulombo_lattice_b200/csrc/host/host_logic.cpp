@@ -192,7 +192,10 @@ void product_states(int p, int* fl, int* fr) {
 // vertex of largest (degree, index) does.
 // ---------------------------------------------------------------------------------------
 std::set<int> vertex_cover(int vertex_count, const std::vector<std::pair<int, int>>& edge_list) {
-    std::set<std::pair<int, int>> edges(edge_list.begin(), edge_list.end());
+    // the distinct edges, in the set order of the reference (sorted pairs)
+    std::vector<std::pair<int, int>> edges(edge_list);
+    std::sort(edges.begin(), edges.end());
+    edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
     std::set<int> cover;
     for (const auto& e : edges)
         if (e.first == e.second) cover.insert(e.first);
@@ -229,6 +232,30 @@ std::set<int> vertex_cover(int vertex_count, const std::vector<std::pair<int, in
 // ---------------------------------------------------------------------------------------
 // src/Planner.hpp:71-104
 // ---------------------------------------------------------------------------------------
+std::vector<PlanStep> orient_steps(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs) {
+    if (specs.size() > static_cast<size_t>(std::numeric_limits<int>::max()))
+        fail(CL_ERR_ARGUMENT, "too many integrals to compute");
+    const int product_count = n_inputs * (n_inputs + 1) / 2;
+    std::vector<PlanStep> steps;
+    steps.reserve(specs.size());
+    std::vector<std::pair<int, int>> edges;
+    edges.reserve(specs.size());
+    for (size_t id = 0; id < specs.size(); ++id) {
+        const auto& s = specs[id];
+        for (int k = 0; k < 4; ++k)
+            if (s[k] < 1 || s[k] > n_inputs) fail(CL_ERR_ARGUMENT, "integral index out of range");
+        PlanStep st{static_cast<int>(id), product_of(s[0], s[3]), product_of(s[1], s[2])};
+        steps.push_back(st);
+        edges.push_back({st.left.product, st.right.product});
+    }
+    const auto cover = vertex_cover(product_count, edges);
+    std::vector<char> in_cover(product_count, 0);
+    for (int v : cover) in_cover[v] = 1;
+    for (auto& st : steps)
+        if (!in_cover[st.left.product]) std::swap(st.left, st.right);
+    return steps;
+}
+
 std::vector<PlanStep> compute_plan(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs) {
     if (specs.size() > static_cast<size_t>(std::numeric_limits<int>::max()))
         fail(CL_ERR_ARGUMENT, "too many integrals to compute");

@@ -59,4 +59,9 @@ struct PlanStep {
 };
 std::vector<PlanStep> compute_plan(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs);
 
+// The same steps with the reference's orientation (which product is prepared) but in input
+// order: the GPU computes every step at once, so the execution order of
+// Planner.hpp:94-101 does not matter to the values.
+std::vector<PlanStep> orient_steps(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs);
+
 }  // namespace cl
