@@ -61,6 +61,13 @@ SIGNATURES = [
     ("cl_compute_rounds", _i, [_vp, _i64, _P(ctypes.c_int16), _i, _P(_d)]),
     ("cl_set_profiling", _i, [_vp, _i]),
     ("cl_kernel_profile", _i, [_vp, _P(_d), _P(_i64), _P(_d)]),
+    ("cl_request_create", _i, [_vp, _i64, _P(ctypes.c_int16), _P(_vp)]),
+    ("cl_request_run", _i, [_vp, _P(_d)]),
+    ("cl_request_destroy", None, [_vp]),
+    ("cl_batch_create", _i, [_P(_vp), _i, _P(_vp)]),
+    ("cl_batch_run", _i, [_vp, _P(_P(_d))]),
+    ("cl_batch_last_ms", _i, [_vp, _P(_d)]),
+    ("cl_batch_destroy", None, [_vp]),
     ("cl_fft3d", _i, [_i, _i, _i, _i, _i, _i, _P(_d)]),
     ("cl_fft3d_noalloc", _i, [_i, _i, _i, _i, _i, _vp]),
     ("cl_round_up_235", _i, [_i, _i]),
@@ -273,6 +280,10 @@ class CoulombCalculator:
         _check(lib().cl_compute(self._h, int(n_int), ctypes.cast(spec_ptr, ctypes.POINTER(ctypes.c_int16)),
                                 ctypes.cast(out_ptr, ctypes.POINTER(ctypes.c_double))))
 
+    def request(self, specs):
+        """A prepared request (Request) for repeated runs of the same integral list."""
+        return Request(self, specs)
+
     def potentials(self):
         out = np.zeros((self.n_states, self.n_atoms))
         _check(lib().cl_potentials(self._h, _ptr(out)))
@@ -282,3 +293,64 @@ class CoulombCalculator:
         t = np.zeros(4)
         _check(lib().cl_last_timings(self._h, _ptr(t)))
         return dict(densities_ms=t[0], transforms_ms=t[1], reductions_ms=t[2], total_ms=t[3])
+
+
+class Request:
+    """cl_request: plan, device buffers and pinned results prepared once; run() enqueues only."""
+
+    def __init__(self, calc, specs):
+        self.calc = calc
+        self.specs = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
+        h = ctypes.c_void_p()
+        _check(lib().cl_request_create(calc._h, self.specs.shape[0], _ptr(self.specs, ctypes.c_int16),
+                                       ctypes.byref(h)))
+        self._h = h
+        self.out = np.zeros(2 * self.specs.shape[0])
+
+    def run(self):
+        _check(lib().cl_request_run(self._h, _ptr(self.out)))
+        return self.out[0::2] + 1j * self.out[1::2]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().cl_request_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """cl_batch: requests on distinct contexts, captured once as one CUDA graph and replayed."""
+
+    def __init__(self, requests):
+        self.requests = list(requests)
+        arr = (ctypes.c_void_p * len(self.requests))(*[r._h.value for r in self.requests])
+        h = ctypes.c_void_p()
+        _check(lib().cl_batch_create(arr, len(self.requests), ctypes.byref(h)))
+        self._h = h
+        self._outs = (ctypes.POINTER(ctypes.c_double) * len(self.requests))(
+            *[_ptr(r.out) for r in self.requests])
+
+    def run(self):
+        _check(lib().cl_batch_run(self._h, self._outs))
+        return [r.out[0::2] + 1j * r.out[1::2] for r in self.requests]
+
+    def last_ms(self):
+        ms = ctypes.c_double()
+        _check(lib().cl_batch_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().cl_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

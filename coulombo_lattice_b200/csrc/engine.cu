@@ -279,8 +279,11 @@ struct cl_ctx {
     long long live_rows = 0;           // rows (y, z) holding at least one atom
     std::vector<long long> atom_slot;  // input atom -> sorted (deduplicated) slot
 
-    // work buffers
+    // work buffers, kept across requests (grown on demand)
     DevBuf<unsigned char> work;
+    DevBuf<cx<double>> req_rho, req_V;
+    DevBuf<double> req_o4;
+    DevBuf<int> req_ridx;
     double timings[4] = {0, 0, 0, 0};
 
     // per-kernel profiling (events recorded around launches on `stream`)
@@ -641,35 +644,60 @@ void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<d
     prof_end(c, e, CL_KCLASS_GRAM, (double)(nl + nr) * n_atoms * 16.0);
 }
 
-// Pair densities rho[p][atom] for products (fl[p], fr[p]) (0-based state indices).
-void pair_densities(cl_ctx* c, const std::vector<int2>& fl, cx<double>* rho) {
-    const int np = (int)fl.size();
+// Pair densities rho[p][atom] for products (fl[p], fr[p]) (0-based state indices): the
+// device lists and launch shape are set up once (setup synchronises), the launch itself only
+// enqueues (it can be captured in a CUDA graph).
+struct PairSetup {
+    DevBuf<int2> prods;  // indices into `states`
+    DevBuf<int> states;
+    int np = 0, n_used = 0, chunk = 1, blocks = 1;
+    size_t smem = 0;
+};
+
+void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
+    ps.np = (int)fl.size();
     std::vector<int> used;
     std::vector<int> where(c->n_states, -1);
     for (const auto& f : fl)
         for (int s : {f.x, f.y})
             if (where[s] < 0) { where[s] = (int)used.size(); used.push_back(s); }
-    std::vector<int2> local(np);
-    for (int p = 0; p < np; ++p) local[p] = make_int2(where[fl[p].x], where[fl[p].y]);
-    DevBuf<int2> dprods;
-    dprods.upload(local.data(), local.size(), c->stream);
-    DevBuf<int> dstates;
-    dstates.upload(used.data(), used.size(), c->stream);
+    std::vector<int2> local(ps.np);
+    for (int p = 0; p < ps.np; ++p) local[p] = make_int2(where[fl[p].x], where[fl[p].y]);
+    ps.prods.upload(local.data(), local.size(), c->stream);
+    ps.states.upload(used.data(), used.size(), c->stream);
+    ps.n_used = (int)used.size();
     const int os = c->n_orb | 1;
     const size_t per_atom = sizeof(cx<double>) * (size_t)used.size() * os;
-    int chunk = (int)std::max<size_t>(1, std::min<size_t>(64, (96 * 1024) / per_atom));
-    const size_t smem = per_atom * chunk;
-    ensure_smem(clk::k_pair_density, smem);
-    const long long chunks = (c->n_sorted + chunk - 1) / chunk;
-    const int blocks = (int)std::min<long long>(chunks, 148LL * 8);
+    ps.chunk = (int)std::max<size_t>(1, std::min<size_t>(64, (40 * 1024) / per_atom));
+    ps.smem = per_atom * ps.chunk;
+    ensure_smem(clk::k_pair_density, ps.smem);
+    const long long chunks = (c->n_sorted + ps.chunk - 1) / ps.chunk;
+    ps.blocks = (int)std::min<long long>(chunks, 148LL * 8);
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+void pair_launch(cl_ctx* c, const PairSetup& ps, cx<double>* rho) {
     cudaEvent_t e = prof_begin(c);
-    clk::k_pair_density<<<blocks, 256, smem, c->stream>>>(c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p,
-                                                         c->n_sorted, dprods.p, np, dstates.p, (int)used.size(),
-                                                         chunk, rho);
+    clk::k_pair_density<<<ps.blocks, 256, ps.smem, c->stream>>>(c->coeff.p, c->n_atoms, c->n_orb,
+                                                               c->orig_sorted.p, c->n_sorted, ps.prods.p, ps.np,
+                                                               ps.states.p, ps.n_used, ps.chunk, rho);
     CL_LAUNCHED();
     prof_end(c, e, CL_KCLASS_DENSITY,
-             (double)used.size() * c->n_atoms * c->n_orb * 16.0 + (double)np * c->n_sorted * 16.0);
+             (double)ps.n_used * c->n_atoms * c->n_orb * 16.0 + (double)ps.np * c->n_sorted * 16.0);
+}
+
+void pair_densities(cl_ctx* c, const std::vector<int2>& fl, cx<double>* rho) {
+    PairSetup ps;
+    pair_setup(c, fl, ps);
+    pair_launch(c, ps, rho);
     CL_CUDA(cudaStreamSynchronize(c->stream));  // device lists go out of scope
+}
+
+// Device buffer of at least `count` elements, reallocated only when it must grow.
+template <typename T>
+void grow(DevBuf<T>& b, size_t count) {
+    if (b.n >= count && b.p) return;
+    b.alloc(count);
 }
 
 void check_ctx(cl_ctx* c) {
@@ -926,13 +954,15 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
             fl[i] = make_int2(a - 1, b - 1);
         }
         const long long As = c->n_sorted;
-        DevBuf<int> dr;
-        dr.upload(rights.data(), rights.size(), c->stream);
-        DevBuf<cx<double>> rho, V;
-        rho.alloc((size_t)nu * As);
-        V.alloc((size_t)nl * As);
-        DevBuf<double> o4;
-        o4.alloc((size_t)4 * nl * nr);
+        DevBuf<int>& dr = c->req_ridx;
+        grow(dr, rights.size());
+        CL_CUDA(cudaMemcpyAsync(dr.p, rights.data(), rights.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        DevBuf<cx<double>>& rho = c->req_rho;
+        DevBuf<cx<double>>& V = c->req_V;
+        grow(rho, (size_t)nu * As);
+        grow(V, (size_t)nl * As);
+        DevBuf<double>& o4 = c->req_o4;
+        grow(o4, (size_t)4 * nl * nr);
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
         CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)nl * As, c->stream));
@@ -1048,6 +1078,234 @@ int cl_potentials(cl_ctx* c, double* out) {
         c->timings[1] = t12;
         c->timings[2] = 0;
         c->timings[3] = t01 + t12;
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Prepared requests and graph-captured batches
+// ---------------------------------------------------------------------------------------
+struct cl_request {
+    cl_ctx* ctx = nullptr;
+    int64_t n_int = 0;
+    std::vector<cl::PlanStep> plan;
+    std::vector<int> slot, rcol;
+    int nl = 0, nr = 0;
+    PairSetup ps;
+    DevBuf<int> ridx;
+    DevBuf<cx<double>> rho, V;
+    DevBuf<double> o4;
+    double* o4_host = nullptr;  // pinned
+    bool warm = false;
+    ~cl_request() {
+        if (o4_host) cudaFreeHost(o4_host);
+    }
+};
+
+struct cl_batch {
+    std::vector<cl_request*> reqs;
+    cudaStream_t master = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double last_ms = 0;
+    ~cl_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto e : joins) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+        if (master) cudaStreamDestroy(master);
+    }
+};
+
+namespace {
+
+// Stream-ordered work of a prepared request: no allocation, no host synchronisation, no
+// pageable copies -- it can be captured.
+void request_enqueue(cl_request* r) {
+    cl_ctx* c = r->ctx;
+    const long long As = c->n_sorted;
+    pair_launch(c, r->ps, r->rho.p);
+    CL_CUDA(cudaMemsetAsync(r->V.p, 0, sizeof(cx<double>) * (size_t)r->nl * As, c->stream));
+    run_rounds_mode(c, r->rho.p, As, r->nl, c->row_ptr.p, c->cell_sorted.p, r->V.p, As);
+    gram(c, r->V.p, As, r->nl, r->rho.p, As, r->ridx.p, r->nr, As, r->o4.p);
+    CL_CUDA(cudaMemcpyAsync(r->o4_host, r->o4.p, sizeof(double) * 4 * (size_t)r->nl * r->nr,
+                            cudaMemcpyDeviceToHost, c->stream));
+}
+
+void request_finish(cl_request* r, double* out) {
+    for (const auto& st : r->plan) {
+        const int l = r->slot[st.left.product], rr = r->rcol[st.right.product];
+        const double* q = &r->o4_host[((size_t)l * r->nr + rr) * 4];
+        const bool rconj = st.left.conjugate != st.right.conjugate;
+        double re = rconj ? q[0] + q[1] : q[0] - q[1];
+        double im = rconj ? q[3] - q[2] : q[2] + q[3];
+        if (st.left.conjugate) im = -im;
+        out[2 * st.id] = re;
+        out[2 * st.id + 1] = im;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cl_request_create(cl_ctx* c, int64_t n_int, const int16_t* spec, cl_request** out) {
+    if (out) *out = nullptr;
+    cl_request* r = nullptr;
+    int st = cl::guarded([&] {
+        check_ctx(c);
+        check_kernel(c);
+        if (!out) cl::fail(CL_ERR_ARGUMENT, "null output pointer");
+        if (c->n_states == 0) cl::fail(CL_ERR_STATE, "no states loaded (call cl_set_states)");
+        if (n_int <= 0 || !spec) cl::fail(CL_ERR_ARGUMENT, "invalid integral list");
+        r = new cl_request();
+        r->ctx = c;
+        r->n_int = n_int;
+        std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
+        for (int64_t i = 0; i < n_int; ++i)
+            for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
+        r->plan = cl::orient_steps(c->n_states, specs);
+        const int P = c->n_states * (c->n_states + 1) / 2;
+        std::vector<int> is_left(P, 0), is_right(P, 0);
+        r->slot.assign(P, -1);
+        r->rcol.assign(P, -1);
+        for (const auto& s : r->plan) {
+            is_left[s.left.product] = 1;
+            is_right[s.right.product] = 1;
+        }
+        std::vector<int> prods, rights;
+        for (int p = 0; p < P; ++p)
+            if (is_left[p]) { r->slot[p] = (int)prods.size(); prods.push_back(p); }
+        r->nl = (int)prods.size();
+        for (int p = 0; p < P; ++p)
+            if (is_right[p] && r->slot[p] < 0) { r->slot[p] = (int)prods.size(); prods.push_back(p); }
+        for (int p = 0; p < P; ++p)
+            if (is_right[p]) { r->rcol[p] = (int)rights.size(); rights.push_back(r->slot[p]); }
+        r->nr = (int)rights.size();
+        std::vector<int2> fl(prods.size());
+        for (size_t i = 0; i < prods.size(); ++i) {
+            int a, b;
+            cl::product_states(prods[i], &a, &b);
+            fl[i] = make_int2(a - 1, b - 1);
+        }
+        const long long As = c->n_sorted;
+        pair_setup(c, fl, r->ps);
+        r->ridx.upload(rights.data(), rights.size(), c->stream);
+        r->rho.alloc((size_t)prods.size() * As);
+        r->V.alloc((size_t)r->nl * As);
+        r->o4.alloc((size_t)4 * r->nl * r->nr);
+        CL_CUDA(cudaMallocHost(&r->o4_host, sizeof(double) * 4 * (size_t)r->nl * r->nr));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        *out = r;
+    });
+    if (st != CL_OK) delete r;
+    return st;
+}
+
+void cl_request_destroy(cl_request* r) {
+    if (!r) return;
+    cudaSetDevice(r->ctx->device);
+    delete r;
+}
+
+int cl_request_run(cl_request* r, double* out) {
+    return cl::guarded([&] {
+        if (!r || !out) cl::fail(CL_ERR_ARGUMENT, "null argument");
+        check_ctx(r->ctx);
+        request_enqueue(r);
+        CL_CUDA(cudaStreamSynchronize(r->ctx->stream));
+        prof_collect(r->ctx);
+        r->warm = true;
+        request_finish(r, out);
+    });
+}
+
+int cl_batch_create(cl_request** reqs, int n, cl_batch** out) {
+    if (out) *out = nullptr;
+    cl_batch* b = nullptr;
+    int st = cl::guarded([&] {
+        if (!reqs || n <= 0 || !out) cl::fail(CL_ERR_ARGUMENT, "invalid batch");
+        const int dev = reqs[0]->ctx->device;
+        for (int i = 0; i < n; ++i) {
+            if (!reqs[i]) cl::fail(CL_ERR_ARGUMENT, "null request");
+            if (reqs[i]->ctx->device != dev) cl::fail(CL_ERR_ARGUMENT, "all requests of a batch must share one device");
+            for (int j = 0; j < i; ++j)
+                if (reqs[j]->ctx == reqs[i]->ctx)
+                    cl::fail(CL_ERR_ARGUMENT, "requests of one batch need distinct contexts (one stream each)");
+        }
+        CL_CUDA(cudaSetDevice(dev));
+        b = new cl_batch();
+        b->reqs.assign(reqs, reqs + n);
+        CL_CUDA(cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking));
+        CL_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        CL_CUDA(cudaEventCreate(&b->t0));
+        CL_CUDA(cudaEventCreate(&b->t1));
+        b->joins.resize(n);
+        for (auto& e : b->joins) CL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        *out = b;
+    });
+    if (st != CL_OK) delete b;
+    return st;
+}
+
+void cl_batch_destroy(cl_batch* b) {
+    if (!b) return;
+    if (!b->reqs.empty()) cudaSetDevice(b->reqs[0]->ctx->device);
+    delete b;
+}
+
+int cl_batch_run(cl_batch* b, double** outs) {
+    return cl::guarded([&] {
+        if (!b || !outs) cl::fail(CL_ERR_ARGUMENT, "null argument");
+        CL_CUDA(cudaSetDevice(b->reqs[0]->ctx->device));
+        if (!b->exec) {
+            // one eager run of every request sizes every buffer and sets every kernel
+            // attribute; then the whole batch is captured once as parallel branches
+            for (cl_request* r : b->reqs)
+                if (!r->warm) {
+                    request_enqueue(r);
+                    CL_CUDA(cudaStreamSynchronize(r->ctx->stream));
+                    prof_collect(r->ctx);
+                    r->warm = true;
+                }
+            std::vector<char> prof(b->reqs.size());
+            for (size_t i = 0; i < b->reqs.size(); ++i) {
+                prof[i] = b->reqs[i]->ctx->profiling;
+                b->reqs[i]->ctx->profiling = false;
+            }
+            CL_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeRelaxed));
+            CL_CUDA(cudaEventRecord(b->fork, b->master));
+            for (size_t i = 0; i < b->reqs.size(); ++i) {
+                cl_request* r = b->reqs[i];
+                CL_CUDA(cudaStreamWaitEvent(r->ctx->stream, b->fork, 0));
+                request_enqueue(r);
+                CL_CUDA(cudaEventRecord(b->joins[i], r->ctx->stream));
+                CL_CUDA(cudaStreamWaitEvent(b->master, b->joins[i], 0));
+            }
+            CL_CUDA(cudaStreamEndCapture(b->master, &b->graph));
+            for (size_t i = 0; i < b->reqs.size(); ++i) b->reqs[i]->ctx->profiling = prof[i];
+            CL_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        }
+        CL_CUDA(cudaEventRecord(b->t0, b->master));
+        CL_CUDA(cudaGraphLaunch(b->exec, b->master));
+        CL_CUDA(cudaEventRecord(b->t1, b->master));
+        CL_CUDA(cudaStreamSynchronize(b->master));
+        float ms = 0;
+        CL_CUDA(cudaEventElapsedTime(&ms, b->t0, b->t1));
+        b->last_ms = ms;
+        for (size_t i = 0; i < b->reqs.size(); ++i) request_finish(b->reqs[i], outs[i]);
+    });
+}
+
+int cl_batch_last_ms(cl_batch* b, double* ms) {
+    return cl::guarded([&] {
+        if (!b || !ms) cl::fail(CL_ERR_ARGUMENT, "null argument");
+        *ms = b->last_ms;
     });
 }
 

@@ -141,6 +141,32 @@ int cl_kernel_profile(cl_ctx* ctx, double ms[CL_NUM_KCLASS], int64_t launches[CL
                       double bytes[CL_NUM_KCLASS]);
 
 /* ---------------------------------------------------------------------------------------
+ * Prepared requests and graph-captured batches of independent structures
+ * ------------------------------------------------------------------------------------- */
+
+typedef struct cl_request cl_request;
+typedef struct cl_batch cl_batch;
+
+/* A request prepared once: the plan of n_int integrals (as for cl_compute), its device
+ * buffers and its pinned result buffer.  Running it only enqueues kernels and copies, which
+ * is what lets batches be captured in a CUDA graph.  Replaces, for repeated requests over the
+ * same states, the per-call planning of coulombo.cpp:121-151. */
+int cl_request_create(cl_ctx* ctx, int64_t n_int, const int16_t* spec, cl_request** out);
+int cl_request_run(cl_request* req, double* out /* [n_int]{re,im} */);
+void cl_request_destroy(cl_request* req);
+
+/* A batch of requests on distinct contexts of one GPU (e.g. nanostructures of uneven grid
+ * sizes).  The first cl_batch_run runs each request once, then captures all of them as
+ * parallel branches of one CUDA graph (each on its own context's stream); every run launches
+ * that graph once.  outs[i] receives request i's values.  No reference counterpart (the
+ * reference runs one structure per process). */
+int cl_batch_create(cl_request** reqs, int n, cl_batch** out);
+int cl_batch_run(cl_batch* batch, double** outs);
+/* Device time (ms, CUDA events around the graph launch) of the last cl_batch_run. */
+int cl_batch_last_ms(cl_batch* batch, double* ms);
+void cl_batch_destroy(cl_batch* batch);
+
+/* ---------------------------------------------------------------------------------------
  * FFT engine (FourierPlan seam, src/FourierPlan.hpp:17-39)
  * ------------------------------------------------------------------------------------- */
 
