@@ -4,8 +4,9 @@
 the all-FP64 plain path within max(1e-6 |I|, 1e-9 eV).
 
 A step is one full request over one synthetic zinc-blende structure: pair densities, the
-8-round convolution of every prepared density and the FP64 real-space reductions of every
-requested integral.  `value` is device time (CUDA events on the library's stream) with the
+8-round convolution of every prepared density and the real-space reductions of every
+requested integral (split-precision tensor-core Gram with FP64 accumulation).  `value` is the
+device time (CUDA events) of one CUDA-graph replay of the prepared request per step, with the
 inputs resident in HBM; `e2e` runs the public C ABI from pinned host buffers (coefficient and
 cell upload, compute, result download) every step.
 
@@ -64,6 +65,14 @@ def measured_peaks():
             d = json.load(fh)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def peak_tflops_bf16():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return float(json.load(fh)["bf16_tflops"])
+    return 1590.0
 
 
 def profiled_traffic(config, kernel):
@@ -358,25 +367,46 @@ def run_ours(args):
                 "max_abs_err_eV": float(err.max()), "worst_err_over_gate": float((err / lim).max()),
                 "gate": "max(1e-6|I|, 1e-9 eV) vs the all-FP64 plain path", "pass": bool(np.all(err <= lim))}
 
-    # ---- timed region: resident inputs, device time ------------------------------------
+    # ---- timed region: resident inputs, one CUDA-graph replay of the prepared request per
+    # step (pair densities, 8 rounds, reductions, results to pinned host), device time ---------
+    req = calc.request(specs)
+    v_req = req.run()
+    if not np.allclose(v_req, v32, rtol=1e-9, atol=1e-15):
+        raise RuntimeError("prepared-request results differ from cl_compute")
+    graph = cl.Batch([req])
+    for _ in range(max(3, args.warmup)):
+        graph.run()
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     except Exception:
         pass
     clocks = ClockSampler(uuid)
-    calc.set_profiling(True)
     barrier()
     wall0 = time.perf_counter()
     dev_ms = 0.0
     for _ in range(args.steps):
-        calc.compute(specs)
-        dev_ms += calc.timings()["total_ms"]
+        graph.run()
+        dev_ms += graph.last_ms()
     barrier()
     wall_ms = 1e3 * (time.perf_counter() - wall0)
+    # per-kernel device times: the same request captured with a CUDA-event pair around every
+    # launch, replayed for the same number of steps
+    calc.set_profiling(True)
+    pgraph = cl.Batch([req])
+    pgraph.run()
+    calc.set_profiling(False)
+    calc.set_profiling(True)
+    prof_dev_ms = 0.0
+    for _ in range(args.steps):
+        pgraph.run()
+        prof_dev_ms += pgraph.last_ms()
     prof = calc.kernel_profile()
     calc.set_profiling(False)
     clock_info = clocks.stop()
+    pgraph.close()
+    graph.close()
+    req.close()
     dev_ms = max_over_ranks(dev_ms)
     ms_per_step = dev_ms / args.steps
     value = world * n_int / (ms_per_step / 1e3)
@@ -415,7 +445,21 @@ def run_ours(args):
     # FFT HBM-roofline %: sum of 2*M*s bytes over every 3D transform (8 forward + 8 inverse
     # per prepared density) / time of all transform passes / peak.
     M = int(np.prod(d["dims"]))
-    n_prepared = len({int(s[1]) for s in cl.plan(n, specs)})
+    plan_steps = cl.plan(n, specs)
+    n_prepared = len({int(s[1]) for s in plan_steps})
+    n_right = len({int(s[3]) for s in plan_steps})
+    n_cells = int(np.unique(d["cells_idx"]).size)
+    gram_tc = None
+    if "gram" in prof and "gram_split" in prof:
+        # split-precision Gram: 3 TF32 products of a (2 n_left) x (2 n_right) x atoms real GEMM;
+        # the TF32 tensor rate is half the measured BF16 rate
+        g_ms, g_launches, _ = prof["gram"]
+        flops = 3 * 2.0 * (2 * n_prepared) * (2 * n_right) * n_cells * args.steps
+        tf32_peak = peak_tflops_bf16() / 2
+        gram_tc = {"bound": "tensor", "kernel": "gram", "achieved": flops / (g_ms / 1e3) / 1e12,
+                   "peak": tf32_peak, "unit": "TFLOP/s", "frac": flops / (g_ms / 1e3) / 1e12 / tf32_peak,
+                   "peak_source": "measured BF16 burst / 2 (TF32 rate)",
+                   "flops_per_launch": flops / g_launches, "avg_launch_ms": g_ms / g_launches}
     fft_bytes = args.steps * 16 * n_prepared * 2.0 * M * 8
     buf_mb = n_prepared * M * 8 / 1e6
     total_launches = sum(v[1] for v in prof.values())
@@ -425,10 +469,14 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.config], "integrals_per_step": int(n_int),
-                   "form": "FP32 transforms, FP64 kernel/twiddles/reductions/round sum",
+                   "form": "FP32 transforms; FP64 kernel, twiddles, V accumulation and round sum; split-precision "
+                           "(3xTF32) tensor-core reductions accumulated in FP64",
                    "l2": "inputs larger than L2 (126 MB): %.0f MB of transformed grids per request, "
                          "streamed in chunks" % buf_mb, "prepared_densities": n_prepared,
-                   "init_ms_kernel_build": init_ms, "wall_ms_per_step": wall_ms / args.steps},
+                   "init_ms_kernel_build": init_ms, "wall_ms_per_step": wall_ms / args.steps,
+                   "timing": "device time (CUDA events) of one CUDA-graph replay of the prepared request per "
+                             "step; per-kernel times from the same graph captured with an event pair around "
+                             "every launch (%.3f ms per step)" % (prof_dev_ms / args.steps)},
         "accuracy": accuracy,
         "plain_fp64": {"value": world * n_int / (plain_ms / 1e3), "ms_per_step": plain_ms,
                        "speedup_of_fp32_form": plain_ms / ms_per_step},
@@ -443,6 +491,7 @@ def run_ours(args):
         "fft_share_of_step": fft_ms / (dev_ms if world == 1 else fft_ms + 1e-30),
         "fft_hbm_roofline": {"frac": fft_bytes / (fft_ms / 1e3) / 1e9 / peak,
                              "transforms_per_density": 16, "bytes_per_transform": "2*M*8 (FP32 complex)"},
+        "gram_tensor_roofline": gram_tc,
         "gpu_launches": int(total_launches),
         "clocks": clock_info,
     }

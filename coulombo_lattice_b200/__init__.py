@@ -25,7 +25,7 @@ MODE_FP64_PLAIN = 0
 MODE_FP32_FOURIER = 1
 
 # kernel classes of cl_kernel_profile (include/coulombo_lattice.h CL_KCLASS_*)
-KERNEL_CLASSES = ["pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram", "kernel_build", "spare"]
+KERNEL_CLASSES = ["pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram", "kernel_build", "gram_split"]
 
 _ERR_NAMES = {1: "argument", 2: "state", 3: "cuda", 4: "memory", 5: "unsupported", 6: "timeout"}
 

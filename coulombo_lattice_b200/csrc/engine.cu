@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <array>
 #include <memory>
+#include <mutex>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -9,6 +10,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "coulombo_lattice.h"
@@ -16,6 +19,7 @@
 #include "host/status.hpp"
 #include "kernels.cuh"
 #include "rfft.cuh"
+#include "gram_tc.cuh"
 
 using clk::cx;
 using clk::FftPlan;
@@ -284,6 +288,7 @@ struct cl_ctx {
     DevBuf<cx<double>> req_rho, req_V;
     DevBuf<double> req_o4;
     DevBuf<int> req_ridx;
+    DevBuf<float> tc_buf;  // TF32 hi/lo operands of the tensor-core Gram
     double timings[4] = {0, 0, 0, 0};
 
     // per-kernel profiling (events recorded around launches on `stream`)
@@ -296,6 +301,9 @@ struct cl_ctx {
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<ProfEntry> prof_pending;
+    // while a batch captures this context with profiling on: event pairs go to the batch
+    std::vector<ProfEntry>* prof_sink = nullptr;
+    std::vector<cudaEvent_t>* prof_owned = nullptr;
     double prof_ms[CL_NUM_KCLASS] = {};
     double prof_bytes[CL_NUM_KCLASS] = {};
     int64_t prof_launches[CL_NUM_KCLASS] = {};
@@ -320,6 +328,12 @@ size_t free_device_bytes() {
 }
 
 cudaEvent_t prof_event(cl_ctx* c) {
+    if (c->prof_owned) {  // captured into a graph: the event lives as long as the graph
+        cudaEvent_t e;
+        CL_CUDA(cudaEventCreate(&e));
+        c->prof_owned->push_back(e);
+        return e;
+    }
     if (c->ev_used == c->ev_pool.size()) {
         cudaEvent_t e;
         CL_CUDA(cudaEventCreate(&e));
@@ -329,18 +343,27 @@ cudaEvent_t prof_event(cl_ctx* c) {
 }
 
 // Marks the start of a launch of class `cls`; returns the start event (or nullptr).
+// Inside a capture an event must be recorded as an external event-record node, so that
+// every replay of the graph records it.
+void prof_record(cl_ctx* c, cudaEvent_t e) {
+    if (c->prof_owned)
+        CL_CUDA(cudaEventRecordWithFlags(e, c->stream, cudaEventRecordExternal));
+    else
+        CL_CUDA(cudaEventRecord(e, c->stream));
+}
+
 cudaEvent_t prof_begin(cl_ctx* c) {
     if (!c->profiling) return nullptr;
     cudaEvent_t a = prof_event(c);
-    CL_CUDA(cudaEventRecord(a, c->stream));
+    prof_record(c, a);
     return a;
 }
 
 void prof_end(cl_ctx* c, cudaEvent_t a, int cls, double bytes) {
     if (!a) return;
     cudaEvent_t b = prof_event(c);
-    CL_CUDA(cudaEventRecord(b, c->stream));
-    c->prof_pending.push_back({cls, a, b, bytes});
+    prof_record(c, b);
+    (c->prof_sink ? *c->prof_sink : c->prof_pending).push_back({cls, a, b, bytes});
 }
 
 // After the stream has been synchronised: fold the pending pairs into the totals.
@@ -610,11 +633,148 @@ void run_rounds_mode(cl_ctx* c, const cx<double>* rho, long long rho_stride, int
         run_rounds<float>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride, round_mask);
 }
 
-// out4[l][r] = {sum ac, bd, ad, bc} over atoms (see k_gram).  The register block IB (tile
-// 16*IB) is the one that pads max(nl, nr) least, preferring larger blocks.
+// ---------------------------------------------------------------------------------------
+// Tensor-core Gram (FP32 form): TF32 split pass + tcgen05 GEMM, see gram_tc.cuh.
+// ---------------------------------------------------------------------------------------
+bool use_tc_gram(const cl_ctx* c) { return c->mode == CL_MODE_FP32_FOURIER && !std::getenv("CL_NO_TC_GRAM"); }
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    if (!fn) cl::fail(CL_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+// 2D FP32 tensor [outer][k_pad] viewed in boxes of 32 x box_rows, 128-byte swizzle.
+CUtensorMap tc_tensor_map(float* base, long long k_pad, long long outer, int box_rows) {
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)k_pad * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)clk::tc::BK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) cl::fail(CL_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return m;
+}
+
+struct TcShape {
+    int rowsA = 0, rowsB = 0;
+    long long chunk = 0, k_pad = 0;  // atoms per operand chunk, chunk rounded up to a k-tile
+};
+
+long long tc_bytes_per_atom(int rowsA, int rowsB) { return 2LL * (rowsA + rowsB) * (long long)sizeof(float); }
+
+TcShape tc_shape(const cl_ctx* c, int nl, int nr, long long n_atoms) {
+    TcShape s;
+    s.rowsA = (2 * nl + clk::tc::BM - 1) / clk::tc::BM * clk::tc::BM;
+    s.rowsB = (2 * nr + clk::tc::BN - 1) / clk::tc::BN * clk::tc::BN;
+    const long long per_atom = tc_bytes_per_atom(s.rowsA, s.rowsB);
+    const long long fit = (long long)(c->tc_buf.n * sizeof(float)) / per_atom / clk::tc::BK * clk::tc::BK;
+    const long long full = (n_atoms + clk::tc::BK - 1) / clk::tc::BK * clk::tc::BK;
+    s.k_pad = std::min(full, fit);
+    s.chunk = std::min(n_atoms, s.k_pad);
+    return s;
+}
+
+// Operand buffer for (nl, nr, n_atoms): whole atom range when it fits in a quarter of the free
+// device memory (at most 8 GiB), else chunks of the atom range.  Called outside any capture.
+void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms) {
+    if (!use_tc_gram(c) || nl <= 0 || nr <= 0 || n_atoms <= 0) return;
+    const int rowsA = (2 * nl + clk::tc::BM - 1) / clk::tc::BM * clk::tc::BM;
+    const int rowsB = (2 * nr + clk::tc::BN - 1) / clk::tc::BN * clk::tc::BN;
+    const long long per_atom = tc_bytes_per_atom(rowsA, rowsB);
+    const long long full = (n_atoms + clk::tc::BK - 1) / clk::tc::BK * clk::tc::BK;
+    const long long have = (long long)(c->tc_buf.n * sizeof(float)) / per_atom;
+    if (have >= full) return;
+    const long long budget = std::min<long long>(8LL << 30, (long long)(free_device_bytes() / 4));
+    long long atoms = std::min(full, std::max<long long>(budget / per_atom, 64LL * clk::tc::BK));
+    if (const char* e = std::getenv("CL_TC_MAX_ATOMS"))  // cap per chunk (exercises the chunked path)
+        atoms = std::min(atoms, std::max<long long>(clk::tc::BK, std::atoll(e)));
+    atoms = atoms / clk::tc::BK * clk::tc::BK;
+    if (atoms <= have) return;
+    c->tc_buf.alloc((size_t)(atoms * per_atom / (long long)sizeof(float)));
+}
+
+// out4[l][r] += {sum ac, bd, ad, bc} (out4 zeroed by the caller, error slot included).
+void gram_tc(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<double>* rho, long long r_stride,
+             const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
+    using namespace clk::tc;
+    const TcShape sh = tc_shape(c, nl, nr, n_atoms);
+    if (sh.k_pad < BK) cl::fail(CL_ERR_STATE, "tensor-core Gram operands not reserved");
+    static bool smem_set = false;
+    if (!smem_set) {
+        ensure_smem(clk::tc::k_gram_tc, SMEM_BYTES);
+        smem_set = true;
+    }
+    float* A = c->tc_buf.p;
+    float* B = A + 2LL * sh.rowsA * sh.k_pad;
+    const CUtensorMap mapA = tc_tensor_map(A, sh.k_pad, 2LL * sh.rowsA, BM);
+    const CUtensorMap mapB = tc_tensor_map(B, sh.k_pad, 2LL * sh.rowsB, BN);
+    const int tiles = (sh.rowsA / BM) * (sh.rowsB / BN);
+    for (long long a0 = 0; a0 < n_atoms; a0 += sh.chunk) {
+        const long long na = std::min(sh.chunk, n_atoms - a0);
+        const long long kp = (na + BK - 1) / BK * BK;  // k-tiles that hold atoms of this chunk
+        const int kt_total = (int)(kp / BK);
+        cudaEvent_t e0 = prof_begin(c);
+        const int xblocks = (int)std::min<long long>((kp + 255) / 256, 64);
+        clk::tc::k_tf32_split<<<dim3(xblocks, sh.rowsA / 2), 256, 0, c->stream>>>(V, v_stride, nullptr, nl, sh.rowsA,
+                                                                                 a0, na, sh.k_pad, A);
+        CL_LAUNCHED();
+        clk::tc::k_tf32_split<<<dim3(xblocks, sh.rowsB / 2), 256, 0, c->stream>>>(rho, r_stride, ridx_dev, nr,
+                                                                                 sh.rowsB, a0, na, sh.k_pad, B);
+        CL_LAUNCHED();
+        prof_end(c, e0, CL_KCLASS_GRAM_SPLIT,
+                 (double)(nl + nr) * na * 16.0 + (double)tc_bytes_per_atom(sh.rowsA, sh.rowsB) * kp);
+        // atom splits: whole waves of 148 blocks, each split at least 2 chunks long
+        int best_s = 1;
+        double best = -1e30;
+        const int s_max = std::max(1, std::min(256, kt_total / 16));
+        for (int s = 1; s <= s_max; ++s) {
+            const int per = (kt_total + s - 1) / s;
+            const int used = (kt_total + per - 1) / per;
+            const long long items = (long long)tiles * used;
+            const long long waves = (items + 147) / 148;
+            const double score = (double)items / (double)(waves * 148) - 0.01 * (double)waves;
+            if (score > best) {
+                best = score;
+                best_s = used;
+            }
+        }
+        const int kt_per = (kt_total + best_s - 1) / best_s;
+        const int splits = (kt_total + kt_per - 1) / kt_per;
+        cudaEvent_t e1 = prof_begin(c);
+        clk::tc::k_gram_tc<<<dim3(sh.rowsA / BM, sh.rowsB / BN, splits), THREADS, SMEM_BYTES, c->stream>>>(
+            mapA, mapB, sh.rowsA, sh.rowsB, kt_total, kt_per, nl, nr, out4_dev);
+        CL_LAUNCHED();
+        prof_end(c, e1, CL_KCLASS_GRAM, (double)tc_bytes_per_atom(sh.rowsA, sh.rowsB) * kp);
+    }
+}
+
+// Error slot after the 4 * nl * nr results: non-zero when a device-side wait gave up.
+void check_gram_slot(double slot) {
+    if (slot != 0.0) cl::fail(CL_ERR_TIMEOUT, "tensor-core Gram: a device-side wait timed out");
+}
+
+// out4[l][r] = {sum ac, bd, ad, bc} over atoms (see k_gram); out4 holds 4 * nl * nr + 1
+// doubles, the last one an error slot.  The FP32 form runs the tensor-core Gram; the plain
+// form runs k_gram in FP64, whose register block IB (tile 16*IB) is the one that pads
+// max(nl, nr) least, preferring larger blocks.
 void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<double>* rho, long long r_stride,
           const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
-    CL_CUDA(cudaMemsetAsync(out4_dev, 0, sizeof(double) * 4 * (size_t)nl * nr, c->stream));
+    CL_CUDA(cudaMemsetAsync(out4_dev, 0, sizeof(double) * (4 * (size_t)nl * nr + 1), c->stream));
+    if (use_tc_gram(c)) {
+        gram_tc(c, V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, out4_dev);
+        return;
+    }
     const int pmax = std::max(nl, nr);
     int ib = 4;
     long long best = -1;
@@ -840,14 +1000,16 @@ int cl_calculate_grid(cl_ctx* c, const double* rho2, double out[2]) {
         if (!rho2 || !out) cl::fail(CL_ERR_ARGUMENT, "null argument");
         c->grid_rho2.upload(reinterpret_cast<const cx<double>*>(rho2), c->M, c->stream);
         DevBuf<double> o4;
-        o4.alloc(4);
+        o4.alloc(5);
         DevBuf<int> ridx;
         int zero = 0;
         ridx.upload(&zero, 1, c->stream);
+        tc_reserve(c, 1, 1, c->M);
         gram(c, c->grid_V.p, c->M, 1, c->grid_rho2.p, c->M, ridx.p, 1, c->M, o4.p);
-        double h[4];
+        double h[5];
         CL_CUDA(cudaMemcpyAsync(h, o4.p, sizeof h, cudaMemcpyDeviceToHost, c->stream));
         CL_CUDA(cudaStreamSynchronize(c->stream));
+        check_gram_slot(h[4]);
         out[0] = h[0] - h[1];
         out[1] = h[2] + h[3];
     });
@@ -962,7 +1124,8 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         grow(rho, (size_t)nu * As);
         grow(V, (size_t)nl * As);
         DevBuf<double>& o4 = c->req_o4;
-        grow(o4, (size_t)4 * nl * nr);
+        grow(o4, (size_t)4 * nl * nr + 1);
+        tc_reserve(c, nl, nr, As);
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
         CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)nl * As, c->stream));
@@ -971,9 +1134,10 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
         gram(c, V.p, As, nl, rho.p, As, dr.p, nr, As, o4.p);
         CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
-        std::vector<double> h((size_t)4 * nl * nr);
+        std::vector<double> h((size_t)4 * nl * nr + 1);
         CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CL_CUDA(cudaStreamSynchronize(c->stream));
+        check_gram_slot(h.back());
         float t01, t12, t23, t03;
         CL_CUDA(cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]));
         CL_CUDA(cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]));
@@ -1111,9 +1275,13 @@ struct cl_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double last_ms = 0;
+    // per-launch event pairs captured into the graph for requests whose context profiles
+    std::vector<std::vector<cl_ctx::ProfEntry>> prof;
+    std::vector<cudaEvent_t> prof_events;
     ~cl_batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        for (auto e : prof_events) cudaEventDestroy(e);
         for (auto e : joins) cudaEventDestroy(e);
         if (fork) cudaEventDestroy(fork);
         if (t0) cudaEventDestroy(t0);
@@ -1133,11 +1301,12 @@ void request_enqueue(cl_request* r) {
     CL_CUDA(cudaMemsetAsync(r->V.p, 0, sizeof(cx<double>) * (size_t)r->nl * As, c->stream));
     run_rounds_mode(c, r->rho.p, As, r->nl, c->row_ptr.p, c->cell_sorted.p, r->V.p, As);
     gram(c, r->V.p, As, r->nl, r->rho.p, As, r->ridx.p, r->nr, As, r->o4.p);
-    CL_CUDA(cudaMemcpyAsync(r->o4_host, r->o4.p, sizeof(double) * 4 * (size_t)r->nl * r->nr,
+    CL_CUDA(cudaMemcpyAsync(r->o4_host, r->o4.p, sizeof(double) * (4 * (size_t)r->nl * r->nr + 1),
                             cudaMemcpyDeviceToHost, c->stream));
 }
 
 void request_finish(cl_request* r, double* out) {
+    check_gram_slot(r->o4_host[4 * (size_t)r->nl * r->nr]);
     for (const auto& st : r->plan) {
         const int l = r->slot[st.left.product], rr = r->rcol[st.right.product];
         const double* q = &r->o4_host[((size_t)l * r->nr + rr) * 4];
@@ -1198,8 +1367,9 @@ int cl_request_create(cl_ctx* c, int64_t n_int, const int16_t* spec, cl_request*
         r->ridx.upload(rights.data(), rights.size(), c->stream);
         r->rho.alloc((size_t)prods.size() * As);
         r->V.alloc((size_t)r->nl * As);
-        r->o4.alloc((size_t)4 * r->nl * r->nr);
-        CL_CUDA(cudaMallocHost(&r->o4_host, sizeof(double) * 4 * (size_t)r->nl * r->nr));
+        r->o4.alloc((size_t)4 * r->nl * r->nr + 1);
+        CL_CUDA(cudaMallocHost(&r->o4_host, sizeof(double) * (4 * (size_t)r->nl * r->nr + 1)));
+        tc_reserve(c, r->nl, r->nr, As);
         CL_CUDA(cudaStreamSynchronize(c->stream));
         *out = r;
     });
@@ -1273,10 +1443,14 @@ int cl_batch_run(cl_batch* b, double** outs) {
                     prof_collect(r->ctx);
                     r->warm = true;
                 }
-            std::vector<char> prof(b->reqs.size());
+            // contexts that profile record their launch events inside the graph
+            b->prof.assign(b->reqs.size(), {});
             for (size_t i = 0; i < b->reqs.size(); ++i) {
-                prof[i] = b->reqs[i]->ctx->profiling;
-                b->reqs[i]->ctx->profiling = false;
+                cl_ctx* c = b->reqs[i]->ctx;
+                if (c->profiling) {
+                    c->prof_sink = &b->prof[i];
+                    c->prof_owned = &b->prof_events;
+                }
             }
             CL_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeRelaxed));
             CL_CUDA(cudaEventRecord(b->fork, b->master));
@@ -1288,7 +1462,10 @@ int cl_batch_run(cl_batch* b, double** outs) {
                 CL_CUDA(cudaStreamWaitEvent(b->master, b->joins[i], 0));
             }
             CL_CUDA(cudaStreamEndCapture(b->master, &b->graph));
-            for (size_t i = 0; i < b->reqs.size(); ++i) b->reqs[i]->ctx->profiling = prof[i];
+            for (cl_request* r : b->reqs) {
+                r->ctx->prof_sink = nullptr;
+                r->ctx->prof_owned = nullptr;
+            }
             CL_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
         }
         CL_CUDA(cudaEventRecord(b->t0, b->master));
@@ -1298,6 +1475,17 @@ int cl_batch_run(cl_batch* b, double** outs) {
         float ms = 0;
         CL_CUDA(cudaEventElapsedTime(&ms, b->t0, b->t1));
         b->last_ms = ms;
+        for (size_t i = 0; i < b->reqs.size(); ++i) {
+            cl_ctx* c = b->reqs[i]->ctx;
+            if (!c->profiling) continue;
+            for (const auto& e : b->prof[i]) {
+                float kms = 0;
+                CL_CUDA(cudaEventElapsedTime(&kms, e.a, e.b));
+                c->prof_ms[e.cls] += kms;
+                c->prof_bytes[e.cls] += e.bytes;
+                c->prof_launches[e.cls] += 1;
+            }
+        }
         for (size_t i = 0; i < b->reqs.size(); ++i) request_finish(b->reqs[i], outs[i]);
     });
 }

@@ -1,0 +1,365 @@
+// Split-precision tensor-core Gram over atoms (FP32 form).
+//
+// The reductions of CoulombCalculator::calculate (CoulombCalculator.cpp:165-172), restricted
+// to atom cells and batched over every (left, right) pair of a request, form the real Gram
+//   C = A . B^T,  A rows = {Re V_l, Im V_l} (2 per left density),
+//                 B rows = {Re rho_r, Im rho_r} (2 per right density),  K = atoms,
+// whose 2x2 blocks are {sum ac, sum ad; sum bc, sum bd} for V = a+ib, rho = c+id.
+//
+// Each FP64 operand is split into two TF32 parts, x = hi + lo (both rounded to nearest), and
+// C = A_hi.B_hi + (A_hi.B_lo + A_lo.B_hi) is accumulated by tcgen05 MMAs (kind::tf32, M=128,
+// N=128, K=8) in FP32 in tensor memory.  The tensor cores' FP32 accumulation rounds toward
+// zero, a bias that grows with every MMA added into a running sum.  So the main products and
+// the two correction products (2^-11 smaller) go to separate accumulators, and both are drained
+// into FP64 registers after every k-tile of 32 atoms (double-buffered in tensor memory): the
+// main accumulator takes 4 MMAs between drains.  The drained partial sums are added across the
+// atom range in FP64 and then across atom splits with FP64 atomics.  The dropped lo.lo term and
+// the rounding of the parts are ~2^-22 of each product.
+//
+// Operands are staged by TMA (no multicast) into 128-byte-swizzled shared-memory tiles: one
+// warp issues the copies, one lane issues the MMAs, eight warps drain the accumulator.
+// Every wait is bounded by a clock deadline; on expiry the block records an error in the
+// slot after the results, waits (again bounded) for its own copies and MMAs, frees its
+// tensor memory and returns.
+#pragma once
+
+#include <cuda.h>
+#include <cstdint>
+
+#include "fft.cuh"
+
+namespace clk {
+namespace tc {
+
+constexpr int BM = 128;          // A rows per tile (64 left densities)
+constexpr int BN = 128;          // B rows per tile (64 right densities)
+constexpr int BK = 32;           // atoms per k-tile: 32 x 4 B = one 128-byte swizzle row
+constexpr int STAGES = 3;        // shared-memory pipeline depth
+constexpr int CH = 1;            // k-tiles per FP32 accumulation chunk (32 atoms)
+constexpr int A_BYTES = BM * BK * 4;
+constexpr int B_BYTES = BN * BK * 4;
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // hi and lo of both operands
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int EPI_WARPS = 8;
+constexpr int THREADS = 32 * (2 + EPI_WARPS);
+constexpr uint32_t TMEM_COLS = 4 * BN;  // {main, correction} x double buffer, FP32
+constexpr long long TIMEOUT_CYCLES = 1LL << 32;  // ~2 s at B200 clocks
+
+static_assert(BN == 128 && BM == 128, "epilogue mapping assumes 128x128 tiles");
+
+// Instruction descriptor, kind::tf32: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12
+// = 2), both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase of parity `parity` to complete.  Returns false when the deadline
+// passes (and raises the block's abort flag) or when another role has already aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag) {
+    const long long t0 = clock64();
+    while (!mbar_test(a, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > TIMEOUT_CYCLES) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+// Teardown wait that ignores the abort flag (still bounded).
+__device__ __forceinline__ void mbar_drain(uint32_t a, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_test(a, parity))
+        if (clock64() - t0 > TIMEOUT_CYCLES) return;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major tile with the 128-byte swizzle: start address
+// >> 4, leading offset 1 (unused for swizzled K-major), stride 1024 B between 8-row groups,
+// descriptor version 1 (bit 46), layout type 2 = SWIZZLE_128B (bits 61-63).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive FP32 accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tf32_rn(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// ---------------------------------------------------------------------------------------
+// Split pass: density d of `src` (row idx[d], or d) over atoms [a0, a0 + na) ->
+//   dst[part][2d + {0: re, 1: im}][k], part 0 = hi, 1 = lo; rows >= 2n and k >= na are zero.
+// grid.y = rows_pad / 2 densities, grid.x strides over k.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_tf32_split(const cx<double>* __restrict__ src, long long stride,
+                                                    const int* __restrict__ idx, int n, int rows_pad,
+                                                    long long a0, long long na, long long k_pad,
+                                                    float* __restrict__ dst) {
+    const int d = blockIdx.y;
+    const long long plane = (long long)rows_pad * k_pad;
+    float* hre = dst + (long long)(2 * d) * k_pad;
+    float* him = hre + k_pad;
+    const cx<double>* s = nullptr;
+    if (d < n) s = src + (long long)(idx ? idx[d] : d) * stride + a0;
+    for (long long k = blockIdx.x * 256LL + threadIdx.x; k < k_pad; k += (long long)gridDim.x * 256) {
+        double re = 0.0, im = 0.0;
+        if (s && k < na) {
+            const cx<double> z = s[k];
+            re = z.re;
+            im = z.im;
+        }
+        const float hr = tf32_rn((float)re), hi_ = tf32_rn((float)im);
+        hre[k] = hr;
+        him[k] = hi_;
+        hre[plane + k] = tf32_rn((float)(re - (double)hr));
+        him[plane + k] = tf32_rn((float)(im - (double)hi_));
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// The Gram.  grid = (rowsA / BM, rowsB / BN, splits); block z covers k-tiles
+// [z * kt_per, min(kt_total, (z + 1) * kt_per)), never empty.  out4[l][r] += {ac, bd, ad, bc};
+// out4[4 * nl * nr] (as int) is set to 1 if any wait expired.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(THREADS, 1)
+    k_gram_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int rowsA,
+              int rowsB, int kt_total, int kt_per, int nl, int nr, double* __restrict__ out4) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - raw);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + STAGES * STAGE_BYTES);
+    // bars: full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], drain
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const auto bar = [&](int i) { return smem_u32(bars + i); };
+    const int FULL = 0, EMPTY = STAGES, ACCF = 2 * STAGES, ACCE = 2 * STAGES + 2, DRAIN = 2 * STAGES + 4;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kt0 = blockIdx.z * kt_per;
+    const int kt1 = min(kt_total, kt0 + kt_per);
+    const int nchunks = (kt1 - kt0 + CH - 1) / CH;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(bar(FULL + s), 1);
+            mbar_init(bar(EMPTY + s), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(bar(ACCF + b), 1);
+            mbar_init(bar(ACCE + b), 32 * EPI_WARPS);
+        }
+        mbar_init(bar(DRAIN), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer ----
+            int s = 0;
+            uint32_t ph = 0;
+            int issued = 0;
+            for (int kt = kt0; kt < kt1; ++kt) {
+                if (!mbar_wait(bar(EMPTY + s), ph ^ 1u, abort_flag)) break;
+                const uint32_t st = base + (uint32_t)(s * STAGE_BYTES);
+                mbar_expect_tx(bar(FULL + s), STAGE_BYTES);
+                const int x = kt * BK;
+                tma_load_2d(st, &mapA, x, m0, bar(FULL + s));
+                tma_load_2d(st + A_BYTES, &mapA, x, rowsA + m0, bar(FULL + s));
+                tma_load_2d(st + 2 * A_BYTES, &mapB, x, n0, bar(FULL + s));
+                tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mapB, x, rowsB + n0, bar(FULL + s));
+                ++issued;
+                if (++s == STAGES) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+            }
+            if (*abort_flag) {
+                // let the last (up to STAGES) copies land before the block's memory goes away
+                for (int i = 1; i <= min(issued, STAGES); ++i) {
+                    const int n = issued - i;
+                    mbar_drain(bar(FULL + n % STAGES), (uint32_t)((n / STAGES) & 1));
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer ----
+            int s = 0;
+            uint32_t ph = 0;
+            int kt = kt0;
+            bool issued_any = false;
+            for (int ch = 0; ch < nchunks; ++ch) {
+                const int b = ch & 1;
+                if (!mbar_wait(bar(ACCE + b), (uint32_t)(((ch >> 1) & 1) ^ 1), abort_flag)) break;
+                fence_after();
+                const uint32_t dm = tmem + (uint32_t)(b * 2 * BN);  // main products
+                const uint32_t dc = dm + (uint32_t)BN;                // correction products
+                const int kend = min(kt1, kt + CH);
+                bool ok = true;
+                uint32_t acc = 0;
+                for (; kt < kend; ++kt) {
+                    if (!mbar_wait(bar(FULL + s), ph, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t st = base + (uint32_t)(s * STAGE_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < BK / 8; ++kk) {
+                        const uint64_t ahi = sw128_desc(st + kk * 32);
+                        const uint64_t alo = sw128_desc(st + A_BYTES + kk * 32);
+                        const uint64_t bhi = sw128_desc(st + 2 * A_BYTES + kk * 32);
+                        const uint64_t blo = sw128_desc(st + 2 * A_BYTES + B_BYTES + kk * 32);
+                        mma_tf32(dm, ahi, bhi, acc);
+                        mma_tf32(dc, alo, bhi, acc);
+                        mma_tf32(dc, ahi, blo, 1u);
+                        acc = 1u;
+                    }
+                    issued_any = true;
+                    mma_commit(bar(EMPTY + s));  // the stage is free once these MMAs finish
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(bar(ACCF + b));  // chunk complete in accumulator b
+            }
+            if (*abort_flag && issued_any) {
+                mma_commit(bar(DRAIN));
+                mbar_drain(bar(DRAIN), 0);
+            }
+        }
+    } else {
+        // ---- epilogue: FP32 accumulator -> FP64 registers ----
+        const int q = warp & 3;             // tensor-memory lane quarter this warp may read
+        const int h = (warp - 2) >> 2;      // column half
+        double acc[64];
+#pragma unroll
+        for (int i = 0; i < 64; ++i) acc[i] = 0.0;
+        bool ok = true;
+        for (int ch = 0; ch < nchunks; ++ch) {
+            const int b = ch & 1;
+            bool got = mbar_wait(bar(ACCF + b), (uint32_t)((ch >> 1) & 1), abort_flag);
+            got = __all_sync(0xffffffffu, got);
+            if (!got) {
+                ok = false;
+                break;
+            }
+            fence_after();
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * 2 * BN + h * 64);
+            float v[32];
+#pragma unroll
+            for (int part = 0; part < 4; ++part) {  // main, main+32, correction, correction+32
+                tmem_ld32(ta + (uint32_t)((part >> 1) * BN + (part & 1) * 32), v);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) acc[(part & 1) * 32 + i] += (double)v[i];
+            }
+            fence_before();
+            mbar_arrive(bar(ACCE + b));
+        }
+        if (ok) {
+            const int R = m0 + 32 * q + lane;
+            const int l = R >> 1, pa = R & 1;
+            if (l < nl) {
+#pragma unroll
+                for (int j = 0; j < 64; ++j) {
+                    const int Cg = n0 + h * 64 + j;
+                    const int r = Cg >> 1, pc = Cg & 1;
+                    if (r < nr) {
+                        const int qi = (pa == pc) ? pa : 2 + pa;  // ac, bd, ad, bc
+                        atomicAdd(out4 + ((long long)l * nr + r) * 4 + qi, acc[j]);
+                    }
+                }
+            }
+        }
+    }
+
+    fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag)
+        *reinterpret_cast<volatile int*>(out4 + (long long)4 * nl * nr) = 1;
+    if (warp == 1) {
+        __syncwarp();
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+}  // namespace tc
+}  // namespace clk

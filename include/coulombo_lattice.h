@@ -130,8 +130,9 @@ int cl_last_timings(cl_ctx* ctx, double t[4]);
 #define CL_KCLASS_YPASS     2  /* FFT along y (both directions) */
 #define CL_KCLASS_ZPASS     3  /* FFT along z, x Khat, inverse FFT along z */
 #define CL_KCLASS_XINV      4  /* inverse FFT along x + phase + accumulate V at atoms */
-#define CL_KCLASS_GRAM      5  /* FP64 real-space reductions */
+#define CL_KCLASS_GRAM      5  /* real-space reductions: FP64 Gram (plain) or tensor-core Gram (FP32 form) */
 #define CL_KCLASS_KERNEL    6  /* Coulomb kernel octant, DCT-I, folded kernels */
+#define CL_KCLASS_GRAM_SPLIT 7 /* TF32 hi/lo operand split of the tensor-core Gram (FP32 form) */
 #define CL_NUM_KCLASS       8
 /* enable != 0 starts recording (and clears the counters); 0 stops. */
 int cl_set_profiling(cl_ctx* ctx, int enable);

@@ -1,0 +1,121 @@
+"""The split-precision tensor-core Gram of the FP32 form (TF32 hi/lo operands, tcgen05 MMAs,
+FP64 accumulation across 64-atom chunks) against the FP64 Gram on the same potentials and
+against the oracle."""
+import numpy as np
+import pytest
+
+import coulombo_lattice_b200 as cl
+from coulombo_lattice_b200 import synth
+from oracle import host as H
+
+pytestmark = pytest.mark.gpu
+
+STEP = (synth.A_ZB / 4,) * 3
+
+
+def _run(d, specs, holes, env=None, monkeypatch=None, profile=False):
+    if env:
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+    try:
+        with cl.CoulombCalculator(d["dims"], STEP, cl.MODE_FP32_FOURIER) as cc:
+            cc.initialize(dielectric=10.89)
+            cc.set_states(d["states"], d["cells_idx"], holes)
+            if profile:
+                cc.set_profiling(True)
+            got = cc.compute(specs)
+            prof = cc.kernel_profile() if profile else None
+    finally:
+        if env:
+            for k in env:
+                monkeypatch.delenv(k, raising=False)
+    return got, prof
+
+
+def _oracle(d, specs):
+    return np.array(H.compute_integrals(list(d["states"]), d["cells_idx"], d["dims"], STEP, specs,
+                                        dielectric=10.89))
+
+
+def _check(got, ref, want, frac):
+    """got (tensor-core Gram) vs ref (FP64 Gram, same potentials): within `frac` of the FP32
+    gate; got vs the FP64 oracle: within the gate max(1e-6 |I|, 1e-9 eV)."""
+    lim = np.maximum(1e-6 * np.abs(want), 1e-9)
+    assert np.all(np.abs(got - ref) <= frac * lim), (np.abs(got - ref) / lim).max()
+    assert np.all(np.abs(got - want) <= lim), (np.abs(got - want) / lim).max()
+
+
+def test_tensor_core_gram_is_used_and_accurate(monkeypatch):
+    d = synth.build("c1")
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    got, prof = _run(d, specs, 2, profile=True)
+    assert "gram_split" in prof and prof["gram"][1] >= 1
+    ref, prof64 = _run(d, specs, 2, env={"CL_NO_TC_GRAM": "1"}, monkeypatch=monkeypatch, profile=True)
+    assert "gram_split" not in prof64
+    _check(got, ref, _oracle(d, specs), 0.25)
+
+
+def test_several_tiles_of_densities(monkeypatch):
+    """12 states -> 78 pair densities on both sides: 2 x 2 tiles of 64 densities, with padding."""
+    d = synth.build("c2", cells=(5, 5, 4))
+    d["states"] = d["states"][:, :, :8]
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 12, 6)][::7]
+    got, _ = _run(d, specs, 6)
+    ref, _ = _run(d, specs, 6, env={"CL_NO_TC_GRAM": "1"}, monkeypatch=monkeypatch)
+    _check(got, ref, _oracle(d, specs), 0.25)
+
+
+def test_chunked_atom_range(monkeypatch):
+    """Operands staged in 1,024-atom chunks (and a ragged last chunk) give the same sums."""
+    d = synth.build("c1", cells=(8, 8, 5))
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("eeee,hhhh,ehhe,eheh", 4, 2)]
+    whole, _ = _run(d, specs, 2)
+    chunked, _ = _run(d, specs, 2, env={"CL_TC_MAX_ATOMS": "1000"}, monkeypatch=monkeypatch)
+    assert np.abs(chunked - whole).max() <= 1e-9 * np.abs(whole).max()
+
+
+def test_grid_calculate_uses_tensor_core_gram():
+    """calculate() on the grid API (one left, one right density, every cell) in the FP32 form."""
+    from oracle import coulomb as C
+    rng = np.random.default_rng(11)
+    dims = (24, 20, 18)
+    F = rng.normal(size=dims[::-1]) + 1j * rng.normal(size=dims[::-1])
+    F2 = rng.normal(size=dims[::-1]) + 1j * rng.normal(size=dims[::-1])
+    g = C.kernel_octant(dims, (1.0, 1.0, 1.0), 1.0, 0.0)
+    V = C.prepare(F, C.kernel_spectrum(g, dims))
+    want = C.calculate(V, F2)
+    with cl.CoulombCalculator(dims, (1.0, 1.0, 1.0), cl.MODE_FP32_FOURIER) as cc:
+        cc.initialize(dielectric=1.0)
+        cc.prepare(F)
+        got = cc.calculate(F2)
+    assert abs(got - want) <= 1e-6 * np.abs(V).max() * np.abs(F2).sum()
+
+
+def test_profile_recorded_inside_graph():
+    """A batch captured while its context profiles records an event pair around every launch in
+    the graph; each replay adds one request's launches, the same classes as an eager request."""
+    d = synth.build("c1", cells=(4, 4, 4))
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    with cl.CoulombCalculator(d["dims"], STEP, cl.MODE_FP32_FOURIER) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], 2)
+        req = cc.request(specs)
+        want = req.run()
+        cc.set_profiling(True)
+        req.run()
+        eager = cc.kernel_profile()
+        b = cl.Batch([req])
+        b.run()
+        cc.set_profiling(False)
+        cc.set_profiling(True)
+        for _ in range(3):
+            got = b.run()[0]
+        prof = cc.kernel_profile()
+        cc.set_profiling(False)
+        b.close()
+        req.close()
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=0)
+    assert set(prof) == set(eager)
+    for k, (ms, n, nbytes) in prof.items():
+        assert n == 3 * eager[k][1] and ms > 0
+        assert nbytes == pytest.approx(3 * eager[k][2])
