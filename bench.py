@@ -50,7 +50,22 @@ def parse_args():
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", default=None,
+                    help="Lx,Ly,Lz conventional cells instead of the workload's own box (a smaller case of the "
+                         "same states and integral list, for profiler captures); the JSON line then names it")
     return ap.parse_args()
+
+
+def cells_arg(args):
+    return tuple(int(v) for v in args.cells.split(",")) if args.cells else None
+
+
+def workload_name(args):
+    if not args.cells:
+        return WORKLOADS[args.config]
+    L = cells_arg(args)
+    return "%s states and integrals on a zinc-blende %dx%dx%d-cell box (%dx%dx%d grid, %d atoms)" % (
+        args.config, L[0], L[1], L[2], 4 * L[0], 4 * L[1], 4 * L[2], 8 * L[0] * L[1] * L[2])
 
 
 def dist_env():
@@ -131,10 +146,10 @@ class ClockSampler:
 # ----------------------------------------------------------------------------------------
 # workload
 # ----------------------------------------------------------------------------------------
-def build_workload(config, seed_index=None):
+def build_workload(config, seed_index=None, cells=None):
     from coulombo_lattice_b200 import synth
     import coulombo_lattice_b200 as cl
-    d = synth.build(config, seed_index=seed_index)
+    d = synth.build(config, cells=cells, seed_index=seed_index)
     n = d["states"].shape[0]
     d["specs"] = np.ascontiguousarray(cl.enumerate_integrals(d["integrals"], n, d["holes"]))
     d["step"] = (synth.A_ZB / 4,) * 3
@@ -197,7 +212,7 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    d = build_workload(args.config)
+    d = build_workload(args.config, cells=cells_arg(args))
     threads = os.cpu_count() or 1
     n_left = {"c1": 2, "c2": 2, "c3": 1, "c4": 1}[args.config]
     for _ in range(args.warmup):
@@ -212,7 +227,7 @@ def run_reference(args):
         "impl": "reference", "metric": "integrals/s", "value": value, "unit": "integrals/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * len(d["specs"]) / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.config], "integrals_per_step": int(len(d["specs"]))},
+        "config": {"workload": workload_name(args), "integrals_per_step": int(len(d["specs"]))},
         "cpu_baseline": {"value": value, "unit": "integrals/s", "cores": threads, "kind": "port",
                          "sample": "each step: %d of %d prepared densities of the oracle's reference-structured "
                                    "FP64 loop, extrapolated to the full request; median of %d steps"
@@ -324,7 +339,8 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    d = build_workload(args.config, seed_index=(int(args.config[1:]) + 1000 * rank) if rank else None)
+    d = build_workload(args.config, seed_index=(int(args.config[1:]) + 1000 * rank) if rank else None,
+                       cells=cells_arg(args))
     n = d["states"].shape[0]
     specs = d["specs"]
     n_int = specs.shape[0]
@@ -468,7 +484,7 @@ def run_ours(args):
         "metric": "integrals/s", "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.config], "integrals_per_step": int(n_int),
+        "config": {"workload": workload_name(args), "integrals_per_step": int(n_int),
                    "form": "FP32 transforms; FP64 kernel, twiddles, V accumulation and round sum; split-precision "
                            "(3xTF32) tensor-core reductions accumulated in FP64",
                    "l2": "inputs larger than L2 (126 MB): %.0f MB of transformed grids per request, "

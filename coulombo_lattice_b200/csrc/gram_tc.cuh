@@ -9,11 +9,13 @@
 // Each FP64 operand is split into two TF32 parts, x = hi + lo (both rounded to nearest), and
 // C = A_hi.B_hi + (A_hi.B_lo + A_lo.B_hi) is accumulated by tcgen05 MMAs (kind::tf32, M=128,
 // N=128, K=8) in FP32 in tensor memory.  The tensor cores' FP32 accumulation rounds toward
-// zero, a bias that grows with every MMA added into a running sum.  So the main products and
-// the two correction products (2^-11 smaller) go to separate accumulators, and both are drained
-// into FP64 registers after every k-tile of 32 atoms (double-buffered in tensor memory): the
-// main accumulator takes 4 MMAs between drains.  The drained partial sums are added across the
-// atom range in FP64 and then across atom splits with FP64 atomics.  The dropped lo.lo term and
+// zero, a bias that grows with every MMA added into a running sum.  So the main products go to
+// an accumulator that is drained into FP64 registers after every k-tile of 32 atoms (4 MMAs,
+// double-buffered in tensor memory), while the two correction products -- 2^-11 of the main
+// ones and of random sign, the lo parts being round-to-nearest residuals -- accumulate in a
+// third accumulator over the block's whole atom range and are drained once.  The drained
+// partial sums are added across the atom range in FP64 and then across atom splits with FP64
+// atomics.  The dropped lo.lo term and
 // the rounding of the parts are ~2^-22 of each product.
 //
 // Operands are staged by TMA (no multicast) into 128-byte-swizzled shared-memory tiles: one
@@ -42,7 +44,7 @@ constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // hi and lo of both ope
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
-constexpr uint32_t TMEM_COLS = 4 * BN;  // {main, correction} x double buffer, FP32
+constexpr uint32_t TMEM_COLS = 4 * BN;  // main x double buffer, correction, unused; FP32
 constexpr long long TIMEOUT_CYCLES = 1LL << 32;  // ~2 s at B200 clocks
 
 static_assert(BN == 128 && BM == 128, "epilogue mapping assumes 128x128 tiles");
@@ -267,8 +269,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int b = ch & 1;
                 if (!mbar_wait(bar(ACCE + b), (uint32_t)(((ch >> 1) & 1) ^ 1), abort_flag)) break;
                 fence_after();
-                const uint32_t dm = tmem + (uint32_t)(b * 2 * BN);  // main products
-                const uint32_t dc = dm + (uint32_t)BN;                // correction products
+                const uint32_t dm = tmem + (uint32_t)(b * BN);  // main products of this chunk
+                const uint32_t dc = tmem + (uint32_t)(2 * BN);  // correction products, whole range
                 const int kend = min(kt1, kt + CH);
                 bool ok = true;
                 uint32_t acc = 0;
@@ -286,7 +288,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         const uint64_t bhi = sw128_desc(st + 2 * A_BYTES + kk * 32);
                         const uint64_t blo = sw128_desc(st + 2 * A_BYTES + B_BYTES + kk * 32);
                         mma_tf32(dm, ahi, bhi, acc);
-                        mma_tf32(dc, alo, bhi, acc);
+                        mma_tf32(dc, alo, bhi, (ch > 0 || acc) ? 1u : 0u);
                         mma_tf32(dc, ahi, blo, 1u);
                         acc = 1u;
                     }
@@ -322,16 +324,28 @@ __global__ void __launch_bounds__(THREADS, 1)
                 break;
             }
             fence_after();
-            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * 2 * BN + h * 64);
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * BN + h * 64);
             float v[32];
+            tmem_ld32(ta, v);
 #pragma unroll
-            for (int part = 0; part < 4; ++part) {  // main, main+32, correction, correction+32
-                tmem_ld32(ta + (uint32_t)((part >> 1) * BN + (part & 1) * 32), v);
+            for (int i = 0; i < 32; ++i) acc[i] += (double)v[i];
+            tmem_ld32(ta + 32, v);
 #pragma unroll
-                for (int i = 0; i < 32; ++i) acc[(part & 1) * 32 + i] += (double)v[i];
-            }
+            for (int i = 0; i < 32; ++i) acc[32 + i] += (double)v[i];
             fence_before();
             mbar_arrive(bar(ACCE + b));
+        }
+        if (ok) {
+            // the correction accumulator is complete with the last chunk's commit
+            fence_after();
+            const uint32_t tc_ = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(2 * BN + h * 64);
+            float v[32];
+            tmem_ld32(tc_, v);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] += (double)v[i];
+            tmem_ld32(tc_ + 32, v);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[32 + i] += (double)v[i];
         }
         if (ok) {
             const int R = m0 + 32 * q + lane;
