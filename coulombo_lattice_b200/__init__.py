@@ -25,7 +25,8 @@ MODE_FP64_PLAIN = 0
 MODE_FP32_FOURIER = 1
 
 # kernel classes of cl_kernel_profile (include/coulombo_lattice.h CL_KCLASS_*)
-KERNEL_CLASSES = ["pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram", "kernel_build", "gram_split"]
+KERNEL_CLASSES = ["pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram", "kernel_build", "gram_split",
+                  "round_sum", "spare"]
 
 _ERR_NAMES = {1: "argument", 2: "state", 3: "cuda", 4: "memory", 5: "unsupported", 6: "timeout"}
 
@@ -263,11 +264,12 @@ class CoulombCalculator:
 
     def kernel_profile(self):
         """{class: (ms, launches, algorithmic bytes)} since profiling was switched on."""
-        ms = np.zeros(8)
-        n = np.zeros(8, dtype=np.int64)
-        b = np.zeros(8)
+        k = len(KERNEL_CLASSES)
+        ms = np.zeros(k)
+        n = np.zeros(k, dtype=np.int64)
+        b = np.zeros(k)
         _check(lib().cl_kernel_profile(self._h, _ptr(ms), _ptr(n, ctypes.c_int64), _ptr(b)))
-        return {KERNEL_CLASSES[k]: (float(ms[k]), int(n[k]), float(b[k])) for k in range(8) if n[k]}
+        return {KERNEL_CLASSES[k]: (float(ms[k]), int(n[k]), float(b[k])) for k in range(len(KERNEL_CLASSES)) if n[k]}
 
     def set_states_raw(self, n_states, n_holes, n_atoms, n_orb, coeff_ptr, cells_ptr):
         """cl_set_states on raw host addresses (e.g. pinned buffers)."""

@@ -285,6 +285,7 @@ struct cl_ctx {
 
     // work buffers, kept across requests (grown on demand)
     DevBuf<unsigned char> work;
+    DevBuf<unsigned char> rounds;  // per-round values at the atoms of a chunk of densities
     DevBuf<cx<double>> req_rho, req_V;
     DevBuf<double> req_o4;
     DevBuf<int> req_ridx;
@@ -489,8 +490,8 @@ bool launch_xfwd_rf(cl_ctx* c, const cx<double>* rho, long long rho_stride, cons
 }
 
 template <typename T>
-bool launch_xinv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const clk::RoundPhase& rp, const int* row_ptr,
-                    const int* cell, cx<double>* V, long long v_stride, int nx, int ny, int nrows, int cnt) {
+bool launch_xinv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const int* row_ptr, const int* cell, cx<T>* out,
+                    long long o_stride, int nx, int nrows, int cnt) {
     if (std::getenv("CL_NO_REGISTER_FFT")) return false;
     constexpr int LR = sizeof(T) == 4 ? 16 : 8;
     return clk::with_split2(nx, [&](auto tag) {
@@ -502,7 +503,7 @@ bool launch_xinv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const clk::RoundPhas
         ensure_smem(kern, smem);
         const long long blocks = (nrows + LR - 1) / LR;
         kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), LR * Q, smem, c->stream>>>(
-            buf, c->M, tw, rp, row_ptr, cell, V, v_stride, ny, nrows, cnt);
+            buf, c->M, tw, row_ptr, cell, out, o_stride, nrows, cnt);
     });
 }
 
@@ -511,8 +512,10 @@ long long row_ptr_count(cl_ctx* c, const int* row_ptr) {
     return row_ptr == c->row_ptr.p ? c->n_sorted : c->M;
 }
 
-// One request's transforms: for every density p in [0, np) (rho rows), V[p] += the 8-round
-// convolution at the atoms of the row CSR.  buf holds `chunk` grids of type T.
+// One request's transforms: for every density p in [0, np) (rho rows), V[p] = the 8-round
+// convolution (the rounds of round_mask) at the atoms of the row CSR.  For a chunk of densities,
+// each round's inverse x pass writes its values at the atoms (type T) to a slot of the rounds
+// buffer; k_round_sum then forms V in FP64.  buf holds `chunk` grids of type T.
 template <typename T>
 void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, const int* row_ptr,
                 const int* cell, cx<double>* V, long long v_stride, int round_mask) {
@@ -523,13 +526,23 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     // Densities per chunk.  When a few grids fit in L2, chunks are sized so that the passes of
     // one round hand their output to the next pass through L2; otherwise chunks are as large
     // as 60% of the free memory allows (fewer, larger launches and Khat reuse in the z pass).
+    const long long n_at = row_ptr_count(c, row_ptr);
+    const int n_rounds = __builtin_popcount(round_mask & 0xFF);
+    if (n_rounds == 0) {  // no round of this share (a split over more ranks than rounds)
+        CL_CUDA(cudaMemset2DAsync(V, sizeof(cx<double>) * v_stride, 0, sizeof(cx<double>) * n_at, np, c->stream));
+        return;
+    }
+    const size_t round_bytes = sizeof(cx<T>) * (size_t)n_at * n_rounds;  // per density
     const size_t l2_budget = l2_chunk_bytes();
-    size_t budget = (size_t)(0.6 * (double)(free_device_bytes() + c->work.n));
-    size_t by_mem = std::max<size_t>(1, budget / grid_bytes);
+    size_t budget = (size_t)(0.6 * (double)(free_device_bytes() + c->work.n + c->rounds.n));
+    size_t by_mem = std::max<size_t>(1, budget / (grid_bytes + round_bytes));
     size_t by_l2 = l2_budget / grid_bytes;
     int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)np, by_l2 >= 2 ? by_l2 : by_mem));
     c->work.alloc(std::max(c->work.n, (size_t)chunk * grid_bytes));
+    c->rounds.alloc(std::max(c->rounds.n, (size_t)chunk * round_bytes));
     cx<T>* buf = reinterpret_cast<cx<T>*>(c->work.p);
+    cx<T>* tr = reinterpret_cast<cx<T>*>(c->rounds.p);
+    const long long tr_slot = (long long)chunk * n_at;  // elements per round slot
 
     const Axis& X = c->ax[0];
     const Axis& Y = c->ax[1];
@@ -572,8 +585,10 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
         const int cnt = std::min(chunk, np - p0);
         const cx<double>* rho_c = rho + (long long)p0 * rho_stride;
         cx<double>* V_c = V + (long long)p0 * v_stride;
+        int slot = 0;
         for (int r = 0; r < 8; ++r) {
             if (!((round_mask >> r) & 1)) continue;
+            cx<T>* tr_r = tr + slot++ * tr_slot;
             clk::RoundPhase rp{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, r & 1, (r >> 1) & 1,
                                (r >> 2) & 1};
             const T* kh = sizeof(T) == 4 ? (const T*)c->khat32[r].p : (const T*)c->khat64[r].p;
@@ -614,13 +629,24 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
             e = prof_begin(c);
             if (pt.fits) {
                 clk::k_xyinv<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
-                    buf, c->M, X.plan, Y.plan, twx, twy, rp, row_ptr, cell, V_c, v_stride, nx, ny, pt.ld);
-            } else if (!launch_xinv_rf<T>(c, buf, twx, rp, row_ptr, cell, V_c, v_stride, nx, ny, nrows, cnt)) {
-                clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, rp, row_ptr, cell, V_c,
-                                                                     v_stride, nx, ny, nrows, xt.rows, xt.ld, cnt);
+                    buf, c->M, X.plan, Y.plan, twx, twy, row_ptr, cell, tr_r, n_at, nx, ny, pt.ld);
+            } else if (!launch_xinv_rf<T>(c, buf, twx, row_ptr, cell, tr_r, n_at, nx, nrows, cnt)) {
+                clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, row_ptr, cell, tr_r,
+                                                                     n_at, nx, nrows, xt.rows, xt.ld, cnt);
             }
             CL_LAUNCHED();
-            prof_end(c, e, CL_KCLASS_XINV, cnt * (row_side * gbytes + atoms * 32.0) + atoms * 4.0);
+            prof_end(c, e, CL_KCLASS_XINV,
+                     cnt * (row_side * gbytes + atoms * (double)sizeof(cx<T>)) + atoms * 4.0);
+        }
+        if (n_rounds > 0) {
+            const clk::RoundPhase base{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
+            const int blocks = (int)std::min<long long>((n_at + 255) / 256, 148LL * 16);
+            cudaEvent_t e = prof_begin(c);
+            clk::k_round_sum<T><<<blocks, 256, 0, c->stream>>>(tr, tr_slot, n_at, round_mask & 0xFF, base, cell, nx,
+                                                              ny, n_at, V_c, v_stride, cnt);
+            CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_ROUND_SUM,
+                     cnt * atoms * (n_rounds * (double)sizeof(cx<T>) + 16.0) + atoms * 4.0);
         }
     }
 }
@@ -986,7 +1012,6 @@ int cl_prepare_grid(cl_ctx* c, const double* rho) {
         identity_atoms(c);
         c->grid_rho.upload(reinterpret_cast<const cx<double>*>(rho), c->M, c->stream);
         c->grid_V.alloc(c->M);
-        CL_CUDA(cudaMemsetAsync(c->grid_V.p, 0, sizeof(cx<double>) * c->M, c->stream));
         run_rounds_mode(c, c->grid_rho.p, c->M, 1, c->grid_row_ptr.p, c->grid_cell.p, c->grid_V.p, c->M);
         CL_CUDA(cudaStreamSynchronize(c->stream));
         c->grid_prepared = true;
@@ -1128,7 +1153,6 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         tc_reserve(c, nl, nr, As);
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
-        CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)nl * As, c->stream));
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
         run_rounds_mode(c, rho.p, As, nl, c->row_ptr.p, c->cell_sorted.p, V.p, As, round_mask);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
@@ -1225,7 +1249,6 @@ int cl_potentials(cl_ctx* c, double* out) {
         V.alloc((size_t)n * As);
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
-        CL_CUDA(cudaMemsetAsync(V.p, 0, sizeof(cx<double>) * (size_t)n * As, c->stream));
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
         run_rounds_mode(c, rho.p, As, n, c->row_ptr.p, c->cell_sorted.p, V.p, As);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
@@ -1298,7 +1321,6 @@ void request_enqueue(cl_request* r) {
     cl_ctx* c = r->ctx;
     const long long As = c->n_sorted;
     pair_launch(c, r->ps, r->rho.p);
-    CL_CUDA(cudaMemsetAsync(r->V.p, 0, sizeof(cx<double>) * (size_t)r->nl * As, c->stream));
     run_rounds_mode(c, r->rho.p, As, r->nl, c->row_ptr.p, c->cell_sorted.p, r->V.p, As);
     gram(c, r->V.p, As, r->nl, r->rho.p, As, r->ridx.p, r->nr, As, r->o4.p);
     CL_CUDA(cudaMemcpyAsync(r->o4_host, r->o4.p, sizeof(double) * (4 * (size_t)r->nl * r->nr + 1),

@@ -336,16 +336,15 @@ __global__ void __launch_bounds__(256) k_zpass(cx<T>* __restrict__ buf, long lon
 }
 
 // ---------------------------------------------------------------------------------------
-// Last pass: inverse FFT along x, x phase_kappa, V(atom) += value (FP64).  Each atom's row
-// belongs to exactly one block, and rounds are ordered on the stream, so the accumulation
-// needs no atomics.
+// Last pass: inverse FFT along x; the round's value at every atom of the rows is written to
+// out[p][atom] (write-only, the pass's working precision).  k_round_sum multiplies by
+// phase_kappa and adds the rounds in FP64.
 // ---------------------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_xinv(const cx<T>* __restrict__ buf, long long stride, FftPlan plan,
-                                             const cx<T>* __restrict__ tw_g, RoundPhase rp,
-                                             const int* __restrict__ row_ptr, const int* __restrict__ cell,
-                                             cx<double>* __restrict__ V, long long v_stride, int nx, int ny,
-                                             int nrows, int rows, int ld, int np) {
+                                             const cx<T>* __restrict__ tw_g, const int* __restrict__ row_ptr,
+                                             const int* __restrict__ cell, cx<T>* __restrict__ out,
+                                             long long o_stride, int nx, int nrows, int rows, int ld, int np) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* a = tw + nx;
@@ -362,12 +361,11 @@ __global__ void __launch_bounds__(256) k_xinv(const cx<T>* __restrict__ buf, lon
         }
         __syncthreads();
         const cx<T>* res = fft_lines<+1>(a, b, tw, plan, rows, ld);
-        cx<double>* vp = V + (long long)p * v_stride;
+        cx<T>* op = out + (long long)p * o_stride;
         for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
             const int c = cell[i];
             const int row = c / nx, x = c - row * nx;
-            const int y = row % ny, z = row / ny;
-            vp[i] = vp[i] + cmul(widen(res[x * ld + (row - r0)]), round_phase(rp, x, y, z));
+            op[i] = res[x * ld + (row - r0)];
         }
         __syncthreads();
     }
@@ -376,8 +374,8 @@ __global__ void __launch_bounds__(256) k_xinv(const cx<T>* __restrict__ buf, lon
 // ---------------------------------------------------------------------------------------
 // Fused x+y passes for planes that fit in shared memory: block = (z-plane, density).
 // Forward: scatter the plane's atoms x conj(phase), FFT along x then y in place, store the
-// plane (one HBM write).  Inverse: load the plane, inverse FFT along y then x, multiply by
-// the phase and accumulate V at the plane's atoms (one HBM read).  The plane sits in shared
+// plane (one HBM write).  Inverse: load the plane, inverse FFT along y then x, and write the
+// round's value at the plane's atoms (one HBM read).  The plane sits in shared
 // memory as [y][ld] with ld odd, so row and column transforms are both free of bank
 // conflicts.
 // ---------------------------------------------------------------------------------------
@@ -419,10 +417,9 @@ __global__ void __launch_bounds__(512, 1) k_xyfwd(const cx<double>* __restrict__
 template <typename T, int VALS>
 __global__ void __launch_bounds__(512, 1) k_xyinv(const cx<T>* __restrict__ buf, long long stride, FftPlan px,
                                               FftPlan py, const cx<T>* __restrict__ twx_g,
-                                              const cx<T>* __restrict__ twy_g, RoundPhase rp,
-                                              const int* __restrict__ row_ptr, const int* __restrict__ cell,
-                                              cx<double>* __restrict__ V, long long v_stride, int nx, int ny,
-                                              int ld) {
+                                              const cx<T>* __restrict__ twy_g, const int* __restrict__ row_ptr,
+                                              const int* __restrict__ cell, cx<T>* __restrict__ out,
+                                              long long o_stride, int nx, int ny, int ld) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* twx = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* twy = twx + nx;
@@ -440,12 +437,53 @@ __global__ void __launch_bounds__(512, 1) k_xyinv(const cx<T>* __restrict__ buf,
     plane_axis<+1, VALS>(pl, twx, nx, ny, ld, 1);
     const int r0 = z * ny;
     const int a0 = row_ptr[r0], a1 = row_ptr[r0 + ny];
-    cx<double>* vp = V + (long long)p * v_stride;
+    cx<T>* op = out + (long long)p * o_stride;
     for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
         const int c = cell[i];
         const int row = c / nx, x = c - row * nx;
         const int y = row - r0;
-        vp[i] = vp[i] + cmul(widen(pl[y * ld + x]), round_phase(rp, x, y, z));
+        op[i] = pl[y * ld + x];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Round sum (CoulombCalculator.cpp:155-160, V += T . phi over the rounds): for every atom i
+// and density p, V[p][i] = sum over the rounds present, in ascending kappa, of
+// widen(t_kappa[p][i]) x phase_kappa(cell i), in FP64.  The rounds' values t_kappa come from the
+// inverse x pass (slot s = kappa's rank among the present rounds; slot stride r_stride).  A
+// thread owns one atom: its (at most 8) phases are formed once and reused for every density.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_round_sum(const cx<T>* __restrict__ t, long long r_stride,
+                                                  long long p_stride, int round_mask, RoundPhase base,
+                                                  const int* __restrict__ cell, int nx, int ny, long long n_atoms,
+                                                  cx<double>* __restrict__ V, long long v_stride, int np) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_atoms;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c = cell[i];
+        const int row = c / nx, x = c - row * nx;
+        const int y = row % ny, z = row / ny;
+        cx<double> ph[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            RoundPhase rp = base;
+            rp.kx = r & 1;
+            rp.ky = (r >> 1) & 1;
+            rp.kz = (r >> 2) & 1;
+            ph[r] = round_phase(rp, x, y, z);
+        }
+        for (int p = 0; p < np; ++p) {
+            const cx<T>* tp = t + (long long)p * p_stride + i;
+            cx<double> acc = mk(0.0, 0.0);
+            long long s = 0;
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if ((round_mask >> r) & 1) {
+                    acc = acc + cmul(widen(tp[s]), ph[r]);
+                    s += r_stride;
+                }
+            V[(long long)p * v_stride + i] = acc;
+        }
     }
 }
 

@@ -58,12 +58,18 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2
     __syncthreads();
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
+    // the next density's column is loaded into registers while the current one is transformed
+    const auto load = [&](int p, cx<T>(&v)[R1]) {
+        const cx<T>* src = buf + (long long)p * stride + c;
+#pragma unroll
+        for (int j = 0; j < R1; ++j) v[j] = valid ? src[(long long)(q + R2 * j) * nxy] : mk(T(0), T(0));
+    };
+    cx<T> v[R1], vn[R1];
+    if (q < R2 && p_begin < p_end) load(p_begin, v);
     for (int p = p_begin; p < p_end; ++p) {
         cx<T>* base = buf + (long long)p * stride + c;
+        if (q < R2 && p + 1 < p_end) load(p + 1, vn);
         if (q < R2) {
-            cx<T> v[R1];
-#pragma unroll
-            for (int j = 0; j < R1; ++j) v[j] = valid ? base[(long long)(q + R2 * j) * nxy] : mk(T(0), T(0));
             dft<R1, -1>(v);
 #pragma unroll
             for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * L + line] = v[r];
@@ -95,6 +101,8 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2
                 for (int r = 0; r < R1; ++r) base[(long long)(q + R2 * r) * nxy] = w[r];
             }
         }
+#pragma unroll
+        for (int j = 0; j < R1; ++j) v[j] = vn[j];
     }
 }
 
@@ -136,15 +144,21 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2
     __syncthreads();
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
+    // the next density's column is loaded into registers while the current one is transformed
+    const auto load = [&](int p, cx<T>(&v)[R1]) {
+        const cx<T>* src = buf + (long long)p * stride + (long long)z * nx * ny + x;
+#pragma unroll
+        for (int j = 0; j < R1; ++j) {
+            const bool ld = valid && (S > 0 || ((live_in >> j) & 1u));
+            v[j] = ld ? src[(long long)(q + R2 * j) * nx] : mk(T(0), T(0));
+        }
+    };
+    cx<T> v[R1], vn[R1];
+    if (q < R2 && p_begin < p_end) load(p_begin, v);
     for (int p = p_begin; p < p_end; ++p) {
         cx<T>* base = buf + (long long)p * stride + (long long)z * nx * ny + x;
+        if (q < R2 && p + 1 < p_end) load(p + 1, vn);
         if (q < R2) {
-            cx<T> v[R1];
-#pragma unroll
-            for (int j = 0; j < R1; ++j) {
-                const bool load = valid && (S > 0 || ((live_in >> j) & 1u));
-                v[j] = load ? base[(long long)(q + R2 * j) * nx] : mk(T(0), T(0));
-            }
             dft<R1, S>(v);
 #pragma unroll
             for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * L + line] = v[r];
@@ -164,6 +178,8 @@ __global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2
             }
         }
         __syncthreads();
+#pragma unroll
+        for (int j = 0; j < R1; ++j) v[j] = vn[j];
     }
 }
 
@@ -277,12 +293,13 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
 }
 
 // Inverse: rows of the next density are prefetched with cp.async while the current one is
-// transformed; then x phase_kappa is accumulated into V at the rows' atoms (FP64).
+// transformed; then the round's value at the rows' atoms is written to out[p][atom]
+// (write-only; the phase and the round sum are applied in FP64 by k_round_sum).
 template <typename T, int R1, int R2, int LR>
 __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R2, LR * cmax<R1, R2>::value>::value)
-    k_xinv_rf(const cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g, RoundPhase rp,
-              const int* __restrict__ row_ptr, const int* __restrict__ cell, cx<double>* __restrict__ V,
-              long long v_stride, int ny, int nrows, int np) {
+    k_xinv_rf(const cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g,
+              const int* __restrict__ row_ptr, const int* __restrict__ cell, cx<T>* __restrict__ out,
+              long long o_stride, int nrows, int np) {
     constexpr int N = R1 * R2;
     constexpr int LP = LR + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -314,7 +331,6 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
     constexpr int KA = 4;
     const bool pre = (a1 - a0) <= KA * (int)blockDim.x;
     int slot[KA];
-    cx<double> ph[KA];
     if (pre) {
 #pragma unroll
         for (int k = 0; k < KA; ++k) {
@@ -324,7 +340,6 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
                 const int c = cell[i];
                 const int row = c / N, x = c - row * N;
                 slot[k] = x * LP + (row - r0);
-                ph[k] = round_phase(rp, x, row % ny, row / ny);
             }
         }
     }
@@ -364,20 +379,16 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             }
         }
         __syncthreads();
-        cx<double>* vp = V + (long long)p * v_stride;
+        cx<T>* op = out + (long long)p * o_stride;
         if (pre) {
 #pragma unroll
             for (int k = 0; k < KA; ++k)
-                if (slot[k] >= 0) {
-                    const int i = a0 + threadIdx.x + k * blockDim.x;
-                    vp[i] = vp[i] + cmul(widen(cur[slot[k]]), ph[k]);
-                }
+                if (slot[k] >= 0) op[a0 + threadIdx.x + k * blockDim.x] = cur[slot[k]];
         } else {
             for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
                 const int c = cell[i];
                 const int row = c / N, x = c - row * N;
-                const int y = row % ny, z = row / ny;
-                vp[i] = vp[i] + cmul(widen(cur[x * LP + (row - r0)]), round_phase(rp, x, y, z));
+                op[i] = cur[x * LP + (row - r0)];
             }
         }
         __syncthreads();

@@ -133,7 +133,8 @@ int cl_last_timings(cl_ctx* ctx, double t[4]);
 #define CL_KCLASS_GRAM      5  /* real-space reductions: FP64 Gram (plain) or tensor-core Gram (FP32 form) */
 #define CL_KCLASS_KERNEL    6  /* Coulomb kernel octant, DCT-I, folded kernels */
 #define CL_KCLASS_GRAM_SPLIT 7 /* TF32 hi/lo operand split of the tensor-core Gram (FP32 form) */
-#define CL_NUM_KCLASS       8
+#define CL_KCLASS_ROUND_SUM 8  /* x phase_kappa and the FP64 sum of the rounds at the atoms */
+#define CL_NUM_KCLASS       10
 /* enable != 0 starts recording (and clears the counters); 0 stops. */
 int cl_set_profiling(cl_ctx* ctx, int enable);
 /* Accumulated device milliseconds, launches and algorithmic bytes (the minimum HBM

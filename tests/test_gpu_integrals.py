@@ -209,3 +209,22 @@ def test_prepared_requests_and_graph_batch(mode):
         r.close()
     for cc in calcs:
         cc.close()
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_round_split_over_more_ranks_than_rounds(mode):
+    """With 10 shares of the 8 rounds, the two shares without a round give exact zeros and all
+    shares still add up to the full request."""
+    from coulombo_lattice_b200 import multi
+    d = synth.build("c1", cells=(3, 4, 3))
+    step = (synth.A_ZB / 4,) * 3
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], 2)
+        full = cc.compute(specs)
+        parts = [cc.compute_rounds(specs, multi.round_mask(r, 10)) for r in range(10)]
+    assert multi.round_mask(8, 10) == 0 and multi.round_mask(9, 10) == 0
+    assert np.all(parts[8] == 0) and np.all(parts[9] == 0)
+    tol = 1e-12 if mode == cl.MODE_FP64_PLAIN else 1e-6
+    assert np.abs(sum(parts) - full).max() <= tol * np.abs(full).max()
