@@ -246,14 +246,25 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             }
         }
     }
+    // cells without an atom stay zero for every density: the tile is cleared once
+    for (int e = threadIdx.x; e < N * LP; e += blockDim.x) tile[e] = mk(T(0), T(0));
+    __syncthreads();
+    // the next density's atom values are loaded into registers while the current one is
+    // transformed
+    cx<double> rv[KA], rn[KA];
+    const auto load = [&](int p, cx<double>(&v)[KA]) {
+        const cx<double>* src = rho + (long long)p * rho_stride + a0 + threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < KA; ++k) v[k] = slot[k] >= 0 ? src[k * blockDim.x] : mk(0.0, 0.0);
+    };
+    if (pre && p_begin < p_end) load(p_begin, rv);
     for (int p = p_begin; p < p_end; ++p) {
-        for (int e = threadIdx.x; e < N * LP; e += blockDim.x) tile[e] = mk(T(0), T(0));
-        __syncthreads();
         const cx<double>* rp_ = rho + (long long)p * rho_stride;
         if (pre) {
+            if (p + 1 < p_end) load(p + 1, rn);
 #pragma unroll
             for (int k = 0; k < KA; ++k)
-                if (slot[k] >= 0) tile[slot[k]] = narrow<T>(cmulc(rp_[a0 + threadIdx.x + k * blockDim.x], ph[k]));
+                if (slot[k] >= 0) tile[slot[k]] = narrow<T>(cmulc(rv[k], ph[k]));
         } else {
             for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
                 const int c = cell[i];
@@ -289,6 +300,10 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
                 for (int r = 0; r < R2; ++r) o[r * R1] = u[r];
             }
         }
+        if (pre) {
+#pragma unroll
+            for (int k = 0; k < KA; ++k) rv[k] = rn[k];
+        }
     }
 }
 
@@ -304,7 +319,8 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
     constexpr int LP = LR + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
-    cx<T>* tb[2] = {tw + N, tw + N + N * LP};
+    cx<T>* const tb0 = tw + N;
+    cx<T>* const tb1 = tw + N + N * LP;
     cx<T>* ex = tw + N + 2 * N * LP;
     __shared__ unsigned char live[LR];
     const int r0 = blockIdx.x * LR;
@@ -343,11 +359,12 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             }
         }
     }
-    if (p_begin < p_end) load(p_begin, tb[0]);
+    if (p_begin < p_end) load(p_begin, tb0);
     for (int p = p_begin; p < p_end; ++p) {
-        cx<T>* cur = tb[(p - p_begin) & 1];
+        const bool odd = ((p - p_begin) & 1) != 0;
+        cx<T>* cur = odd ? tb1 : tb0;
         if (p + 1 < p_end) {
-            load(p + 1, tb[(p + 1 - p_begin) & 1]);
+            load(p + 1, odd ? tb0 : tb1);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
