@@ -508,6 +508,8 @@ def run_ours(args):
         "fft_hbm_roofline": {"frac": fft_bytes / (fft_ms / 1e3) / 1e9 / peak,
                              "transforms_per_density": 16, "bytes_per_transform": "2*M*8 (FP32 complex)"},
         "gram_tensor_roofline": gram_tc,
+        "autotune": [ln for ln in cl.autotune_report().splitlines()
+                     if "fp32 %dx%dx%d:" % tuple(d["dims"]) in ln],
         "gpu_launches": int(total_launches),
         "clocks": clock_info,
     }

@@ -59,6 +59,7 @@ SIGNATURES = [
     ("cl_compute", _i, [_vp, _i64, _P(ctypes.c_int16), _P(_d)]),
     ("cl_potentials", _i, [_vp, _P(_d)]),
     ("cl_last_timings", _i, [_vp, _P(_d)]),
+    ("cl_autotune_report", _i, [ctypes.c_char_p, _i64, _P(_i64)]),
     ("cl_compute_rounds", _i, [_vp, _i64, _P(ctypes.c_int16), _i, _P(_d)]),
     ("cl_set_profiling", _i, [_vp, _i]),
     ("cl_kernel_profile", _i, [_vp, _P(_d), _P(_i64), _P(_d)]),
@@ -151,6 +152,15 @@ def plan(n_inputs, specs):
     steps = np.empty((s.shape[0], 5), dtype=np.int32)
     _check(lib().cl_plan(n_inputs, s.shape[0], _ptr(s, ctypes.c_int16), _ptr(steps, ctypes.c_int32)))
     return steps
+
+
+def autotune_report():
+    """The autotuner's choices so far (cl_autotune_report), one line per pass/shape/precision."""
+    need = ctypes.c_int64()
+    _check(lib().cl_autotune_report(None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(int(need.value))
+    _check(lib().cl_autotune_report(buf, need.value, None))
+    return buf.value.decode()
 
 
 def fft3d(data, sign=-1, fp32=False):

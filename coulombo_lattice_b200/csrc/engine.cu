@@ -2,9 +2,12 @@
 #include <algorithm>
 #include <array>
 #include <memory>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -18,7 +21,7 @@
 #include "host/host_logic.hpp"
 #include "host/status.hpp"
 #include "kernels.cuh"
-#include "rfft.cuh"
+#include "passes.hpp"
 #include "gram_tc.cuh"
 
 using clk::cx;
@@ -228,13 +231,7 @@ PlaneTile plane_tile(int nx, int ny) {
     return PlaneTile{fits, ld, smem};
 }
 
-// Density groups of the z pass: enough blocks to fill every SM several times over, while
-// each block still reuses its Khat tile for a run of densities.
-unsigned zgroups(long long zblocks, int cnt) {
-    const long long target = 148LL * 16;
-    long long g = (target + zblocks - 1) / zblocks;
-    return (unsigned)std::max(1LL, std::min<long long>(g, cnt));
-}
+unsigned zgroups(long long zblocks, int cnt) { return clp::density_groups(zblocks, cnt); }
 
 // Bytes of grids a chunk may hold so that consecutive passes meet in L2 (CL_L2_CHUNK_MB;
 // off by default: measured on B200 it gave no gain at 96^3 over whole-request chunks).
@@ -434,77 +431,93 @@ void transform_kernel(cl_ctx* c) {
     c->kernel_ready = true;
 }
 
-// Register two-factor column passes (rfft.cuh) where the length has a compiled split; these
-// return false (nothing launched) otherwise.  CL_NO_REGISTER_FFT forces the generic passes.
-template <typename T>
-bool launch_zconv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const T* kh, long long nxy, int nz, int cnt) {
-    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
-    constexpr int L = sizeof(T) == 4 ? 16 : 8;
-    return clk::with_split2(nz, [&](auto tag) {
-        using Tag = decltype(tag);
-        constexpr int N = Tag::r1 * Tag::r2;
-        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
-        auto kern = clk::k_zconv_rf<T, Tag::r1, Tag::r2, L>;
-        const size_t smem = sizeof(cx<T>) * ((size_t)N + 2ull * N * L);
-        ensure_smem(kern, smem);
-        const long long blocks = (nxy + L - 1) / L;
-        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), L * Q, smem, c->stream>>>(buf, c->M, tw, kh, nxy, cnt);
-    });
+// ---------------------------------------------------------------------------------------
+// Autotuner of the register passes (passes.hpp).  For each pass of a grid shape and
+// precision, every compiled variant (radix split of the line length x lines per block) is
+// timed with CUDA events on the request's own buffers, and the fastest is kept for the rest of
+// the process.  Tuning runs at the first eager request of a shape (never inside a graph
+// capture); CL_AUTOTUNE=0 keeps the default variants.
+// ---------------------------------------------------------------------------------------
+struct TuneKey {
+    int pass, fp32, nx, ny, nz;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(pass, fp32, nx, ny, nz) < std::tie(o.pass, o.fp32, o.nx, o.ny, o.nz);
+    }
+};
+struct TuneEntry {
+    clp::Variant v;
+    int candidates = 0;
+    double ms = 0, ms_default = 0;  // per launch of the tuning sample
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneEntry> g_tune;
+
+bool autotune_enabled() {
+    const char* e = std::getenv("CL_AUTOTUNE");
+    return !(e && e[0] == '0');
 }
 
-template <int S, typename T>
-bool launch_ycol_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, int nx, int ny, int nz, int cnt, const int* row_ptr) {
-    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
-    constexpr int L = sizeof(T) == 4 ? 16 : 8;
-    return clk::with_split2(ny, [&](auto tag) {
-        using Tag = decltype(tag);
-        constexpr int N = Tag::r1 * Tag::r2;
-        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
-        auto kern = clk::k_ycol_rf<S, T, Tag::r1, Tag::r2, L>;
-        const size_t smem = sizeof(cx<T>) * ((size_t)N + (size_t)N * L);
-        ensure_smem(kern, smem);
-        const int xchunks = (nx + L - 1) / L;
-        const long long blocks = (long long)xchunks * nz;
-        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), L * Q, smem, c->stream>>>(buf, c->M, tw, nx, ny, xchunks,
-                                                                                        cnt, row_ptr);
-    });
+bool register_passes_enabled() { return !std::getenv("CL_NO_REGISTER_FFT"); }
+
+clp::Variant tuned_variant(const cl_ctx* c, int pass, bool fp32) {
+    if (const char* f = std::getenv("CL_TUNE_FORCE")) {  // "split,half": one variant for every pass
+        clp::Variant v;
+        if (std::sscanf(f, "%d,%d", &v.split, &v.half) == 2) return v;
+    }
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(TuneKey{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]});
+    return it == g_tune.end() ? clp::Variant{} : it->second.v;
 }
 
-template <typename T>
-bool launch_xfwd_rf(cl_ctx* c, const cx<double>* rho, long long rho_stride, const int* row_ptr, const int* cell,
-                    cx<T>* buf, const cx<T>* tw, const clk::RoundPhase& rp, int nx, int ny, int nrows, int cnt,
-                    int skip_empty) {
-    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
-    constexpr int LR = sizeof(T) == 4 ? 16 : 8;
-    return clk::with_split2(nx, [&](auto tag) {
-        using Tag = decltype(tag);
-        constexpr int N = Tag::r1 * Tag::r2;
-        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
-        auto kern = clk::k_xfwd_rf<T, Tag::r1, Tag::r2, LR>;
-        const size_t smem = sizeof(cx<T>) * ((size_t)N + 2ull * N * (LR + 1));
-        ensure_smem(kern, smem);
-        const long long blocks = (nrows + LR - 1) / LR;
-        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), LR * Q, smem, c->stream>>>(
-            rho, rho_stride, row_ptr, cell, buf, c->M, tw, rp, ny, nrows, cnt, skip_empty);
-    });
+bool stream_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    CL_CUDA(cudaStreamIsCapturing(s, &st));
+    return st != cudaStreamCaptureStatusNone;
 }
 
-template <typename T>
-bool launch_xinv_rf(cl_ctx* c, cx<T>* buf, const cx<T>* tw, const int* row_ptr, const int* cell, cx<T>* out,
-                    long long o_stride, int nx, int nrows, int cnt) {
-    if (std::getenv("CL_NO_REGISTER_FFT")) return false;
-    constexpr int LR = sizeof(T) == 4 ? 16 : 8;
-    return clk::with_split2(nx, [&](auto tag) {
-        using Tag = decltype(tag);
-        constexpr int N = Tag::r1 * Tag::r2;
-        constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
-        auto kern = clk::k_xinv_rf<T, Tag::r1, Tag::r2, LR>;
-        const size_t smem = sizeof(cx<T>) * ((size_t)N + 3ull * N * (LR + 1));
-        ensure_smem(kern, smem);
-        const long long blocks = (nrows + LR - 1) / LR;
-        kern<<<dim3((unsigned)blocks, zgroups(blocks, cnt)), LR * Q, smem, c->stream>>>(
-            buf, c->M, tw, row_ptr, cell, out, o_stride, nrows, cnt);
-    });
+// Times launch(variant) -- one warm-up and three timed launches per candidate -- and records
+// the fastest variant of the pass.  Candidates: the split variants of the line length `len`,
+// each with the default and (FP32) the half lines per block; the default is tried first.
+template <typename F>
+void tune_pass(cl_ctx* c, int pass, bool fp32, int len, F&& launch) {
+    const TuneKey key{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]};
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        if (g_tune.count(key)) return;
+    }
+    std::vector<clp::Variant> cands;
+    for (int sv = 0; sv < clp::split_variants(len); ++sv)
+        for (int h = 0; h < (fp32 ? 2 : 1); ++h) cands.push_back(clp::Variant{sv, h});
+    TuneEntry best;
+    best.candidates = (int)cands.size();
+    if (cands.size() >= 2) {
+        cudaEvent_t a, b;
+        CL_CUDA(cudaEventCreate(&a));
+        CL_CUDA(cudaEventCreate(&b));
+        double best_ms = 1e30;
+        for (size_t i = 0; i < cands.size(); ++i) {
+            launch(cands[i]);
+            CL_LAUNCHED();
+            CL_CUDA(cudaEventRecord(a, c->stream));
+            for (int k = 0; k < 3; ++k) launch(cands[i]);
+            CL_LAUNCHED();
+            CL_CUDA(cudaEventRecord(b, c->stream));
+            CL_CUDA(cudaEventSynchronize(b));
+            float ms = 0;
+            CL_CUDA(cudaEventElapsedTime(&ms, a, b));
+            const double per = ms / 3.0;
+            if (i == 0) best.ms_default = per;
+            if (per < best_ms) {
+                best_ms = per;
+                best.v = cands[i];
+            }
+        }
+        best.ms = best_ms;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune[key] = best;
 }
 
 // Number of atoms listed by a row CSR (host-side copy kept with the CSR).
@@ -571,9 +584,45 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     const long long zblocks = (nxy + zt.W - 1) / zt.W;
     // Rows without atoms are skipped (not stored / not loaded) when the x and y passes are both
     // the register ones, which agree on it; CL_NO_ROW_SKIP turns it off.
-    const bool reg_x = !std::getenv("CL_NO_REGISTER_FFT") && clk::with_split2(nx, [](auto) {});
-    const bool reg_y = !std::getenv("CL_NO_REGISTER_FFT") && clk::with_split2(ny, [](auto) {});
+    const bool reg_x = register_passes_enabled() && clp::split_variants(nx) > 0;
+    const bool reg_y = register_passes_enabled() && clp::split_variants(ny) > 0;
+    const bool reg_z = register_passes_enabled() && clp::split_variants(nz) > 0;
     const int skip_empty = (!pt.fits && reg_x && reg_y && !std::getenv("CL_NO_ROW_SKIP")) ? 1 : 0;
+    const bool fp32 = sizeof(T) == 4;
+
+    // Autotuning at the first eager request of this shape: the variants run on the first
+    // densities of the request (about 512 MB of grids) in the work and rounds buffers, which
+    // the request's own passes overwrite afterwards.
+    if (autotune_enabled() && !std::getenv("CL_TUNE_FORCE") && np > 0 && !stream_capturing(c->stream)) {
+        const int cnt_t = (int)std::max<size_t>(1, std::min<size_t>((size_t)chunk, (512ull << 20) / grid_bytes));
+        const clk::RoundPhase rp0{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
+        const T* kh0 = sizeof(T) == 4 ? (const T*)c->khat32[0].p : (const T*)c->khat64[0].p;
+        const int* rp_skip = skip_empty ? row_ptr : nullptr;
+        if (!pt.fits && reg_x)
+            tune_pass(c, clp::kXFwd, fp32, nx, [&](clp::Variant v) {
+                clp::xfwd<T>(c->stream, v, rho, rho_stride, row_ptr, cell, buf, c->M, twx, rp0, nx, ny, nrows, cnt_t,
+                             skip_empty);
+            });
+        if (!pt.fits && reg_y) {
+            tune_pass(c, clp::kYFwd, fp32, ny, [&](clp::Variant v) {
+                clp::ycol<-1, T>(c->stream, v, buf, c->M, twy, nx, ny, nz, cnt_t, rp_skip);
+            });
+            tune_pass(c, clp::kYInv, fp32, ny, [&](clp::Variant v) {
+                clp::ycol<+1, T>(c->stream, v, buf, c->M, twy, nx, ny, nz, cnt_t, rp_skip);
+            });
+        }
+        if (reg_z)
+            tune_pass(c, clp::kZConv, fp32, nz, [&](clp::Variant v) {
+                clp::zconv<T>(c->stream, v, buf, c->M, twz, kh0, nxy, nz, cnt_t);
+            });
+        if (!pt.fits && reg_x)
+            tune_pass(c, clp::kXInv, fp32, nx, [&](clp::Variant v) {
+                clp::xinv<T>(c->stream, v, buf, c->M, twx, row_ptr, cell, tr, n_at, nx, nrows, cnt_t);
+            });
+    }
+    const clp::Variant v_xf = tuned_variant(c, clp::kXFwd, fp32), v_yf = tuned_variant(c, clp::kYFwd, fp32),
+                       v_z = tuned_variant(c, clp::kZConv, fp32), v_yi = tuned_variant(c, clp::kYInv, fp32),
+                       v_xi = tuned_variant(c, clp::kXInv, fp32);
 
     // algorithmic bytes per density of each pass (minimum HBM traffic of its work); with
     // skipped rows only the live fraction of a row-side sweep counts
@@ -596,8 +645,8 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
             if (pt.fits) {
                 clk::k_xyfwd<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
                     rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan, Y.plan, twx, twy, rp, nx, ny, pt.ld);
-            } else if (!launch_xfwd_rf<T>(c, rho_c, rho_stride, row_ptr, cell, buf, twx, rp, nx, ny, nrows, cnt,
-                                          skip_empty)) {
+            } else if (!(reg_x && clp::xfwd<T>(c->stream, v_xf, rho_c, rho_stride, row_ptr, cell, buf, c->M, twx,
+                                                rp, nx, ny, nrows, cnt, skip_empty))) {
                 clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, c->M,
                                                                      X.plan, twx, rp, nx, ny, nrows, xt.rows, xt.ld,
                                                                      cnt);
@@ -606,21 +655,23 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
             prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * 16.0 + live * gbytes) + atoms * 4.0);
             if (!pt.fits) {
                 e = prof_begin(c);
-                if (!launch_ycol_rf<-1, T>(c, buf, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr))
+                if (!(reg_y &&
+                      clp::ycol<-1, T>(c->stream, v_yf, buf, c->M, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr)))
                     clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy,
                                                                                               nx, ny, yt.W, ychunks);
                 CL_LAUNCHED();
                 prof_end(c, e, CL_KCLASS_YPASS, cnt * (1.0 + live) * gbytes);
             }
             e = prof_begin(c);
-            if (!launch_zconv_rf<T>(c, buf, twz, kh, nxy, nz, cnt))
+            if (!(reg_z && clp::zconv<T>(c->stream, v_z, buf, c->M, twz, kh, nxy, nz, cnt)))
                 clk::k_zpass<T><<<dim3((unsigned)zblocks, zgroups(zblocks, cnt)), 256, zt.smem, c->stream>>>(
                     buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W, cnt, 0);
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
             if (!pt.fits) {
                 e = prof_begin(c);
-                if (!launch_ycol_rf<+1, T>(c, buf, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr))
+                if (!(reg_y &&
+                      clp::ycol<+1, T>(c->stream, v_yi, buf, c->M, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr)))
                     clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, c->M, Y.plan, twy,
                                                                                               nx, ny, yt.W, ychunks);
                 CL_LAUNCHED();
@@ -630,7 +681,8 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
             if (pt.fits) {
                 clk::k_xyinv<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
                     buf, c->M, X.plan, Y.plan, twx, twy, row_ptr, cell, tr_r, n_at, nx, ny, pt.ld);
-            } else if (!launch_xinv_rf<T>(c, buf, twx, row_ptr, cell, tr_r, n_at, nx, nrows, cnt)) {
+            } else if (!(reg_x && clp::xinv<T>(c->stream, v_xi, buf, c->M, twx, row_ptr, cell, tr_r, n_at, nx, nrows,
+                                                cnt))) {
                 clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, row_ptr, cell, tr_r,
                                                                      n_at, nx, nrows, xt.rows, xt.ld, cnt);
             }
@@ -1516,6 +1568,32 @@ int cl_batch_last_ms(cl_batch* b, double* ms) {
     return cl::guarded([&] {
         if (!b || !ms) cl::fail(CL_ERR_ARGUMENT, "null argument");
         *ms = b->last_ms;
+    });
+}
+
+int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
+    return cl::guarded([&] {
+        static const char* names[clp::kNumPasses] = {"x_forward", "y_forward", "z_pass", "y_inverse", "x_inverse"};
+        std::string out;
+        {
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            for (const auto& kv : g_tune) {
+                char line[256];
+                std::snprintf(line, sizeof line,
+                              "%s %s %dx%dx%d: split %s, lines %s, %d candidates, %.4f ms (default %.4f ms)\n",
+                              names[kv.first.pass], kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny,
+                              kv.first.nz, kv.second.v.split ? "swapped" : "balanced",
+                              kv.second.v.half ? "half" : "default", kv.second.candidates, kv.second.ms,
+                              kv.second.ms_default);
+                out += line;
+            }
+        }
+        if (needed) *needed = (int64_t)out.size() + 1;
+        if (buf && len > 0) {
+            const size_t n = std::min<size_t>(out.size(), (size_t)len - 1);
+            std::memcpy(buf, out.data(), n);
+            buf[n] = 0;
+        }
     });
 }
 

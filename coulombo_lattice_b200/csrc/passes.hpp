@@ -1,0 +1,59 @@
+// Launchers of the register-FFT passes (rfft.cuh) for every compiled variant.
+//
+// A variant picks the radix split of the line length (the balanced split, or its two factors
+// swapped) and the lines per block (the default -- 16 for FP32, 8 for FP64 -- or half).  The
+// autotuner in engine.cu times the variants of each pass on the request's own shapes and
+// keeps the fastest.  Each launcher returns false (nothing launched) when the length has no
+// compiled two-factor split; launch errors surface through cudaGetLastError.
+//
+// The launchers are instantiated in passes_xfwd.cu, passes_xinv.cu, passes_yfwd.cu,
+// passes_yinv.cu and passes_z.cu (one translation unit per pass, compiled in parallel).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fft.cuh"
+#include "kernels.cuh"
+
+namespace clp {
+
+using clk::cx;
+
+struct Variant {
+    int split = 0;  // 0: the balanced split; 1: its factors swapped
+    int half = 0;   // 1: half the default lines (rows) per block (FP32 only)
+    bool operator==(const Variant& o) const { return split == o.split && half == o.half; }
+};
+
+enum Pass { kXFwd = 0, kYFwd = 1, kZConv = 2, kYInv = 3, kXInv = 4, kNumPasses = 5 };
+
+// Number of distinct split variants compiled for a line length: 0 (no register pass), 1
+// (square split) or 2.
+int split_variants(int n);
+
+// Density groups of a launch (gridDim.y): enough blocks to fill every SM several times over,
+// while each block still reuses its per-block setup for a run of densities.
+unsigned density_groups(long long blocks, int cnt);
+
+// z pass: forward FFT along z, x Khat, inverse FFT along z (in place).
+template <typename T>
+bool zconv(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, const T* kh, long long nxy, int nz,
+           int cnt);
+
+// y pass of direction S (in place); row_ptr (or nullptr) marks the rows without atoms.
+template <int S, typename T>
+bool ycol(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, int nx, int ny, int nz, int cnt,
+          const int* row_ptr);
+
+// forward x pass: scatter of the atoms x conj(phase), FFT along x, rows stored.
+template <typename T>
+bool xfwd(cudaStream_t s, Variant v, const cx<double>* rho, long long rho_stride, const int* row_ptr,
+          const int* cell, cx<T>* buf, long long M, const cx<T>* tw, const clk::RoundPhase& rp, int nx, int ny,
+          int nrows, int cnt, int skip_empty);
+
+// inverse x pass: inverse FFT along x, the round's values at the atoms written to out.
+template <typename T>
+bool xinv(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, const int* row_ptr,
+          const int* cell, cx<T>* out, long long o_stride, int nx, int nrows, int cnt);
+
+}  // namespace clp

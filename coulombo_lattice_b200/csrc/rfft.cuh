@@ -414,18 +414,25 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
 
 // ---------------------------------------------------------------------------------------
 // Host-side dispatch: calls f(SplitTag<R1, R2>{}) for a length with a compiled two-factor
-// split (factors are register codelets 2..16, as balanced as possible); false otherwise.
+// split (factors are register codelets 2..16, as balanced as possible, or swapped); false
+// otherwise.
 // ---------------------------------------------------------------------------------------
 template <int A, int B>
 struct SplitTag {
     static constexpr int r1 = A, r2 = B;
 };
 
+// variant 1 calls f with the two factors swapped (the same split when they are equal).
 template <typename F>
-bool with_split2(int n, F&& f) {
+bool with_split2(int n, F&& f, int variant = 0) {
     switch (n) {
-#define CLK_SPLIT(N, A, B) \
-    case N: f(SplitTag<A, B>{}); return true;
+#define CLK_SPLIT(N, A, B)                  \
+    case N:                                 \
+        if (variant != 0 && (A) != (B))     \
+            f(SplitTag<B, A>{});            \
+        else                                \
+            f(SplitTag<A, B>{});            \
+        return true;
         CLK_SPLIT(16, 4, 4)
         CLK_SPLIT(20, 4, 5)
         CLK_SPLIT(24, 4, 6)

@@ -123,6 +123,14 @@ int cl_compute_rounds(cl_ctx* ctx, int64_t n_int, const int16_t* spec, int round
  * t[0] pair densities, t[1] transforms (all rounds), t[2] reductions, t[3] total. */
 int cl_last_timings(cl_ctx* ctx, double t[4]);
 
+/* Choices of the autotuner (process-wide): one text line per tuned pass, grid shape and
+ * precision -- the radix split and lines per block kept, with the per-launch time of the
+ * tuning sample next to the default variant's.  Writes at most len bytes (NUL-terminated) to
+ * buf when buf is non-null; *needed (if non-null) receives the full size.  No reference
+ * counterpart: the reference plans its FFTs with FFTW_MEASURE / FFTW_ESTIMATE
+ * (CoulombCalculator.cpp:17-39).  CL_AUTOTUNE=0 in the environment disables tuning. */
+int cl_autotune_report(char* buf, int64_t len, int64_t* needed);
+
 /* Per-kernel timing with CUDA events recorded on the context's stream around every launch.
  * Classes: */
 #define CL_KCLASS_DENSITY   0  /* pair densities at atoms */
