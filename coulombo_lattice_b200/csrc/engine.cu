@@ -692,10 +692,10 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
         }
         if (n_rounds > 0) {
             const clk::RoundPhase base{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
-            const int blocks = (int)std::min<long long>((n_at + 255) / 256, 148LL * 16);
+            const long long blocks = std::min<long long>((n_at + 255) / 256, 148LL * 16);
             cudaEvent_t e = prof_begin(c);
-            clk::k_round_sum<T><<<blocks, 256, 0, c->stream>>>(tr, tr_slot, n_at, round_mask & 0xFF, base, cell, nx,
-                                                              ny, n_at, V_c, v_stride, cnt);
+            clk::k_round_sum<T><<<dim3((unsigned)blocks, zgroups(blocks, cnt)), 256, 0, c->stream>>>(
+                tr, tr_slot, n_at, round_mask & 0xFF, base, cell, nx, ny, n_at, V_c, v_stride, cnt);
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_ROUND_SUM,
                      cnt * atoms * (n_rounds * (double)sizeof(cx<T>) + 16.0) + atoms * 4.0);

@@ -451,13 +451,16 @@ __global__ void __launch_bounds__(512, 1) k_xyinv(const cx<T>* __restrict__ buf,
 // and density p, V[p][i] = sum over the rounds present, in ascending kappa, of
 // widen(t_kappa[p][i]) x phase_kappa(cell i), in FP64.  The rounds' values t_kappa come from the
 // inverse x pass (slot s = kappa's rank among the present rounds; slot stride r_stride).  A
-// thread owns one atom: its (at most 8) phases are formed once and reused for every density.
+// thread owns one atom: its (at most 8) phases are formed once and reused for the densities
+// [blockIdx.y * per, ...) of its block.
 // ---------------------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_round_sum(const cx<T>* __restrict__ t, long long r_stride,
                                                   long long p_stride, int round_mask, RoundPhase base,
                                                   const int* __restrict__ cell, int nx, int ny, long long n_atoms,
                                                   cx<double>* __restrict__ V, long long v_stride, int np) {
+    const int per = (np + gridDim.y - 1) / gridDim.y;
+    const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_atoms;
          i += (long long)gridDim.x * blockDim.x) {
         const int c = cell[i];
@@ -472,7 +475,7 @@ __global__ void __launch_bounds__(256) k_round_sum(const cx<T>* __restrict__ t, 
             rp.kz = (r >> 2) & 1;
             ph[r] = round_phase(rp, x, y, z);
         }
-        for (int p = 0; p < np; ++p) {
+        for (int p = p_begin; p < p_end; ++p) {
             const cx<T>* tp = t + (long long)p * p_stride + i;
             cx<double> acc = mk(0.0, 0.0);
             long long s = 0;

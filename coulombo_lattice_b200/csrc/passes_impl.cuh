@@ -117,7 +117,8 @@ bool xinv(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, c
                 constexpr int N = Tag::r1 * Tag::r2;
                 constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
                 auto kern = clk::k_xinv_rf<T, Tag::r1, Tag::r2, LR>;
-                const size_t smem = sizeof(cx<T>) * ((size_t)N + 3ull * N * (LR + 1));
+                using Pitch = clk::XinvPitch<Tag::r1, Tag::r2, LR, sizeof(cx<T>)>;
+                const size_t smem = sizeof(cx<T>) * ((size_t)N + (size_t)LR * Pitch::PP + (size_t)LR * Pitch::NP);
                 set_smem(kern, smem);
                 const long long blocks = (nrows + LR - 1) / LR;
                 kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), LR * Q, smem, s>>>(

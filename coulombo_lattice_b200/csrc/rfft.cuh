@@ -307,108 +307,134 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
     }
 }
 
-// Inverse: rows of the next density are prefetched with cp.async while the current one is
-// transformed; then the round's value at the rows' atoms is written to out[p][atom]
-// (write-only; the phase and the round sum are applied in FP64 by k_round_sum).
+// Row pitches of the inverse row pass, chosen at compile time: every pad in [0, W) is tried
+// and the one whose worst shared-memory bank conflict (over the thread groups served by one
+// wavefront, W = 128 B / element) is lowest is kept -- for the exchange (phase A writes
+// la*PP + ta*(R1+1) + r, phase B reads lb*PP + jb + r*(R1+1)) and for the natural-order rows
+// (phase B writes lb*NP + jb + r*R1).
+template <int R1, int R2, int LR, int ES>
+struct XinvPitch {
+    static constexpr int N = R1 * R2;
+    static constexpr int Q = R1 > R2 ? R1 : R2;
+    static constexpr int T = LR * Q;
+    static constexpr int W = 128 / ES;
+    // worst number of distinct elements per bank slot over the wavefront groups;
+    // which: 0 phase-A exchange write, 1 phase-B exchange read, 2 phase-B row write
+    static constexpr int degree(int pitch, int which) {
+        int worst = 0;
+        for (int g0 = 0; g0 < T; g0 += W) {
+            int count[32] = {};
+            for (int tid = g0; tid < g0 + W && tid < T; ++tid) {
+                int e = -1;
+                if (which == 0) {
+                    const int ta = tid % R2, la = tid / R2;
+                    if (la < LR) e = la * pitch + ta * (R1 + 1);
+                } else {
+                    const int jb = tid % R1, lb = tid / R1;
+                    if (lb < LR) e = lb * pitch + jb;  // the r terms shift every thread alike
+                }
+                if (e >= 0) {
+                    const int slot = e % W;
+                    if (++count[slot] > worst) worst = count[slot];
+                }
+            }
+        }
+        return worst;
+    }
+    static constexpr int ex_pitch() {
+        int best = N + R2, bd = 1 << 30;
+        for (int pad = 0; pad < W; ++pad) {
+            const int pp = N + R2 + pad;
+            const int d = degree(pp, 0) > degree(pp, 1) ? degree(pp, 0) : degree(pp, 1);
+            if (d < bd) {
+                bd = d;
+                best = pp;
+            }
+        }
+        return best;
+    }
+    static constexpr int row_pitch() {
+        int best = N, bd = 1 << 30;
+        for (int pad = 0; pad < W; ++pad) {
+            const int d = degree(N + pad, 2);
+            if (d < bd) {
+                bd = d;
+                best = N + pad;
+            }
+        }
+        return best;
+    }
+    static constexpr int PP = ex_pitch();
+    static constexpr int NP = row_pitch();
+};
+
+// Inverse: phase A loads a row's points straight from HBM into registers (thread t of a row
+// reads x = t + R2*j, so a warp covers whole row segments), the next density's points being
+// loaded while the current one is transformed; rows without atoms are not loaded.  The
+// exchange between the stages uses a padded layout (one pad per R1 points, conflict-free in
+// both directions); phase B writes the rows in natural order to shared memory, from which the
+// round's values at the rows' atoms are gathered to out[p][atom] with consecutive threads on
+// consecutive atoms (write-only; the phase and the round sum are applied in FP64 by
+// k_round_sum).
 template <typename T, int R1, int R2, int LR>
 __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R2, LR * cmax<R1, R2>::value>::value)
     k_xinv_rf(const cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g,
               const int* __restrict__ row_ptr, const int* __restrict__ cell, cx<T>* __restrict__ out,
               long long o_stride, int nrows, int np) {
     constexpr int N = R1 * R2;
-    constexpr int LP = LR + 1;
+    // exchange row: position x' at x' + x' / R1 (one pad per R1 points), rows PP apart
+    constexpr int PP = XinvPitch<R1, R2, LR, sizeof(cx<T>)>::PP;
+    constexpr int NP = XinvPitch<R1, R2, LR, sizeof(cx<T>)>::NP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
-    cx<T>* const tb0 = tw + N;
-    cx<T>* const tb1 = tw + N + N * LP;
-    cx<T>* ex = tw + N + 2 * N * LP;
-    __shared__ unsigned char live[LR];
+    cx<T>* ex = tw + N;          // [LR][PP]
+    cx<T>* rows = ex + LR * PP;  // [LR][NP], natural order
     const int r0 = blockIdx.x * LR;
     const int nr = min(LR, nrows - r0);
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
-    if (threadIdx.x < LR) {
-        const int r = r0 + threadIdx.x;
-        live[threadIdx.x] = (threadIdx.x < nr && row_ptr[r + 1] > row_ptr[r]) ? 1 : 0;
-    }
-    __syncthreads();
     const int a0 = row_ptr[r0], a1 = row_ptr[r0 + nr];
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
-    // rows without atoms are never gathered, so they are not loaded (their slots keep
-    // whatever the buffer held; each row's transform is independent)
-    auto load = [&](int p, cx<T>* dst) {
-        const cx<T>* src = buf + (long long)p * stride + (long long)r0 * N;
-        for (int e = threadIdx.x; e < nr * N; e += blockDim.x) {
-            const int lr = e / N, x = e - lr * N;
-            if (live[lr]) cp_async<sizeof(cx<T>)>(dst + x * LP + lr, src + e);
-        }
-        cp_async_commit();
+    // phase A: thread (ta, la) transforms row la from points ta + R2*j
+    const int ta = threadIdx.x % R2, la = threadIdx.x / R2;
+    const bool load_row = la < nr && row_ptr[r0 + la + 1] > row_ptr[r0 + la];
+    // phase B: thread (jb, lb) holds points jb + r*R1 of row lb
+    const int jb = threadIdx.x % R1, lb = threadIdx.x / R1;
+    const auto load = [&](int p, cx<T>(&v)[R1]) {
+        const cx<T>* src = buf + (long long)p * stride + (long long)(r0 + la) * N + ta;
+#pragma unroll
+        for (int j = 0; j < R1; ++j) v[j] = load_row ? src[R2 * j] : mk(T(0), T(0));
     };
-    constexpr int KA = 4;
-    const bool pre = (a1 - a0) <= KA * (int)blockDim.x;
-    int slot[KA];
-    if (pre) {
-#pragma unroll
-        for (int k = 0; k < KA; ++k) {
-            const int i = a0 + threadIdx.x + k * blockDim.x;
-            slot[k] = -1;
-            if (i < a1) {
-                const int c = cell[i];
-                const int row = c / N, x = c - row * N;
-                slot[k] = x * LP + (row - r0);
-            }
-        }
-    }
-    if (p_begin < p_end) load(p_begin, tb0);
+    cx<T> v[R1], vn[R1];
+    if (la < LR && p_begin < p_end) load(p_begin, v);
+    __syncthreads();
     for (int p = p_begin; p < p_end; ++p) {
-        const bool odd = ((p - p_begin) & 1) != 0;
-        cx<T>* cur = odd ? tb1 : tb0;
-        if (p + 1 < p_end) {
-            load(p + 1, odd ? tb0 : tb1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
+        if (la < LR) {
+            if (p + 1 < p_end) load(p + 1, vn);
+            dft<R1, +1>(v);
+#pragma unroll
+            for (int r = 0; r < R1; ++r) ex[la * PP + ta * (R1 + 1) + r] = v[r];
         }
         __syncthreads();
-        {
-            const int lr = threadIdx.x % LR, t = threadIdx.x / LR;
-            if (t < R2) {
-                cx<T> v[R1];
+        if (lb < LR) {
+            cx<T> u[R2];
 #pragma unroll
-                for (int j = 0; j < R1; ++j) v[j] = cur[(t + R2 * j) * LP + lr];
-                dft<R1, +1>(v);
+            for (int r = 0; r < R2; ++r) u[r] = ex[lb * PP + jb + r * (R1 + 1)];
 #pragma unroll
-                for (int r = 0; r < R1; ++r) ex[(t * R1 + r) * LP + lr] = v[r];
-            }
-        }
-        __syncthreads();
-        {
-            const int j = threadIdx.x % R1, lr = threadIdx.x / R1;
-            if (lr < LR) {
-                cx<T> u[R2];
+            for (int r = 1; r < R2; ++r) u[r] = cmulc(u[r], tw[r * jb]);
+            dft<R2, +1>(u);
 #pragma unroll
-                for (int r = 0; r < R2; ++r) u[r] = ex[(j + r * R1) * LP + lr];
-#pragma unroll
-                for (int r = 1; r < R2; ++r) u[r] = cmulc(u[r], tw[r * j]);
-                dft<R2, +1>(u);
-#pragma unroll
-                for (int r = 0; r < R2; ++r) cur[(j + r * R1) * LP + lr] = u[r];
-            }
+            for (int r = 0; r < R2; ++r) rows[lb * NP + jb + r * R1] = u[r];
         }
         __syncthreads();
         cx<T>* op = out + (long long)p * o_stride;
-        if (pre) {
-#pragma unroll
-            for (int k = 0; k < KA; ++k)
-                if (slot[k] >= 0) op[a0 + threadIdx.x + k * blockDim.x] = cur[slot[k]];
-        } else {
-            for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
-                const int c = cell[i];
-                const int row = c / N, x = c - row * N;
-                op[i] = cur[x * LP + (row - r0)];
-            }
+        for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+            const int c = cell[i];
+            const int row = c / N, x = c - row * N;
+            op[i] = rows[(row - r0) * NP + x];
         }
-        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < R1; ++j) v[j] = vn[j];
     }
 }
 

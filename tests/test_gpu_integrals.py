@@ -228,3 +228,27 @@ def test_round_split_over_more_ranks_than_rounds(mode):
     assert np.all(parts[8] == 0) and np.all(parts[9] == 0)
     tol = 1e-12 if mode == cl.MODE_FP64_PLAIN else 1e-6
     assert np.abs(sum(parts) - full).max() <= tol * np.abs(full).max()
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_prepared_request_follows_new_coefficients(mode):
+    """New coefficients on the same atoms (cl_set_states) are picked up by an existing prepared
+    request and by its graph batch."""
+    d = synth.build("c1", cells=(4, 4, 4))
+    step = (synth.A_ZB / 4,) * 3
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    other = synth.make_states(d["pos"], d["orbitals"], 4, 777, "gauss")
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], 2)
+        req = cc.request(specs)
+        first = req.run()
+        batch = cl.Batch([req])
+        np.testing.assert_allclose(batch.run()[0], first, rtol=1e-12, atol=0)
+        cc.set_states(other, d["cells_idx"], 2)
+        want = cc.compute(specs)
+        np.testing.assert_allclose(req.run(), want, rtol=1e-12, atol=0)
+        np.testing.assert_allclose(batch.run()[0], want, rtol=1e-12, atol=0)
+        assert np.abs(want - first).max() > 1e-6 * np.abs(first).max()
+        batch.close()
+        req.close()
