@@ -362,10 +362,16 @@ def run_ours(args):
     plain.initialize(dielectric=DIELECTRIC)
     plain.set_states(d["states"], d["cells_idx"], d["holes"])
     v64 = plain.compute(specs)
+    # timed like the FP32 form: graph replays of the prepared request (best of 3)
+    preq = plain.request(specs)
+    pgraph64 = cl.Batch([preq])
+    pgraph64.run()
     plain_ms = []
-    for _ in range(2):
-        plain.compute(specs)
-        plain_ms.append(plain.timings()["total_ms"])
+    for _ in range(3):
+        pgraph64.run()
+        plain_ms.append(pgraph64.last_ms())
+    pgraph64.close()
+    preq.close()
     plain.close()
     plain_ms = max_over_ranks(min(plain_ms))
 
@@ -495,6 +501,7 @@ def run_ours(args):
                              "every launch (%.3f ms per step)" % (prof_dev_ms / args.steps)},
         "accuracy": accuracy,
         "plain_fp64": {"value": world * n_int / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                       "timing": "device time of a CUDA-graph replay of the prepared request, best of 3",
                        "speedup_of_fp32_form": plain_ms / ms_per_step},
         "e2e": {"value": world * n_int / (e2e_ms / 1e3), "unit": "integrals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},

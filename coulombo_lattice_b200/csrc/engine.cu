@@ -451,6 +451,41 @@ struct TuneEntry {
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;
+bool g_tune_loaded = false;
+
+// CL_TUNE_FILE: choices persist across processes.  Lines "pass fp32 nx ny nz split half";
+// the file is read once (before the first lookup) and every new choice is appended.
+const char* tune_file() {
+    const char* f = std::getenv("CL_TUNE_FILE");
+    return (f && *f) ? f : nullptr;
+}
+
+void tune_load_locked() {  // g_tune_mu held
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = tune_file();
+    if (!path) return;
+    FILE* fh = std::fopen(path, "r");
+    if (!fh) return;
+    TuneKey k{};
+    TuneEntry e;
+    while (std::fscanf(fh, "%d %d %d %d %d %d %d", &k.pass, &k.fp32, &k.nx, &k.ny, &k.nz, &e.v.split, &e.v.half) ==
+           7) {
+        if (k.pass < 0 || k.pass >= clp::kNumPasses) continue;
+        e.candidates = 0;  // loaded, not timed in this process
+        g_tune[k] = e;
+    }
+    std::fclose(fh);
+}
+
+void tune_save(const TuneKey& k, const TuneEntry& e) {
+    const char* path = tune_file();
+    if (!path) return;
+    if (FILE* fh = std::fopen(path, "a")) {
+        std::fprintf(fh, "%d %d %d %d %d %d %d\n", k.pass, k.fp32, k.nx, k.ny, k.nz, e.v.split, e.v.half);
+        std::fclose(fh);
+    }
+}
 
 bool autotune_enabled() {
     const char* e = std::getenv("CL_AUTOTUNE");
@@ -465,6 +500,7 @@ clp::Variant tuned_variant(const cl_ctx* c, int pass, bool fp32) {
         if (std::sscanf(f, "%d,%d", &v.split, &v.half) == 2) return v;
     }
     std::lock_guard<std::mutex> g(g_tune_mu);
+    tune_load_locked();
     auto it = g_tune.find(TuneKey{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]});
     return it == g_tune.end() ? clp::Variant{} : it->second.v;
 }
@@ -483,6 +519,7 @@ void tune_pass(cl_ctx* c, int pass, bool fp32, int len, F&& launch) {
     const TuneKey key{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]};
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
+        tune_load_locked();
         if (g_tune.count(key)) return;
     }
     std::vector<clp::Variant> cands;
@@ -518,6 +555,7 @@ void tune_pass(cl_ctx* c, int pass, bool fp32, int len, F&& launch) {
     }
     std::lock_guard<std::mutex> g(g_tune_mu);
     g_tune[key] = best;
+    tune_save(key, best);
 }
 
 // Number of atoms listed by a row CSR (host-side copy kept with the CSR).
@@ -1579,12 +1617,18 @@ int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
             std::lock_guard<std::mutex> g(g_tune_mu);
             for (const auto& kv : g_tune) {
                 char line[256];
-                std::snprintf(line, sizeof line,
-                              "%s %s %dx%dx%d: split %s, lines %s, %d candidates, %.4f ms (default %.4f ms)\n",
-                              names[kv.first.pass], kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny,
-                              kv.first.nz, kv.second.v.split ? "swapped" : "balanced",
-                              kv.second.v.half ? "half" : "default", kv.second.candidates, kv.second.ms,
-                              kv.second.ms_default);
+                const char* pn = names[kv.first.pass];
+                const char* pr = kv.first.fp32 ? "fp32" : "fp64";
+                const char* sp = kv.second.v.split ? "swapped" : "balanced";
+                const char* ln = kv.second.v.half ? "half" : "default";
+                if (kv.second.candidates == 0)
+                    std::snprintf(line, sizeof line, "%s %s %dx%dx%d: split %s, lines %s, from CL_TUNE_FILE\n", pn, pr,
+                                  kv.first.nx, kv.first.ny, kv.first.nz, sp, ln);
+                else
+                    std::snprintf(line, sizeof line,
+                                  "%s %s %dx%dx%d: split %s, lines %s, %d candidates, %.4f ms (default %.4f ms)\n", pn,
+                                  pr, kv.first.nx, kv.first.ny, kv.first.nz, sp, ln, kv.second.candidates,
+                                  kv.second.ms, kv.second.ms_default);
                 out += line;
             }
         }

@@ -128,7 +128,8 @@ int cl_last_timings(cl_ctx* ctx, double t[4]);
  * tuning sample next to the default variant's.  Writes at most len bytes (NUL-terminated) to
  * buf when buf is non-null; *needed (if non-null) receives the full size.  No reference
  * counterpart: the reference plans its FFTs with FFTW_MEASURE / FFTW_ESTIMATE
- * (CoulombCalculator.cpp:17-39).  CL_AUTOTUNE=0 in the environment disables tuning. */
+ * (CoulombCalculator.cpp:17-39).  CL_AUTOTUNE=0 in the environment disables tuning;
+ * CL_TUNE_FILE=<path> loads earlier choices from that file and appends new ones to it. */
 int cl_autotune_report(char* buf, int64_t len, int64_t* needed);
 
 /* Per-kernel timing with CUDA events recorded on the context's stream around every launch.

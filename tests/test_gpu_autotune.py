@@ -84,3 +84,39 @@ def test_tuned_choice_is_reported_and_agrees(mode, monkeypatch):
     default = run()
     tol = 1e-12 if mode == cl.MODE_FP64_PLAIN else 1e-6
     assert np.abs(tuned - default).max() <= tol * np.abs(default).max()
+
+
+def test_tune_file_persists_choices(tmp_path):
+    """CL_TUNE_FILE: a first process appends its choices; a second one loads them instead of
+    timing, and computes the same values."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = (
+        "import sys, numpy as np\n"
+        "sys.path.insert(0, %r)\n"
+        "import coulombo_lattice_b200 as cl\n"
+        "from coulombo_lattice_b200 import synth\n"
+        "d = synth.build('c1', cells=(10, 12, 8))\n"
+        "specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals('****', 4, 2)]\n"
+        "with cl.CoulombCalculator(d['dims'], (synth.A_ZB / 4,) * 3, cl.MODE_FP32_FOURIER) as cc:\n"
+        "    cc.initialize(dielectric=10.89)\n"
+        "    cc.set_states(d['states'], d['cells_idx'], 2)\n"
+        "    v = cc.compute(specs)\n"
+        "np.save(sys.argv[1], v)\n"
+        "print(cl.autotune_report())\n" % root)
+    env = dict(os.environ, CL_TUNE_FILE=str(tmp_path / "tune.txt"))
+    env.pop("CL_TUNE_FORCE", None)
+    env.pop("CL_AUTOTUNE", None)
+    r1 = subprocess.run([sys.executable, "-c", script, str(tmp_path / "a.npy")], env=env, capture_output=True,
+                        text=True, timeout=300)
+    assert r1.returncode == 0, r1.stderr
+    saved = (tmp_path / "tune.txt").read_text().split("\n")
+    assert len([ln for ln in saved if ln.strip()]) == 5  # one line per pass of the 40x48x32 shape
+    r2 = subprocess.run([sys.executable, "-c", script, str(tmp_path / "b.npy")], env=env, capture_output=True,
+                        text=True, timeout=300)
+    assert r2.returncode == 0, r2.stderr
+    assert r2.stdout.count("from CL_TUNE_FILE") == 5
+    a, b = np.load(tmp_path / "a.npy"), np.load(tmp_path / "b.npy")
+    np.testing.assert_allclose(b, a, rtol=1e-12, atol=0)
