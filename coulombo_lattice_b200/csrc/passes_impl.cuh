@@ -46,13 +46,12 @@ bool zconv(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, 
             using Tag = decltype(tag);
             with_lines<T>(v, [&](auto lines) {
                 constexpr int L = decltype(lines)::value;
-                constexpr int N = Tag::r1 * Tag::r2;
-                constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
+                constexpr int P = clk::ColShape<Tag::r1, Tag::r2>::P;
                 auto kern = clk::k_zconv_rf<T, Tag::r1, Tag::r2, L>;
-                const size_t smem = sizeof(cx<T>) * ((size_t)N + 2ull * N * L);
+                const size_t smem = clk::ZconvLayout<T, Tag::r1, Tag::r2, L>::smem;
                 set_smem(kern, smem);
                 const long long blocks = (nxy + L - 1) / L;
-                kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), L * Q, smem, s>>>(buf, M, tw, kh, nxy,
+                kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), L * P, smem, s>>>(buf, M, tw, kh, nxy,
                                                                                               cnt);
             });
         },
@@ -68,14 +67,13 @@ bool ycol(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, i
             using Tag = decltype(tag);
             with_lines<T>(v, [&](auto lines) {
                 constexpr int L = decltype(lines)::value;
-                constexpr int N = Tag::r1 * Tag::r2;
-                constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
+                constexpr int P = clk::ColShape<Tag::r1, Tag::r2>::P;
                 auto kern = clk::k_ycol_rf<S, T, Tag::r1, Tag::r2, L>;
-                const size_t smem = sizeof(cx<T>) * ((size_t)N + (size_t)N * L);
+                const size_t smem = clk::YcolLayout<T, Tag::r1, Tag::r2, L>::smem;
                 set_smem(kern, smem);
                 const int xchunks = (nx + L - 1) / L;
                 const long long blocks = (long long)xchunks * nz;
-                kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), L * Q, smem, s>>>(buf, M, tw, nx, ny,
+                kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), L * P, smem, s>>>(buf, M, tw, nx, ny,
                                                                                               xchunks, cnt, row_ptr);
             });
         },

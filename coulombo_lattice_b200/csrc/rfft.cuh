@@ -35,151 +35,279 @@ struct col_min_blocks {
 };
 
 // ---------------------------------------------------------------------------------------
-// z pass: forward FFT along z, x Khat, inverse FFT along z; block = L adjacent xy columns,
-// densities [blockIdx.y * per, ...).
+// Thread layout of the column passes.  A line of N = R1*R2 points has R2 phase-A items
+// (R1-point DFTs) and R1 phase-B items (R2-point DFTs).  When one factor divides the other,
+// P = the smaller factor threads serve a line and each takes IA = R2/P phase-A items and
+// IB = R1/P phase-B items, so no thread idles at the barriers between the phases; otherwise
+// P = the larger factor and the threads beyond a phase's item count sit that phase out.
+// ---------------------------------------------------------------------------------------
+template <int R1, int R2>
+struct ColShape {
+    static constexpr int lo = R1 < R2 ? R1 : R2;
+    static constexpr int hi = R1 < R2 ? R2 : R1;
+    static constexpr int P = (hi % lo == 0) ? lo : hi;
+    static constexpr int IA = (R2 + P - 1) / P;
+    static constexpr int IB = (R1 + P - 1) / P;
+};
+
+// Minimum resident blocks of the column passes when a factor is a radix-16 codelet: about 512
+// threads per SM in FP32 (<= 128 registers a thread) and 256 in FP64 (<= 256, room for the
+// 16-point butterflies and the prefetched column without spilling); otherwise the compiler's
+// choice.
+template <typename T, int R1, int R2, int THREADS>
+struct colp_min_blocks {
+    static constexpr int per_sm = sizeof(T) == 4 ? 512 : 256;
+    static constexpr int value = (R1 >= 16 || R2 >= 16) ? (per_sm / THREADS > 0 ? per_sm / THREADS : 1) : 0;
+};
+
+// Point pitch LP of an exchange buffer [pos][line] (address pos*LP + line), written at
+// pos = q*RW + r by items q < QW and read at pos = q + r*RW by items q < QR: the pitch in
+// [L, L + W) with the fewest bank conflicts over the thread groups served by one
+// shared-memory wavefront (W = 128 B / element; the r terms shift every thread alike).
+template <int L, int P, int RW, int QW, int QR, int ES>
+struct ColPitch {
+    static constexpr int W = 128 / ES;
+    static constexpr int degree(int lp, int write) {
+        int worst = 0;
+        for (int g0 = 0; g0 < L * P; g0 += W) {
+            int count[32] = {};
+            for (int tid = g0; tid < g0 + W && tid < L * P; ++tid) {
+                const int line = tid % L, q = tid / L;
+                if (q >= (write ? QW : QR)) continue;
+                const int pos = write ? q * RW : q;
+                const int slot = (pos * lp + line) % W;
+                if (++count[slot] > worst) worst = count[slot];
+            }
+        }
+        return worst;
+    }
+    static constexpr int pick() {
+        int best = L, bd = 1 << 30;
+        for (int lp = L; lp < L + W; ++lp) {
+            const int d = degree(lp, 1) > degree(lp, 0) ? degree(lp, 1) : degree(lp, 0);
+            if (d < bd) {
+                bd = d;
+                best = lp;
+            }
+        }
+        return best;
+    }
+    static constexpr int LP = pick();
+};
+
+template <typename T, int R1, int R2, int L>
+struct ZconvLayout {
+    using S = ColShape<R1, R2>;
+    static constexpr int LP0 = ColPitch<L, S::P, R1, R2, R1, sizeof(cx<T>)>::LP;  // phase A -> B
+    static constexpr int LP1 = ColPitch<L, S::P, R2, R1, R2, sizeof(cx<T>)>::LP;  // phase B -> C
+    static constexpr size_t smem = sizeof(cx<T>) * ((size_t)R1 * R2 * (1 + LP0 + LP1));
+};
+
+template <typename T, int R1, int R2, int L>
+struct YcolLayout {
+    using S = ColShape<R1, R2>;
+    static constexpr int LP0 = ColPitch<L, S::P, R1, R2, R1, sizeof(cx<T>)>::LP;
+    static constexpr size_t smem = sizeof(cx<T>) * ((size_t)R1 * R2 * (1 + LP0));
+};
+
+// ---------------------------------------------------------------------------------------
+// z pass: forward FFT along z, x Khat, inverse FFT along z; block = L adjacent xy columns
+// x P threads, densities [blockIdx.y * per, ...).
 // ---------------------------------------------------------------------------------------
 template <typename T, int R1, int R2, int L>
-__global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2, L * cmax<R1, R2>::value>::value)
+__global__ void __launch_bounds__(L * ColShape<R1, R2>::P, colp_min_blocks<T, R1, R2, L * ColShape<R1, R2>::P>::value)
     k_zconv_rf(cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g,
                const T* __restrict__ khat, long long nxy, int np) {
-    constexpr int N = R1 * R2;
+    using S = ColShape<R1, R2>;
+    using Lay = ZconvLayout<T, R1, R2, L>;
+    constexpr int N = R1 * R2, P = S::P, IA = S::IA, IB = S::IB, LP0 = Lay::LP0, LP1 = Lay::LP1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* s0 = tw + N;
-    cx<T>* s1 = s0 + N * L;
+    cx<T>* s1 = s0 + N * LP0;
     const int line = threadIdx.x % L;
-    const int q = threadIdx.x / L;
+    const int qt = threadIdx.x / L;
     const long long c = (long long)blockIdx.x * L + line;
     const bool valid = c < nxy;
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
-    T kv[R2];
+    // Khat of the positions q + r*R1 that phase-B item q holds, for all densities
+    T kv[IB][R2];
 #pragma unroll
-    for (int r = 0; r < R2; ++r) kv[r] = (q < R1 && valid) ? khat[(long long)(q + r * R1) * nxy + c] : T(0);
+    for (int b = 0; b < IB; ++b) {
+        const int q = qt + b * P;
+#pragma unroll
+        for (int r = 0; r < R2; ++r) kv[b][r] = (q < R1 && valid) ? khat[(long long)(q + r * R1) * nxy + c] : T(0);
+    }
     __syncthreads();
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
     // the next density's column is loaded into registers while the current one is transformed
-    const auto load = [&](int p, cx<T>(&v)[R1]) {
+    const auto load = [&](int p, cx<T>(&v)[IA][R1]) {
         const cx<T>* src = buf + (long long)p * stride + c;
 #pragma unroll
-        for (int j = 0; j < R1; ++j) v[j] = valid ? src[(long long)(q + R2 * j) * nxy] : mk(T(0), T(0));
+        for (int a = 0; a < IA; ++a) {
+            const int q = qt + a * P;
+#pragma unroll
+            for (int j = 0; j < R1; ++j)
+                v[a][j] = (valid && q < R2) ? src[(long long)(q + R2 * j) * nxy] : mk(T(0), T(0));
+        }
     };
-    cx<T> v[R1], vn[R1];
-    if (q < R2 && p_begin < p_end) load(p_begin, v);
+    cx<T> v[IA][R1], vn[IA][R1];
+    if (p_begin < p_end) load(p_begin, v);
     for (int p = p_begin; p < p_end; ++p) {
         cx<T>* base = buf + (long long)p * stride + c;
-        if (q < R2 && p + 1 < p_end) load(p + 1, vn);
-        if (q < R2) {
-            dft<R1, -1>(v);
+        if (p + 1 < p_end) load(p + 1, vn);
 #pragma unroll
-            for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * L + line] = v[r];
+        for (int a = 0; a < IA; ++a) {
+            const int q = qt + a * P;
+            if (q < R2) {
+                dft<R1, -1>(v[a]);
+#pragma unroll
+                for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * LP0 + line] = v[a][r];
+            }
         }
         __syncthreads();
-        if (q < R1) {
-            cx<T> u[R2];
 #pragma unroll
-            for (int r = 0; r < R2; ++r) u[r] = s0[(q + r * R1) * L + line];
+        for (int b = 0; b < IB; ++b) {
+            const int q = qt + b * P;
+            if (q < R1) {
+                cx<T> u[R2];
 #pragma unroll
-            for (int r = 1; r < R2; ++r) u[r] = cmul(u[r], tw[r * q]);
-            dft<R2, -1>(u);
+                for (int r = 0; r < R2; ++r) u[r] = s0[(q + r * R1) * LP0 + line];
 #pragma unroll
-            for (int r = 0; r < R2; ++r) u[r] = mk(u[r].re * kv[r], u[r].im * kv[r]);
-            dft<R2, +1>(u);
+                for (int r = 1; r < R2; ++r) u[r] = cmul(u[r], tw[r * q]);
+                dft<R2, -1>(u);
 #pragma unroll
-            for (int r = 0; r < R2; ++r) s1[(q * R2 + r) * L + line] = u[r];
+                for (int r = 0; r < R2; ++r) u[r] = mk(u[r].re * kv[b][r], u[r].im * kv[b][r]);
+                dft<R2, +1>(u);
+#pragma unroll
+                for (int r = 0; r < R2; ++r) s1[(q * R2 + r) * LP1 + line] = u[r];
+            }
         }
         __syncthreads();
-        if (q < R2) {
-            cx<T> w[R1];
 #pragma unroll
-            for (int r = 0; r < R1; ++r) w[r] = s1[(q + r * R2) * L + line];
+        for (int a = 0; a < IA; ++a) {
+            const int q = qt + a * P;
+            if (q < R2) {
+                cx<T> w[R1];
 #pragma unroll
-            for (int r = 1; r < R1; ++r) w[r] = cmulc(w[r], tw[r * q]);
-            dft<R1, +1>(w);
-            if (valid) {
+                for (int r = 0; r < R1; ++r) w[r] = s1[(q + r * R2) * LP1 + line];
 #pragma unroll
-                for (int r = 0; r < R1; ++r) base[(long long)(q + R2 * r) * nxy] = w[r];
+                for (int r = 1; r < R1; ++r) w[r] = cmulc(w[r], tw[r * q]);
+                dft<R1, +1>(w);
+                if (valid) {
+#pragma unroll
+                    for (int r = 0; r < R1; ++r) base[(long long)(q + R2 * r) * nxy] = w[r];
+                }
             }
         }
 #pragma unroll
-        for (int j = 0; j < R1; ++j) v[j] = vn[j];
+        for (int a = 0; a < IA; ++a)
+#pragma unroll
+            for (int j = 0; j < R1; ++j) v[a][j] = vn[a][j];
     }
 }
 
 // ---------------------------------------------------------------------------------------
-// y pass (one direction): block = L adjacent x of one z-plane, densities
+// y pass (one direction): block = L adjacent x of one z-plane x P threads, densities
 // [blockIdx.y * per, ...).
 // ---------------------------------------------------------------------------------------
 template <int S, typename T, int R1, int R2, int L>
-__global__ void __launch_bounds__(L * cmax<R1, R2>::value, col_min_blocks<R1, R2, L * cmax<R1, R2>::value>::value)
+__global__ void __launch_bounds__(L * ColShape<R1, R2>::P, colp_min_blocks<T, R1, R2, L * ColShape<R1, R2>::P>::value)
     k_ycol_rf(cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g, int nx, int ny,
               int xchunks, int np, const int* __restrict__ row_ptr) {
-    constexpr int N = R1 * R2;
+    using Sh = ColShape<R1, R2>;
+    constexpr int N = R1 * R2, P = Sh::P, IA = Sh::IA, IB = Sh::IB;
+    constexpr int LP0 = YcolLayout<T, R1, R2, L>::LP0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* s0 = tw + N;
     const int line = threadIdx.x % L;
-    const int q = threadIdx.x / L;
+    const int qt = threadIdx.x / L;
     const int xc = blockIdx.x % xchunks, z = blockIdx.x / xchunks;
     const int x = xc * L + line;
     const bool valid = x < nx;
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
     // Rows (y, z) without atoms: after the forward x pass they are zero and were not stored;
     // after the inverse y pass nothing reads them.  row_ptr == nullptr: every row is live.
-    unsigned live_in = 0, live_out = 0;
-    if (q < R2) {
+    unsigned live_in[IA], live_out[IB];
 #pragma unroll
-        for (int j = 0; j < R1; ++j) {
-            const int r = z * ny + q + R2 * j;
-            if (!row_ptr || row_ptr[r + 1] > row_ptr[r]) live_in |= 1u << j;
+    for (int a = 0; a < IA; ++a) {
+        const int q = qt + a * P;
+        live_in[a] = 0;
+        if (q < R2) {
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const int r = z * ny + q + R2 * j;
+                if (!row_ptr || row_ptr[r + 1] > row_ptr[r]) live_in[a] |= 1u << j;
+            }
         }
     }
-    if (q < R1) {
 #pragma unroll
-        for (int j = 0; j < R2; ++j) {
-            const int r = z * ny + q + j * R1;
-            if (!row_ptr || row_ptr[r + 1] > row_ptr[r]) live_out |= 1u << j;
+    for (int b = 0; b < IB; ++b) {
+        const int q = qt + b * P;
+        live_out[b] = 0;
+        if (q < R1) {
+#pragma unroll
+            for (int j = 0; j < R2; ++j) {
+                const int r = z * ny + q + j * R1;
+                if (!row_ptr || row_ptr[r + 1] > row_ptr[r]) live_out[b] |= 1u << j;
+            }
         }
     }
     __syncthreads();
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
     // the next density's column is loaded into registers while the current one is transformed
-    const auto load = [&](int p, cx<T>(&v)[R1]) {
+    const auto load = [&](int p, cx<T>(&v)[IA][R1]) {
         const cx<T>* src = buf + (long long)p * stride + (long long)z * nx * ny + x;
 #pragma unroll
-        for (int j = 0; j < R1; ++j) {
-            const bool ld = valid && (S > 0 || ((live_in >> j) & 1u));
-            v[j] = ld ? src[(long long)(q + R2 * j) * nx] : mk(T(0), T(0));
+        for (int a = 0; a < IA; ++a) {
+            const int q = qt + a * P;
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const bool ld = valid && q < R2 && (S > 0 || ((live_in[a] >> j) & 1u));
+                v[a][j] = ld ? src[(long long)(q + R2 * j) * nx] : mk(T(0), T(0));
+            }
         }
     };
-    cx<T> v[R1], vn[R1];
-    if (q < R2 && p_begin < p_end) load(p_begin, v);
+    cx<T> v[IA][R1], vn[IA][R1];
+    if (p_begin < p_end) load(p_begin, v);
     for (int p = p_begin; p < p_end; ++p) {
         cx<T>* base = buf + (long long)p * stride + (long long)z * nx * ny + x;
-        if (q < R2 && p + 1 < p_end) load(p + 1, vn);
-        if (q < R2) {
-            dft<R1, S>(v);
+        if (p + 1 < p_end) load(p + 1, vn);
 #pragma unroll
-            for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * L + line] = v[r];
-        }
-        __syncthreads();
-        if (q < R1) {
-            cx<T> u[R2];
+        for (int a = 0; a < IA; ++a) {
+            const int q = qt + a * P;
+            if (q < R2) {
+                dft<R1, S>(v[a]);
 #pragma unroll
-            for (int r = 0; r < R2; ++r) u[r] = s0[(q + r * R1) * L + line];
-#pragma unroll
-            for (int r = 1; r < R2; ++r) u[r] = S < 0 ? cmul(u[r], tw[r * q]) : cmulc(u[r], tw[r * q]);
-            dft<R2, S>(u);
-            if (valid) {
-#pragma unroll
-                for (int r = 0; r < R2; ++r)
-                    if (S < 0 || ((live_out >> r) & 1u)) base[(long long)(q + r * R1) * nx] = u[r];
+                for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * LP0 + line] = v[a][r];
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < R1; ++j) v[j] = vn[j];
+        for (int b = 0; b < IB; ++b) {
+            const int q = qt + b * P;
+            if (q < R1) {
+                cx<T> u[R2];
+#pragma unroll
+                for (int r = 0; r < R2; ++r) u[r] = s0[(q + r * R1) * LP0 + line];
+#pragma unroll
+                for (int r = 1; r < R2; ++r) u[r] = S < 0 ? cmul(u[r], tw[r * q]) : cmulc(u[r], tw[r * q]);
+                dft<R2, S>(u);
+                if (valid) {
+#pragma unroll
+                    for (int r = 0; r < R2; ++r)
+                        if (S < 0 || ((live_out[b] >> r) & 1u)) base[(long long)(q + r * R1) * nx] = u[r];
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < IA; ++a)
+#pragma unroll
+            for (int j = 0; j < R1; ++j) v[a][j] = vn[a][j];
     }
 }
 
