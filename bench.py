@@ -440,20 +440,22 @@ def run_ours(args):
     out_h = torch.zeros(2 * n_int, dtype=torch.float64).pin_memory()
     h2d = coeff_h.numel() * 8 + cells_h.numel() * 8 + spec_h.numel() * 2
     d2h = out_h.numel() * 8
+    def e2e_step():
+        # one C-ABI call: coefficients and cells in (pinned host memory), integrals out; the
+        # coefficient upload overlaps the transforms (cl_compute_states)
+        calc.compute_states_raw(n, d["holes"], d["states"].shape[1], d["states"].shape[2], coeff_h.data_ptr(),
+                                cells_h.data_ptr(), n_int, spec_h.data_ptr(), out_h.data_ptr())
+
     for _ in range(2):
-        calc.set_states_raw(n, d["holes"], d["states"].shape[1], d["states"].shape[2], coeff_h.data_ptr(),
-                            cells_h.data_ptr())
-        calc.compute_raw(n_int, spec_h.data_ptr(), out_h.data_ptr())
+        e2e_step()
     barrier()
     e0 = time.perf_counter()
     for _ in range(args.steps):
-        calc.set_states_raw(n, d["holes"], d["states"].shape[1], d["states"].shape[2], coeff_h.data_ptr(),
-                            cells_h.data_ptr())
-        calc.compute_raw(n_int, spec_h.data_ptr(), out_h.data_ptr())
+        e2e_step()
     barrier()
     e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - e0) / args.steps)
     e2e_vals = out_h.numpy()[0::2] + 1j * out_h.numpy()[1::2]
-    if not np.allclose(e2e_vals, v32, rtol=1e-12, atol=0):
+    if not np.allclose(e2e_vals, v32, rtol=1e-9, atol=1e-15):
         raise RuntimeError("e2e results differ from the resident-input results")
 
     # ---- roofline of the dominant kernel --------------------------------------------------
@@ -504,7 +506,9 @@ def run_ours(args):
                        "timing": "device time of a CUDA-graph replay of the prepared request, best of 3",
                        "speedup_of_fp32_form": plain_ms / ms_per_step},
         "e2e": {"value": world * n_int / (e2e_ms / 1e3), "unit": "integrals/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms,
+                "call": "cl_compute_states from pinned host buffers (coefficient upload overlapped with the "
+                        "transforms), wall clock per call"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": bytes_k / launches_k,

@@ -57,6 +57,7 @@ SIGNATURES = [
     ("cl_potential_grid", _i, [_vp, _P(_d)]),
     ("cl_set_states", _i, [_vp, _i, _i, _i64, _i, _P(_d), _P(_i64)]),
     ("cl_compute", _i, [_vp, _i64, _P(ctypes.c_int16), _P(_d)]),
+    ("cl_compute_states", _i, [_vp, _i, _i, _i64, _i, _P(_d), _P(_i64), _i64, _P(ctypes.c_int16), _P(_d)]),
     ("cl_potentials", _i, [_vp, _P(_d)]),
     ("cl_last_timings", _i, [_vp, _P(_d)]),
     ("cl_autotune_report", _i, [ctypes.c_char_p, _i64, _P(_i64)]),
@@ -261,6 +262,29 @@ class CoulombCalculator:
         out = np.zeros(2 * s.shape[0])
         _check(lib().cl_compute(self._h, s.shape[0], _ptr(s, ctypes.c_int16), _ptr(out)))
         return out[0::2] + 1j * out[1::2]
+
+    def compute_states(self, states, cells, n_holes, specs):
+        """cl_compute_states: set_states + compute in one call, the coefficient upload
+        overlapped with the transforms."""
+        c = _cplx(states)
+        cl_ = np.ascontiguousarray(cells, dtype=np.int64)
+        n, a, o = c.shape
+        s = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
+        out = np.zeros(2 * s.shape[0])
+        _check(lib().cl_compute_states(self._h, n, int(n_holes), a, o, _ptr(c.view(np.float64)),
+                                       _ptr(cl_, ctypes.c_int64), s.shape[0], _ptr(s, ctypes.c_int16), _ptr(out)))
+        self.n_states, self.n_atoms = n, a
+        return out[0::2] + 1j * out[1::2]
+
+    def compute_states_raw(self, n_states, n_holes, n_atoms, n_orb, coeff_ptr, cells_ptr, n_int, spec_ptr,
+                           out_ptr):
+        """cl_compute_states on raw host addresses (e.g. pinned buffers)."""
+        _check(lib().cl_compute_states(self._h, int(n_states), int(n_holes), int(n_atoms), int(n_orb),
+                                       ctypes.cast(coeff_ptr, ctypes.POINTER(ctypes.c_double)),
+                                       ctypes.cast(cells_ptr, ctypes.POINTER(ctypes.c_int64)), int(n_int),
+                                       ctypes.cast(spec_ptr, ctypes.POINTER(ctypes.c_int16)),
+                                       ctypes.cast(out_ptr, ctypes.POINTER(ctypes.c_double))))
+        self.n_states, self.n_atoms = int(n_states), int(n_atoms)
 
     def compute_rounds(self, specs, round_mask):
         """Partial integrals over the rounds in round_mask (bit k = round kappa k)."""

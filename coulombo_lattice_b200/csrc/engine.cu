@@ -279,6 +279,9 @@ struct cl_ctx {
     DevBuf<int> cell_sorted, orig_sorted, row_ptr;
     long long live_rows = 0;           // rows (y, z) holding at least one atom
     std::vector<long long> atom_slot;  // input atom -> sorted (deduplicated) slot
+    std::vector<int64_t> cells_seen;   // the cells of the last load (an identical list skips the sort)
+    cudaStream_t copy_stream = nullptr;  // coefficient uploads of cl_compute_states
+    std::vector<cudaEvent_t> state_ev;   // one per state: its coefficients are on the device
 
     // work buffers, kept across requests (grown on demand)
     DevBuf<unsigned char> work;
@@ -307,6 +310,11 @@ struct cl_ctx {
     int64_t prof_launches[CL_NUM_KCLASS] = {};
 
     ~cl_ctx() {
+        if (copy_stream) {
+            cudaStreamSynchronize(copy_stream);
+            for (auto& e : state_ev) cudaEventDestroy(e);
+            cudaStreamDestroy(copy_stream);
+        }
         if (stream) {
             cudaStreamSynchronize(stream);
             for (auto& e : ev)
@@ -953,6 +961,9 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
 }
 
 void pair_launch(cl_ctx* c, const PairSetup& ps, cx<double>* rho) {
+    // the attribute is per kernel, so another setup (of another group or request) may have
+    // lowered it since this one was prepared
+    ensure_smem(clk::k_pair_density, ps.smem);
     cudaEvent_t e = prof_begin(c);
     clk::k_pair_density<<<ps.blocks, 256, ps.smem, c->stream>>>(c->coeff.p, c->n_atoms, c->n_orb,
                                                                c->orig_sorted.p, c->n_sorted, ps.prods.p, ps.np,
@@ -1140,53 +1151,77 @@ int cl_potential_grid(cl_ctx* c, double* V) {
     });
 }
 
+}  // extern "C"
+
+namespace {
+
+void check_states_args(int n_states, int n_holes, int64_t n_atoms, int n_orb, const double* coeff,
+                       const int64_t* cells) {
+    if (n_states <= 0 || n_holes < 0 || n_holes > n_states || n_atoms <= 0 || n_orb <= 0 || !coeff || !cells)
+        cl::fail(CL_ERR_ARGUMENT, "invalid states description");
+    if (n_atoms >= (1LL << 31)) cl::fail(CL_ERR_UNSUPPORTED, "too many atoms");
+}
+
+// Atoms sorted by cell; where several atoms share a cell the one listed last wins, as with
+// F[cell] = value in atom order (Product.cpp:16-30).  Builds the sorted cell list, the input
+// atom of each slot, the row CSR and the live-row count, and uploads them (synchronously).  A
+// list identical to the previous load's is not processed again.
+void load_cells(cl_ctx* c, int64_t n_atoms, const int64_t* cells) {
+    if ((int64_t)c->cells_seen.size() == n_atoms && c->n_sorted > 0 &&
+        std::memcmp(c->cells_seen.data(), cells, sizeof(int64_t) * (size_t)n_atoms) == 0)
+        return;
+    c->cells_seen.clear();
+    std::vector<int> order((size_t)n_atoms);
+    std::iota(order.begin(), order.end(), 0);
+    for (int64_t a = 0; a < n_atoms; ++a)
+        if (cells[a] < 0 || cells[a] >= c->M) cl::fail(CL_ERR_ARGUMENT, "atom %lld lies outside the grid", (long long)a);
+    bool sorted = true;
+    for (int64_t a = 1; a < n_atoms && sorted; ++a) sorted = cells[a - 1] < cells[a];
+    if (!sorted) std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells[x] < cells[y]; });
+    std::vector<int> cell_s, orig_s;
+    cell_s.reserve((size_t)n_atoms);
+    orig_s.reserve((size_t)n_atoms);
+    c->atom_slot.assign((size_t)n_atoms, 0);
+    for (size_t i = 0; i < order.size(); ++i) {
+        const int a = order[i];
+        if (!cell_s.empty() && cell_s.back() == (int)cells[a]) {
+            orig_s.back() = a;  // later atom of the same cell replaces the earlier one
+        } else {
+            cell_s.push_back((int)cells[a]);
+            orig_s.push_back(a);
+        }
+        c->atom_slot[a] = (long long)cell_s.size() - 1;
+    }
+    const int nx = c->n[0];
+    const int nrows = c->n[1] * c->n[2];
+    std::vector<int> rp((size_t)nrows + 1, 0);
+    for (int cs : cell_s) rp[cs / nx + 1]++;
+    for (int r = 0; r < nrows; ++r) rp[r + 1] += rp[r];
+    long long live = 0;
+    for (int r = 0; r < nrows; ++r) live += rp[r + 1] > rp[r];
+    c->live_rows = live;
+    c->n_sorted = (long long)cell_s.size();
+    c->cell_sorted.upload(cell_s.data(), cell_s.size(), c->stream);
+    c->orig_sorted.upload(orig_s.data(), orig_s.size(), c->stream);
+    c->row_ptr.upload(rp.data(), rp.size(), c->stream);
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    c->cells_seen.assign(cells, cells + n_atoms);
+}
+
+}  // namespace
+
+extern "C" {
+
 int cl_set_states(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_orb, const double* coeff,
                   const int64_t* cells) {
     return cl::guarded([&] {
         check_ctx(c);
-        if (n_states <= 0 || n_holes < 0 || n_holes > n_states || n_atoms <= 0 || n_orb <= 0 || !coeff || !cells)
-            cl::fail(CL_ERR_ARGUMENT, "invalid states description");
-        if (n_atoms >= (1LL << 31)) cl::fail(CL_ERR_UNSUPPORTED, "too many atoms");
-        // Sort atoms by cell; where several atoms share a cell the one listed last wins, as
-        // with F[cell] = value in atom order (Product.cpp:16-30).
-        std::vector<int> order((size_t)n_atoms);
-        std::iota(order.begin(), order.end(), 0);
-        for (int64_t a = 0; a < n_atoms; ++a)
-            if (cells[a] < 0 || cells[a] >= c->M) cl::fail(CL_ERR_ARGUMENT, "atom %lld lies outside the grid", (long long)a);
-        bool sorted = true;
-        for (int64_t a = 1; a < n_atoms && sorted; ++a) sorted = cells[a - 1] < cells[a];
-        if (!sorted)
-            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells[x] < cells[y]; });
-        std::vector<int> cell_s, orig_s;
-        cell_s.reserve((size_t)n_atoms);
-        orig_s.reserve((size_t)n_atoms);
-        c->atom_slot.assign((size_t)n_atoms, 0);
-        for (size_t i = 0; i < order.size(); ++i) {
-            const int a = order[i];
-            if (!cell_s.empty() && cell_s.back() == (int)cells[a]) {
-                orig_s.back() = a;  // later atom of the same cell replaces the earlier one
-            } else {
-                cell_s.push_back((int)cells[a]);
-                orig_s.push_back(a);
-            }
-            c->atom_slot[a] = (long long)cell_s.size() - 1;
-        }
-        const int nx = c->n[0];
-        const int nrows = c->n[1] * c->n[2];
-        std::vector<int> rp((size_t)nrows + 1, 0);
-        for (int cs : cell_s) rp[cs / nx + 1]++;
-        for (int r = 0; r < nrows; ++r) rp[r + 1] += rp[r];
-        long long live = 0;
-        for (int r = 0; r < nrows; ++r) live += rp[r + 1] > rp[r];
-        c->live_rows = live;
+        check_states_args(n_states, n_holes, n_atoms, n_orb, coeff, cells);
+        load_cells(c, n_atoms, cells);
         c->n_states = n_states;
         c->n_holes = n_holes;
         c->n_orb = n_orb;
         c->n_atoms = n_atoms;
-        c->n_sorted = (long long)cell_s.size();
-        c->cell_sorted.upload(cell_s.data(), cell_s.size(), c->stream);
-        c->orig_sorted.upload(orig_s.data(), orig_s.size(), c->stream);
-        c->row_ptr.upload(rp.data(), rp.size(), c->stream);
         c->coeff.upload(reinterpret_cast<const cx<double>*>(coeff), (size_t)n_states * n_atoms * n_orb, c->stream);
         CL_CUDA(cudaStreamSynchronize(c->stream));
     });
@@ -1281,9 +1316,162 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         }
     }
 }
+
+// cl_compute_states: the states' coefficients are uploaded one state at a time on a copy stream
+// while the densities whose states have arrived are transformed.  Left densities are grouped by
+// their higher state index; a group's pair densities and rounds wait only for its last state.
+void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_orb, const double* coeff,
+                         const int64_t* cells, int64_t n_int, const int16_t* spec, double* out) {
+    check_ctx(c);
+    check_kernel(c);
+    check_states_args(n_states, n_holes, n_atoms, n_orb, coeff, cells);
+    if (n_int < 0 || (n_int && (!spec || !out))) cl::fail(CL_ERR_ARGUMENT, "invalid integral list");
+    load_cells(c, n_atoms, cells);
+    c->n_states = n_states;
+    c->n_holes = n_holes;
+    c->n_orb = n_orb;
+    c->n_atoms = n_atoms;
+    const size_t per_state = (size_t)n_atoms * n_orb;
+    grow(c->coeff, (size_t)n_states * per_state);
+    std::memset(c->timings, 0, sizeof c->timings);
+    if (!c->copy_stream) CL_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    while ((int)c->state_ev.size() < n_states) {
+        cudaEvent_t e;
+        CL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->state_ev.push_back(e);
+    }
+    if (n_int == 0) {
+        CL_CUDA(cudaMemcpyAsync(c->coeff.p, coeff, sizeof(cx<double>) * n_states * per_state, cudaMemcpyHostToDevice,
+                                c->stream));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        return;
+    }
+    std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
+    for (int64_t i = 0; i < n_int; ++i)
+        for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
+    const auto plan = cl::orient_steps(n_states, specs);
+    const int P = n_states * (n_states + 1) / 2;
+    std::vector<int> is_left(P, 0), is_right(P, 0);
+    for (const auto& st : plan) {
+        is_left[st.left.product] = 1;
+        is_right[st.right.product] = 1;
+    }
+    // product -> (higher, lower) 0-based state
+    auto states_of = [](int p) {
+        int a, b;
+        cl::product_states(p, &a, &b);
+        return std::make_pair(a - 1, b - 1);
+    };
+    // left densities ordered by their higher state (stable), then right-only densities
+    std::vector<int> lefts, prods, slot(P, -1);
+    for (int p = 0; p < P; ++p)
+        if (is_left[p]) lefts.push_back(p);
+    std::stable_sort(lefts.begin(), lefts.end(),
+                     [&](int x, int y) { return states_of(x).first < states_of(y).first; });
+    for (int p : lefts) { slot[p] = (int)prods.size(); prods.push_back(p); }
+    const int nl = (int)lefts.size();
+    for (int p = 0; p < P; ++p)
+        if (is_right[p] && slot[p] < 0) { slot[p] = (int)prods.size(); prods.push_back(p); }
+    std::vector<int> rights, rcol(P, -1);
+    for (int p = 0; p < P; ++p)
+        if (is_right[p]) { rcol[p] = (int)rights.size(); rights.push_back(slot[p]); }
+    const int nu = (int)prods.size(), nr = (int)rights.size();
+    // groups of left densities: cut at a state boundary once a group holds nl/6 densities
+    struct Group {
+        int begin, end, last_state;
+        PairSetup ps;
+    };
+    std::vector<std::unique_ptr<Group>> groups;
+    const int min_group = std::max(1, nl / 6);
+    for (int i = 0; i < nl;) {
+        int j = i;
+        int hi = states_of(prods[i]).first;
+        while (j < nl && (j - i < min_group || states_of(prods[j]).first == hi)) {
+            hi = std::max(hi, states_of(prods[j]).first);
+            ++j;
+        }
+        auto g = std::make_unique<Group>();
+        g->begin = i;
+        g->end = j;
+        g->last_state = hi;
+        groups.push_back(std::move(g));
+        i = j;
+    }
+    auto pairs_of = [&](int b, int e) {
+        std::vector<int2> fl;
+        for (int i = b; i < e; ++i) {
+            const auto st = states_of(prods[i]);
+            fl.push_back(make_int2(st.first, st.second));
+        }
+        return fl;
+    };
+    for (auto& g : groups) pair_setup(c, pairs_of(g->begin, g->end), g->ps);
+    PairSetup ps_right;
+    if (nu > nl) pair_setup(c, pairs_of(nl, nu), ps_right);
+    const long long As = c->n_sorted;
+    DevBuf<int>& dr = c->req_ridx;
+    grow(dr, rights.size());
+    CL_CUDA(cudaMemcpyAsync(dr.p, rights.data(), rights.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    DevBuf<cx<double>>& rho = c->req_rho;
+    DevBuf<cx<double>>& V = c->req_V;
+    grow(rho, (size_t)nu * As);
+    grow(V, (size_t)nl * As);
+    DevBuf<double>& o4 = c->req_o4;
+    grow(o4, (size_t)4 * nl * nr + 1);
+    tc_reserve(c, nl, nr, As);
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    // uploads, one state at a time, in the order the groups need them
+    CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    CL_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev[0], 0));
+    for (int sidx = 0; sidx < n_states; ++sidx) {
+        CL_CUDA(cudaMemcpyAsync(c->coeff.p + sidx * per_state, coeff + 2 * sidx * per_state,
+                                sizeof(cx<double>) * per_state, cudaMemcpyHostToDevice, c->copy_stream));
+        CL_CUDA(cudaEventRecord(c->state_ev[sidx], c->copy_stream));
+    }
+    for (auto& g : groups) {
+        CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[g->last_state], 0));
+        pair_launch(c, g->ps, rho.p + (long long)g->begin * As);
+        run_rounds_mode(c, rho.p + (long long)g->begin * As, As, g->end - g->begin, c->row_ptr.p, c->cell_sorted.p,
+                        V.p + (long long)g->begin * As, As);
+    }
+    CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[n_states - 1], 0));
+    if (nu > nl) pair_launch(c, ps_right, rho.p + (long long)nl * As);
+    CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    gram(c, V.p, As, nl, rho.p, As, dr.p, nr, As, o4.p);
+    CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    std::vector<double> h((size_t)4 * nl * nr + 1);
+    CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    check_gram_slot(h.back());
+    float t02, t23, t03;
+    CL_CUDA(cudaEventElapsedTime(&t02, c->ev[0], c->ev[2]));
+    CL_CUDA(cudaEventElapsedTime(&t23, c->ev[2], c->ev[3]));
+    CL_CUDA(cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]));
+    c->timings[0] = 0;  // pair densities are interleaved with the uploads and the rounds
+    c->timings[1] = t02;
+    c->timings[2] = t23;
+    c->timings[3] = t03;
+    prof_collect(c);
+    for (const auto& st : plan) {
+        const int l = slot[st.left.product], r = rcol[st.right.product];
+        const double* q = &h[((size_t)l * nr + r) * 4];
+        const bool rconj = st.left.conjugate != st.right.conjugate;
+        double re = rconj ? q[0] + q[1] : q[0] - q[1];
+        double im = rconj ? q[3] - q[2] : q[2] + q[3];
+        if (st.left.conjugate) im = -im;
+        out[2 * st.id] = re;
+        out[2 * st.id + 1] = im;
+    }
+}
 }  // namespace
 
 extern "C" {
+
+int cl_compute_states(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_orb, const double* coeff,
+                      const int64_t* cells, int64_t n_int, const int16_t* spec, double* out) {
+    return cl::guarded(
+        [&] { compute_states_impl(c, n_states, n_holes, n_atoms, n_orb, coeff, cells, n_int, spec, out); });
+}
 
 int cl_compute(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out) {
     return cl::guarded([&] { compute_impl(c, n_int, spec, out, 0xFF); });

@@ -106,6 +106,16 @@ int cl_set_states(cl_ctx* ctx, int n_states, int n_holes, int64_t n_atoms, int n
  * coulombo.cpp:186-209).  Replaces the whole "Computing requested integrals" phase. */
 int cl_compute(cl_ctx* ctx, int64_t n_int, const int16_t* spec, double* out);
 
+/* cl_set_states followed by cl_compute in one call, with the coefficient upload overlapped
+ * with the transforms: the states are copied one at a time on a second stream, and each
+ * group of left densities starts its pair densities and rounds as soon as its last state has
+ * arrived.  Same arguments, results and errors as the two calls; the coefficient buffer is only
+ * read during the call (pinned host memory lets the copies run asynchronously).  A cell list
+ * identical to the previous call's is not sorted or uploaded again.  No reference counterpart:
+ * the reference reads every file before computing (coulombo.cpp:99-117, 186-209). */
+int cl_compute_states(cl_ctx* ctx, int n_states, int n_holes, int64_t n_atoms, int n_orb, const double* coeff,
+                      const int64_t* cells, int64_t n_int, const int16_t* spec, double* out);
+
 /* V of every state's own density |psi_s|^2 (real part) at every atom, out[state][atom].
  * Replaces the loop of potentials.cpp:137-158 (createSelfProducts, prepare,
  * extractAtomCellValues at src/FunctionCollection.cpp:122-131). */

@@ -252,3 +252,53 @@ def test_prepared_request_follows_new_coefficients(mode):
         assert np.abs(want - first).max() > 1e-6 * np.abs(first).max()
         batch.close()
         req.close()
+
+
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+def test_compute_states_overlapped_matches(mode):
+    """cl_compute_states (upload overlapped with the transforms, densities grouped by state)
+    gives the values of cl_set_states + cl_compute, on a first call and on a repeat with the same
+    cells and new coefficients; the oracle agrees."""
+    d = synth.build("c2", cells=(5, 6, 4))
+    d["states"] = d["states"][:, :, :6]
+    step = (synth.A_ZB / 4,) * 3
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("eeee,hhhh,ehhe,eheh", 12, 6)]
+    other = synth.make_states(d["pos"], 6, 12, 4242, "gauss")
+    with cl.CoulombCalculator(d["dims"], step, mode) as cc:
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], 6)
+        want = cc.compute(specs)
+        got = cc.compute_states(d["states"], d["cells_idx"], 6, specs)
+        np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-15)
+        got2 = cc.compute_states(other, d["cells_idx"], 6, specs)
+        cc.set_states(other, d["cells_idx"], 6)
+        np.testing.assert_allclose(got2, cc.compute(specs), rtol=1e-9, atol=1e-15)
+    err, lim = gate(got, _oracle_values(d, specs), mode)
+    assert np.all(err <= lim), (err / lim).max()
+
+
+def test_graph_batch_of_requests_with_different_state_counts():
+    """A batch whose requests stage different numbers of states per atom chunk (different
+    shared-memory sizes of the pair-density kernel) runs each request as prepared."""
+    step = (synth.A_ZB / 4,) * 3
+    calcs, reqs, wants = [], [], []
+    for n_states, cells in [(8, (4, 4, 3)), (4, (3, 4, 4)), (6, (4, 3, 4))]:
+        d = synth.build("c3", cells=cells)
+        d["states"] = d["states"][:n_states, :, :5]
+        holes = n_states // 2
+        specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", n_states, holes)]
+        cc = cl.CoulombCalculator(d["dims"], step, cl.MODE_FP32_FOURIER)
+        cc.initialize(dielectric=10.89)
+        cc.set_states(d["states"], d["cells_idx"], holes)
+        wants.append(cc.compute(specs))
+        reqs.append(cc.request(specs))
+        calcs.append(cc)
+    batch = cl.Batch(reqs)
+    for _ in range(2):
+        for got, want in zip(batch.run(), wants):
+            np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-15)
+    batch.close()
+    for r in reqs:
+        r.close()
+    for cc in calcs:
+        cc.close()
