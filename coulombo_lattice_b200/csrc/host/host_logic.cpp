@@ -2,6 +2,7 @@
 #include "host_logic.hpp"
 
 #include <algorithm>
+#include <cstdint>
 #include <cctype>
 #include <cmath>
 #include <limits>
@@ -192,10 +193,28 @@ void product_states(int p, int* fl, int* fr) {
 // vertex of largest (degree, index) does.
 // ---------------------------------------------------------------------------------------
 std::set<int> vertex_cover(int vertex_count, const std::vector<std::pair<int, int>>& edge_list) {
-    // the distinct edges, in the set order of the reference (sorted pairs)
-    std::vector<std::pair<int, int>> edges(edge_list);
-    std::sort(edges.begin(), edges.end());
-    edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+    // the distinct edges, in the set order of the reference (sorted pairs): through a bitmap
+    // over the vertex pairs when it is small (one pass, no sort), else by sorting
+    std::vector<std::pair<int, int>> edges;
+    const size_t vc = (size_t)std::max(vertex_count, 0);
+    if (vc * vc <= (size_t{1} << 28)) {
+        std::vector<uint64_t> seen((vc * vc + 63) / 64, 0);
+        for (const auto& e : edge_list) {
+            if (e.first < 0 || e.second < 0 || e.first >= vertex_count || e.second >= vertex_count)
+                fail(CL_ERR_ARGUMENT, "edge vertex out of range");
+            const size_t bit = (size_t)e.first * vc + (size_t)e.second;
+            seen[bit >> 6] |= uint64_t{1} << (bit & 63);
+        }
+        for (size_t w = 0; w < seen.size(); ++w)
+            for (uint64_t m = seen[w]; m; m &= m - 1) {
+                const size_t bit = w * 64 + (size_t)__builtin_ctzll(m);
+                edges.push_back({(int)(bit / vc), (int)(bit % vc)});
+            }
+    } else {
+        edges = edge_list;
+        std::sort(edges.begin(), edges.end());
+        edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+    }
     std::set<int> cover;
     for (const auto& e : edges)
         if (e.first == e.second) cover.insert(e.first);
