@@ -71,12 +71,12 @@ void run(const clio::ParseResults& pr) {
     const clapp::KernelOptions kopt = clapp::kernel_options(pr, in);
     clapp::Calculator calc(in.pad, in.step, in.mode);
     clapp::check(cl_set_kernel_coulomb(calc.get(), in.dielectric, kopt.onsite, kopt.tf_lattice));
-    clapp::check(cl_set_states(calc.get(), input_count, holes, in.n_atoms, in.orbitals, in.coeff.data(),
-                               in.cells.data()));
 
+    // the coefficient upload overlaps the transforms (cl_compute_states)
     timer.start("Computing requested integrals");
     std::vector<double> values((size_t)count * 2, 0.0);
-    clapp::check(cl_compute(calc.get(), count, specs.data(), values.data()));
+    clapp::check(cl_compute_states(calc.get(), input_count, holes, in.n_atoms, in.orbitals, in.coeff.data(),
+                                   in.cells.data(), count, specs.data(), values.data()));
 
     timer.start("Exporting results");
     clio::write_integrals(in.output_dir, specs, values.data(), holes, electrons);

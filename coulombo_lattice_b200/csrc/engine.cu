@@ -1346,6 +1346,26 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
         CL_CUDA(cudaStreamSynchronize(c->stream));
         return;
     }
+    // Uploads, one state at a time on the copy stream.  From pinned memory they are all enqueued
+    // now and overlap the planning below; from pageable memory a copy returns only once staged,
+    // so they are interleaved with the groups that need them (the groups already enqueued run
+    // meanwhile).
+    CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    CL_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev[0], 0));
+    int uploaded = 0;
+    const auto upload_through = [&](int last) {
+        for (; uploaded <= last && uploaded < n_states; ++uploaded) {
+            CL_CUDA(cudaMemcpyAsync(c->coeff.p + uploaded * per_state, coeff + 2 * uploaded * per_state,
+                                    sizeof(cx<double>) * per_state, cudaMemcpyHostToDevice, c->copy_stream));
+            CL_CUDA(cudaEventRecord(c->state_ev[uploaded], c->copy_stream));
+        }
+    };
+    {
+        cudaPointerAttributes attr{};
+        if (cudaPointerGetAttributes(&attr, coeff) == cudaSuccess && attr.type == cudaMemoryTypeHost)
+            upload_through(n_states - 1);
+        cudaGetLastError();  // pageable memory is not an error
+    }
     std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
     for (int64_t i = 0; i < n_int; ++i)
         for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
@@ -1420,20 +1440,14 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     grow(o4, (size_t)4 * nl * nr + 1);
     tc_reserve(c, nl, nr, As);
     CL_CUDA(cudaStreamSynchronize(c->stream));
-    // uploads, one state at a time, in the order the groups need them
-    CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
-    CL_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev[0], 0));
-    for (int sidx = 0; sidx < n_states; ++sidx) {
-        CL_CUDA(cudaMemcpyAsync(c->coeff.p + sidx * per_state, coeff + 2 * sidx * per_state,
-                                sizeof(cx<double>) * per_state, cudaMemcpyHostToDevice, c->copy_stream));
-        CL_CUDA(cudaEventRecord(c->state_ev[sidx], c->copy_stream));
-    }
     for (auto& g : groups) {
+        upload_through(g->last_state);
         CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[g->last_state], 0));
         pair_launch(c, g->ps, rho.p + (long long)g->begin * As);
         run_rounds_mode(c, rho.p + (long long)g->begin * As, As, g->end - g->begin, c->row_ptr.p, c->cell_sorted.p,
                         V.p + (long long)g->begin * As, As);
     }
+    upload_through(n_states - 1);
     CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[n_states - 1], 0));
     if (nu > nl) pair_launch(c, ps_right, rho.p + (long long)nl * As);
     CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
