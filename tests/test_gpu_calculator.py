@@ -130,3 +130,28 @@ def test_register_row_passes_match_oracle(mode, dims):
         got = cc.calculate(F2)
     assert np.abs(Vg - V).max() <= TOL[mode] * 10 * np.abs(V).max()
     assert abs(got - want) <= TOL[mode] * 10 * np.sqrt(np.sum(np.abs(V) ** 2) * np.sum(np.abs(F2) ** 2))
+
+
+# lengths beyond the compiled two-factor splits (> 256) take the generic shared-memory passes,
+# mixed with register passes on the other axes
+GENERIC_SHAPES = [(288, 6, 5), (6, 270, 5), (5, 6, 300), (320, 4, 270)]
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("dims", GENERIC_SHAPES)
+def test_generic_passes_beyond_register_splits(mode, dims):
+    nx, ny, nz = dims
+    rng = np.random.default_rng(nx + 5 * ny + 9 * nz)
+    F = rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx))
+    F2 = rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx))
+    step = (0.7, 1.2, 1.0)
+    ghat = C.kernel_spectrum(C.kernel_octant(dims, step, dielectric=2.0), dims)
+    V = C.prepare(F, ghat)
+    want = C.calculate(V, F2)
+    with cl.CoulombCalculator(dims, step, mode) as cc:
+        cc.initialize(dielectric=2.0)
+        cc.prepare(F)
+        Vg = cc.potential()
+        got = cc.calculate(F2)
+    assert np.abs(Vg - V).max() <= TOL[mode] * 10 * np.abs(V).max()
+    assert abs(got - want) <= TOL[mode] * 10 * np.sqrt(np.sum(np.abs(V) ** 2) * np.sum(np.abs(F2) ** 2))
