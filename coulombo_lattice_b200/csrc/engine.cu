@@ -461,7 +461,7 @@ std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;
 bool g_tune_loaded = false;
 
-// CL_TUNE_FILE: choices persist across processes.  Lines "pass fp32 nx ny nz split half";
+// CL_TUNE_FILE: choices persist across processes.  Lines "pass fp32 nx ny nz split half pad";
 // the file is read once (before the first lookup) and every new choice is appended.
 const char* tune_file() {
     const char* f = std::getenv("CL_TUNE_FILE");
@@ -477,8 +477,8 @@ void tune_load_locked() {  // g_tune_mu held
     if (!fh) return;
     TuneKey k{};
     TuneEntry e;
-    while (std::fscanf(fh, "%d %d %d %d %d %d %d", &k.pass, &k.fp32, &k.nx, &k.ny, &k.nz, &e.v.split, &e.v.half) ==
-           7) {
+    while (std::fscanf(fh, "%d %d %d %d %d %d %d %d", &k.pass, &k.fp32, &k.nx, &k.ny, &k.nz, &e.v.split, &e.v.half,
+                       &e.v.pad) == 8) {
         if (k.pass < 0 || k.pass >= clp::kNumPasses) continue;
         e.candidates = 0;  // loaded, not timed in this process
         g_tune[k] = e;
@@ -490,7 +490,8 @@ void tune_save(const TuneKey& k, const TuneEntry& e) {
     const char* path = tune_file();
     if (!path) return;
     if (FILE* fh = std::fopen(path, "a")) {
-        std::fprintf(fh, "%d %d %d %d %d %d %d\n", k.pass, k.fp32, k.nx, k.ny, k.nz, e.v.split, e.v.half);
+        std::fprintf(fh, "%d %d %d %d %d %d %d %d\n", k.pass, k.fp32, k.nx, k.ny, k.nz, e.v.split, e.v.half,
+                     e.v.pad);
         std::fclose(fh);
     }
 }
@@ -503,9 +504,9 @@ bool autotune_enabled() {
 bool register_passes_enabled() { return !std::getenv("CL_NO_REGISTER_FFT"); }
 
 clp::Variant tuned_variant(const cl_ctx* c, int pass, bool fp32) {
-    if (const char* f = std::getenv("CL_TUNE_FORCE")) {  // "split,half": one variant for every pass
+    if (const char* f = std::getenv("CL_TUNE_FORCE")) {  // "split,half[,pad]": one variant for every pass
         clp::Variant v;
-        if (std::sscanf(f, "%d,%d", &v.split, &v.half) == 2) return v;
+        if (std::sscanf(f, "%d,%d,%d", &v.split, &v.half, &v.pad) >= 2) return v;
     }
     std::lock_guard<std::mutex> g(g_tune_mu);
     tune_load_locked();
@@ -531,8 +532,10 @@ void tune_pass(cl_ctx* c, int pass, bool fp32, int len, F&& launch) {
         if (g_tune.count(key)) return;
     }
     std::vector<clp::Variant> cands;
+    const int pads = (fp32 && pass == clp::kXFwd) ? 2 : 1;
     for (int sv = 0; sv < clp::split_variants(len); ++sv)
-        for (int h = 0; h < (fp32 ? 2 : 1); ++h) cands.push_back(clp::Variant{sv, h});
+        for (int h = 0; h < (fp32 ? 2 : 1); ++h)
+            for (int pd = 0; pd < pads; ++pd) cands.push_back(clp::Variant{sv, h, pd});
     TuneEntry best;
     best.candidates = (int)cands.size();
     if (cands.size() >= 2) {
@@ -1823,13 +1826,14 @@ int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
                 const char* pr = kv.first.fp32 ? "fp32" : "fp64";
                 const char* sp = kv.second.v.split ? "swapped" : "balanced";
                 const char* ln = kv.second.v.half ? "half" : "default";
+                const char* pd = kv.second.v.pad ? ", padded tile" : "";
                 if (kv.second.candidates == 0)
-                    std::snprintf(line, sizeof line, "%s %s %dx%dx%d: split %s, lines %s, from CL_TUNE_FILE\n", pn, pr,
-                                  kv.first.nx, kv.first.ny, kv.first.nz, sp, ln);
+                    std::snprintf(line, sizeof line, "%s %s %dx%dx%d: split %s, lines %s%s, from CL_TUNE_FILE\n", pn,
+                                  pr, kv.first.nx, kv.first.ny, kv.first.nz, sp, ln, pd);
                 else
                     std::snprintf(line, sizeof line,
-                                  "%s %s %dx%dx%d: split %s, lines %s, %d candidates, %.4f ms (default %.4f ms)\n", pn,
-                                  pr, kv.first.nx, kv.first.ny, kv.first.nz, sp, ln, kv.second.candidates,
+                                  "%s %s %dx%dx%d: split %s, lines %s%s, %d candidates, %.4f ms (default %.4f ms)\n",
+                                  pn, pr, kv.first.nx, kv.first.ny, kv.first.nz, sp, ln, pd, kv.second.candidates,
                                   kv.second.ms, kv.second.ms_default);
                 out += line;
             }

@@ -1,7 +1,8 @@
 // Launchers of the register-FFT passes (rfft.cuh) for every compiled variant.
 //
 // A variant picks the radix split of the line length (the balanced split, or its two factors
-// swapped) and the lines per block (the default -- 16 for FP32, 8 for FP64 -- or half).  The
+// swapped), the lines per block (the default -- 16 for FP32, 8 for FP64 -- or half) and, for
+// the forward x pass, the layout of its tile.  The
 // autotuner in engine.cu times the variants of each pass on the request's own shapes and
 // keeps the fastest.  Each launcher returns false (nothing launched) when the length has no
 // compiled two-factor split; launch errors surface through cudaGetLastError.
@@ -22,7 +23,8 @@ using clk::cx;
 struct Variant {
     int split = 0;  // 0: the balanced split; 1: its factors swapped
     int half = 0;   // 1: half the default lines (rows) per block (FP32 only)
-    bool operator==(const Variant& o) const { return split == o.split && half == o.half; }
+    int pad = 0;    // forward x pass, FP32: 1 pads its tile one point in four
+    bool operator==(const Variant& o) const { return split == o.split && half == o.half && pad == o.pad; }
 };
 
 enum Pass { kXFwd = 0, kYFwd = 1, kZConv = 2, kYInv = 3, kXInv = 4, kNumPasses = 5 };

@@ -89,15 +89,26 @@ bool xfwd(cudaStream_t s, Variant v, const cx<double>* rho, long long rho_stride
         [&](auto tag) {
             using Tag = decltype(tag);
             with_lines<T>(v, [&](auto lines) {
-                constexpr int LR = decltype(lines)::value;
-                constexpr int N = Tag::r1 * Tag::r2;
-                constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
-                auto kern = clk::k_xfwd_rf<T, Tag::r1, Tag::r2, LR>;
-                const size_t smem = sizeof(cx<T>) * ((size_t)N + 2ull * N * (LR + 1));
-                set_smem(kern, smem);
-                const long long blocks = (nrows + LR - 1) / LR;
-                kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), LR * Q, smem, s>>>(
-                    rho, rho_stride, row_ptr, cell, buf, M, tw, rp, ny, nrows, cnt, skip_empty);
+                const auto launch = [&](auto pad) {
+                    constexpr int LR = decltype(lines)::value;
+                    constexpr bool PAD = decltype(pad)::value;
+                    constexpr int N = Tag::r1 * Tag::r2;
+                    constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
+                    auto kern = clk::k_xfwd_rf<T, Tag::r1, Tag::r2, LR, PAD>;
+                    const size_t smem =
+                        sizeof(cx<T>) * ((size_t)N + (size_t)(clk::XfwdTile<N, PAD>::points + N) * (LR + 1));
+                    set_smem(kern, smem);
+                    const long long blocks = (nrows + LR - 1) / LR;
+                    kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), LR * Q, smem, s>>>(
+                        rho, rho_stride, row_ptr, cell, buf, M, tw, rp, ny, nrows, cnt, skip_empty);
+                };
+                if constexpr (sizeof(T) == 4) {
+                    if (v.pad) {
+                        launch(std::true_type{});
+                        return;
+                    }
+                }
+                launch(std::false_type{});
             });
         },
         v.split);

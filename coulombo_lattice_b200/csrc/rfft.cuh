@@ -331,7 +331,17 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // Forward: scatter the rows' atoms x conj(phase_kappa), FFT along x, store whole rows.
-template <typename T, int R1, int R2, int LR>
+// The transposed tile holds point x of a row at pos(x)*(LR+1) + row.  With PAD there is one
+// spare point every 4 points, so that atoms 4 points apart along a row (zinc-blende) scatter
+// to distinct banks; dense rows then see 2-way conflicts instead, and the tile grows by a
+// quarter, so the autotuner decides per shape.
+template <int N, bool PAD>
+struct XfwdTile {
+    __host__ __device__ static constexpr int pos(int x) { return PAD ? x + x / 4 : x; }
+    static constexpr int points = pos(N - 1) + 1;
+};
+
+template <typename T, int R1, int R2, int LR, bool PAD>
 __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R2, LR * cmax<R1, R2>::value>::value)
     k_xfwd_rf(const cx<double>* __restrict__ rho, long long rho_stride, const int* __restrict__ row_ptr,
               const int* __restrict__ cell, cx<T>* __restrict__ out, long long out_stride,
@@ -339,9 +349,10 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
     constexpr int N = R1 * R2;
     constexpr int LP = LR + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    using Tile = XfwdTile<N, PAD>;
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* tile = tw + N;
-    cx<T>* ex = tile + N * LP;
+    cx<T>* ex = tile + Tile::points * LP;
     const int r0 = blockIdx.x * LR;
     const int nr = min(LR, nrows - r0);
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
@@ -369,13 +380,13 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             if (i < a1) {
                 const int c = cell[i];
                 const int row = c / N, x = c - row * N;
-                slot[k] = x * LP + (row - r0);
+                slot[k] = Tile::pos(x) * LP + (row - r0);
                 ph[k] = round_phase(rp, x, row % ny, row / ny);
             }
         }
     }
     // cells without an atom stay zero for every density: the tile is cleared once
-    for (int e = threadIdx.x; e < N * LP; e += blockDim.x) tile[e] = mk(T(0), T(0));
+    for (int e = threadIdx.x; e < Tile::points * LP; e += blockDim.x) tile[e] = mk(T(0), T(0));
     __syncthreads();
     // the next density's atom values are loaded into registers while the current one is
     // transformed
@@ -398,7 +409,7 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
                 const int c = cell[i];
                 const int row = c / N, x = c - row * N;
                 const int y = row % ny, z = row / ny;
-                tile[x * LP + (row - r0)] = narrow<T>(cmulc(rp_[i], round_phase(rp, x, y, z)));
+                tile[Tile::pos(x) * LP + (row - r0)] = narrow<T>(cmulc(rp_[i], round_phase(rp, x, y, z)));
             }
         }
         __syncthreads();
@@ -407,7 +418,7 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             if (t < R2) {
                 cx<T> v[R1];
 #pragma unroll
-                for (int j = 0; j < R1; ++j) v[j] = tile[(t + R2 * j) * LP + lr];
+                for (int j = 0; j < R1; ++j) v[j] = tile[Tile::pos(t + R2 * j) * LP + lr];
                 dft<R1, -1>(v);
 #pragma unroll
                 for (int r = 0; r < R1; ++r) ex[(t * R1 + r) * LP + lr] = v[r];
@@ -439,31 +450,39 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
 // and the one whose worst shared-memory bank conflict (over the thread groups served by one
 // wavefront, W = 128 B / element) is lowest is kept -- for the exchange (phase A writes
 // la*PP + ta*(R1+1) + r, phase B reads lb*PP + jb + r*(R1+1)) and for the natural-order rows
-// (phase B writes lb*NP + jb + r*R1).
+// (phase B writes point x = jb + r*R1 at lb*NP + pos(x)).
 template <int R1, int R2, int LR, int ES>
 struct XinvPitch {
     static constexpr int N = R1 * R2;
     static constexpr int Q = R1 > R2 ? R1 : R2;
     static constexpr int T = LR * Q;
     static constexpr int W = 128 / ES;
+    // Row position of point x: one pad slot after every W points, so that gathers of atoms
+    // spaced 1, 2 or 4 points apart along a row hit distinct banks.
+    __host__ __device__ static constexpr int pos(int x) { return x + x / W; }
     // worst number of distinct elements per bank slot over the wavefront groups;
     // which: 0 phase-A exchange write, 1 phase-B exchange read, 2 phase-B row write
     static constexpr int degree(int pitch, int which) {
         int worst = 0;
-        for (int g0 = 0; g0 < T; g0 += W) {
-            int count[32] = {};
-            for (int tid = g0; tid < g0 + W && tid < T; ++tid) {
-                int e = -1;
-                if (which == 0) {
-                    const int ta = tid % R2, la = tid / R2;
-                    if (la < LR) e = la * pitch + ta * (R1 + 1);
-                } else {
-                    const int jb = tid % R1, lb = tid / R1;
-                    if (lb < LR) e = lb * pitch + jb;  // the r terms shift every thread alike
-                }
-                if (e >= 0) {
-                    const int slot = e % W;
-                    if (++count[slot] > worst) worst = count[slot];
+        for (int r = 0; r < (which == 2 ? R2 : 1); ++r) {
+            for (int g0 = 0; g0 < T; g0 += W) {
+                int count[32] = {};
+                for (int tid = g0; tid < g0 + W && tid < T; ++tid) {
+                    int e = -1;
+                    if (which == 0) {
+                        const int ta = tid % R2, la = tid / R2;
+                        if (la < LR) e = la * pitch + ta * (R1 + 1);
+                    } else if (which == 1) {
+                        const int jb = tid % R1, lb = tid / R1;
+                        if (lb < LR) e = lb * pitch + jb;  // the r terms shift every thread alike
+                    } else {
+                        const int jb = tid % R1, lb = tid / R1;
+                        if (lb < LR) e = lb * pitch + pos(jb + r * R1);
+                    }
+                    if (e >= 0) {
+                        const int slot = e % W;
+                        if (++count[slot] > worst) worst = count[slot];
+                    }
                 }
             }
         }
@@ -482,12 +501,13 @@ struct XinvPitch {
         return best;
     }
     static constexpr int row_pitch() {
-        int best = N, bd = 1 << 30;
+        const int base = pos(N - 1) + 1;
+        int best = base, bd = 1 << 30;
         for (int pad = 0; pad < W; ++pad) {
-            const int d = degree(N + pad, 2);
+            const int d = degree(base + pad, 2);
             if (d < bd) {
                 bd = d;
-                best = N + pad;
+                best = base + pad;
             }
         }
         return best;
@@ -511,8 +531,9 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
               long long o_stride, int nrows, int np) {
     constexpr int N = R1 * R2;
     // exchange row: position x' at x' + x' / R1 (one pad per R1 points), rows PP apart
-    constexpr int PP = XinvPitch<R1, R2, LR, sizeof(cx<T>)>::PP;
-    constexpr int NP = XinvPitch<R1, R2, LR, sizeof(cx<T>)>::NP;
+    using Pitch = XinvPitch<R1, R2, LR, sizeof(cx<T>)>;
+    constexpr int PP = Pitch::PP;
+    constexpr int NP = Pitch::NP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* ex = tw + N;          // [LR][PP]
@@ -552,14 +573,14 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             for (int r = 1; r < R2; ++r) u[r] = cmulc(u[r], tw[r * jb]);
             dft<R2, +1>(u);
 #pragma unroll
-            for (int r = 0; r < R2; ++r) rows[lb * NP + jb + r * R1] = u[r];
+            for (int r = 0; r < R2; ++r) rows[lb * NP + Pitch::pos(jb + r * R1)] = u[r];
         }
         __syncthreads();
         cx<T>* op = out + (long long)p * o_stride;
         for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
             const int c = cell[i];
             const int row = c / N, x = c - row * N;
-            op[i] = rows[(row - r0) * NP + x];
+            op[i] = rows[(row - r0) * NP + Pitch::pos(x)];
         }
 #pragma unroll
         for (int j = 0; j < R1; ++j) v[j] = vn[j];

@@ -134,7 +134,7 @@ int cl_compute_rounds(cl_ctx* ctx, int64_t n_int, const int16_t* spec, int round
 int cl_last_timings(cl_ctx* ctx, double t[4]);
 
 /* Choices of the autotuner (process-wide): one text line per tuned pass, grid shape and
- * precision -- the radix split and lines per block kept, with the per-launch time of the
+ * precision -- the radix split, lines per block and tile layout kept, with the per-launch time of the
  * tuning sample next to the default variant's.  Writes at most len bytes (NUL-terminated) to
  * buf when buf is non-null; *needed (if non-null) receives the full size.  No reference
  * counterpart: the reference plans its FFTs with FFTW_MEASURE / FFTW_ESTIMATE

@@ -17,7 +17,7 @@ TOL = {cl.MODE_FP64_PLAIN: 1e-10, cl.MODE_FP32_FOURIER: 1e-6}
 SHAPES = [(96, 128, 40), (160, 72, 48), (48, 80, 96)]
 
 
-@pytest.mark.parametrize("force", ["0,1", "1,0", "1,1"])
+@pytest.mark.parametrize("force", ["0,1", "1,0", "1,1", "0,0,1", "1,1,1"])
 @pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("dims", SHAPES)
 def test_every_variant_matches_oracle(dims, mode, force, monkeypatch):
@@ -39,7 +39,7 @@ def test_every_variant_matches_oracle(dims, mode, force, monkeypatch):
     assert abs(got - want) <= TOL[mode] * 10 * np.sqrt(np.sum(np.abs(V) ** 2) * np.sum(np.abs(F2) ** 2))
 
 
-@pytest.mark.parametrize("force", ["0,0", "1,1"])
+@pytest.mark.parametrize("force", ["0,0", "1,1", "0,1,1"])
 @pytest.mark.parametrize("mode", MODES)
 def test_variants_on_atoms_with_skipped_rows(mode, force, monkeypatch):
     """The integral path (atom scatter/gather, rows without atoms skipped) under a forced
