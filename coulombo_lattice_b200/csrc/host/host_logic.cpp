@@ -2,11 +2,13 @@
 #include "host_logic.hpp"
 
 #include <algorithm>
-#include <cstdint>
+#include <atomic>
 #include <cctype>
 #include <cmath>
+#include <cstdint>
 #include <limits>
 #include <map>
+#include <thread>
 
 #include "status.hpp"
 
@@ -192,7 +194,77 @@ void product_states(int p, int* fl, int* fr) {
 // of smallest (degree, index): if it is a leaf its neighbour joins the cover, otherwise the
 // vertex of largest (degree, index) does.
 // ---------------------------------------------------------------------------------------
+namespace {
+
+// Greedy vertex cover on a dense bitmap adjacency (vertex counts up to 16,384): the same rule
+// and the same order of choices as the set-based form below -- self-loops force their vertex
+// in; then, repeatedly, the queued vertex of least (degree, index) gives way to its single
+// neighbour if it is a leaf, else the vertex of greatest (degree, index) is taken -- with
+// degrees kept as counters and neighbourhoods as bit rows.
+std::set<int> vertex_cover_dense(int vertex_count, const std::vector<std::pair<int, int>>& edge_list) {
+    const size_t vc = (size_t)vertex_count;
+    const size_t words = (vc + 63) / 64;
+    std::vector<uint8_t> in_cover(vc, 0);
+    for (const auto& e : edge_list) {
+        if (e.first < 0 || e.second < 0 || e.first >= vertex_count || e.second >= vertex_count)
+            fail(CL_ERR_ARGUMENT, "edge vertex out of range");
+        if (e.first == e.second) in_cover[(size_t)e.first] = 1;
+    }
+    std::vector<uint64_t> adj(vc * words, 0);
+    for (const auto& e : edge_list) {
+        const size_t a = (size_t)e.first, b = (size_t)e.second;
+        if (a == b || in_cover[a] || in_cover[b]) continue;
+        adj[a * words + (b >> 6)] |= uint64_t{1} << (b & 63);
+        adj[b * words + (a >> 6)] |= uint64_t{1} << (a & 63);
+    }
+    std::vector<int> degree(vc, 0);
+    for (size_t v = 0; v < vc; ++v)
+        for (size_t w = 0; w < words; ++w) degree[v] += __builtin_popcountll(adj[v * words + w]);
+    std::set<std::pair<int, int>> queue;
+    std::vector<uint8_t> queued(vc, 0);
+    for (size_t v = 0; v < vc; ++v)
+        if (degree[v] > 0) {
+            queue.insert({degree[v], (int)v});
+            queued[v] = 1;
+        }
+    std::set<int> cover;
+    for (size_t v = 0; v < vc; ++v)
+        if (in_cover[v]) cover.insert((int)v);
+    while (!queue.empty()) {
+        int v = queue.begin()->second;
+        if (degree[v] == 1) {
+            const uint64_t* row = &adj[(size_t)v * words];
+            for (size_t w = 0; w < words; ++w)
+                if (row[w]) {
+                    v = (int)(w * 64 + (size_t)__builtin_ctzll(row[w]));
+                    break;
+                }
+        } else {
+            v = queue.rbegin()->second;
+        }
+        queue.erase({degree[v], v});
+        queued[(size_t)v] = 0;
+        cover.insert(v);
+        const uint64_t* row = &adj[(size_t)v * words];
+        for (size_t w = 0; w < words; ++w)
+            for (uint64_t m = row[w]; m; m &= m - 1) {
+                const size_t u = w * 64 + (size_t)__builtin_ctzll(m);
+                if (!queued[u]) continue;
+                queue.erase({degree[u], (int)u});
+                adj[u * words + ((size_t)v >> 6)] &= ~(uint64_t{1} << (v & 63));
+                if (--degree[u] > 0)
+                    queue.insert({degree[u], (int)u});
+                else
+                    queued[u] = 0;
+            }
+    }
+    return cover;
+}
+
+}  // namespace
+
 std::set<int> vertex_cover(int vertex_count, const std::vector<std::pair<int, int>>& edge_list) {
+    if (vertex_count > 0 && vertex_count <= 16384) return vertex_cover_dense(vertex_count, edge_list);
     // the distinct edges, in the set order of the reference (sorted pairs): through a bitmap
     // over the vertex pairs when it is small (one pass, no sort), else by sorting
     std::vector<std::pair<int, int>> edges;
@@ -251,46 +323,65 @@ std::set<int> vertex_cover(int vertex_count, const std::vector<std::pair<int, in
 // ---------------------------------------------------------------------------------------
 // src/Planner.hpp:71-104
 // ---------------------------------------------------------------------------------------
-std::vector<PlanStep> orient_steps(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs) {
+namespace {
+
+// Runs f(begin, end) over [0, n) on up to hardware_concurrency threads (one when n is small).
+template <typename F>
+void parallel_ranges(size_t n, F&& f) {
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 32), n / 65536 + 1);
+    if (nt <= 1) {
+        f(size_t{0}, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t) pool.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt); });
+    for (auto& th : pool) th.join();
+}
+
+// The steps of the integral list (id, left and right products) and their graph edges.
+void build_steps(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs, std::vector<PlanStep>& steps,
+                 std::vector<std::pair<int, int>>& edges) {
     if (specs.size() > static_cast<size_t>(std::numeric_limits<int>::max()))
         fail(CL_ERR_ARGUMENT, "too many integrals to compute");
+    steps.resize(specs.size());
+    edges.resize(specs.size());
+    std::atomic<bool> bad{false};
+    parallel_ranges(specs.size(), [&](size_t i0, size_t i1) {
+        for (size_t id = i0; id < i1; ++id) {
+            const auto& s = specs[id];
+            for (int k = 0; k < 4; ++k)
+                if (s[k] < 1 || s[k] > n_inputs) bad = true;
+            const PlanStep st{static_cast<int>(id), product_of(s[0], s[3]), product_of(s[1], s[2])};
+            steps[id] = st;
+            edges[id] = {st.left.product, st.right.product};
+        }
+    });
+    if (bad) fail(CL_ERR_ARGUMENT, "integral index out of range");
+}
+
+}  // namespace
+
+std::vector<PlanStep> orient_steps(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs) {
     const int product_count = n_inputs * (n_inputs + 1) / 2;
     std::vector<PlanStep> steps;
-    steps.reserve(specs.size());
     std::vector<std::pair<int, int>> edges;
-    edges.reserve(specs.size());
-    for (size_t id = 0; id < specs.size(); ++id) {
-        const auto& s = specs[id];
-        for (int k = 0; k < 4; ++k)
-            if (s[k] < 1 || s[k] > n_inputs) fail(CL_ERR_ARGUMENT, "integral index out of range");
-        PlanStep st{static_cast<int>(id), product_of(s[0], s[3]), product_of(s[1], s[2])};
-        steps.push_back(st);
-        edges.push_back({st.left.product, st.right.product});
-    }
+    build_steps(n_inputs, specs, steps, edges);
     const auto cover = vertex_cover(product_count, edges);
     std::vector<char> in_cover(product_count, 0);
     for (int v : cover) in_cover[v] = 1;
-    for (auto& st : steps)
-        if (!in_cover[st.left.product]) std::swap(st.left, st.right);
+    parallel_ranges(steps.size(), [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i)
+            if (!in_cover[steps[i].left.product]) std::swap(steps[i].left, steps[i].right);
+    });
     return steps;
 }
 
 std::vector<PlanStep> compute_plan(int n_inputs, const std::vector<std::array<int16_t, 4>>& specs) {
-    if (specs.size() > static_cast<size_t>(std::numeric_limits<int>::max()))
-        fail(CL_ERR_ARGUMENT, "too many integrals to compute");
     const int product_count = n_inputs * (n_inputs + 1) / 2;
     std::vector<PlanStep> steps;
-    steps.reserve(specs.size());
     std::vector<std::pair<int, int>> edges;
-    edges.reserve(specs.size());
-    for (size_t id = 0; id < specs.size(); ++id) {
-        const auto& s = specs[id];
-        for (int k = 0; k < 4; ++k)
-            if (s[k] < 1 || s[k] > n_inputs) fail(CL_ERR_ARGUMENT, "integral index out of range");
-        PlanStep st{static_cast<int>(id), product_of(s[0], s[3]), product_of(s[1], s[2])};
-        steps.push_back(st);
-        edges.push_back({st.left.product, st.right.product});
-    }
+    build_steps(n_inputs, specs, steps, edges);
     auto cover = vertex_cover(product_count, edges);
     for (auto& st : steps)
         if (!cover.count(st.left.product)) std::swap(st.left, st.right);
