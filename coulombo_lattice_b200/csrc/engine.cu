@@ -11,6 +11,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda.h>
@@ -270,6 +271,7 @@ struct cl_ctx {
     // grid API ("every cell is an atom")
     DevBuf<int> grid_cell, grid_row_ptr;
     DevBuf<cx<double>> grid_rho, grid_V, grid_rho2;
+    DevBuf<cx<float>> grid_rho32;  // the grid density in the FP32 form
     bool grid_prepared = false;
 
     // states
@@ -579,7 +581,7 @@ long long row_ptr_count(cl_ctx* c, const int* row_ptr) {
 // each round's inverse x pass writes its values at the atoms (type T) to a slot of the rounds
 // buffer; k_round_sum then forms V in FP64.  buf holds `chunk` grids of type T.
 template <typename T>
-void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, const int* row_ptr,
+void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const int* row_ptr,
                 const int* cell, cx<double>* V, long long v_stride, int round_mask) {
     const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
     const int nrows = ny * nz;
@@ -681,7 +683,7 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     const double row_side = (row_ptr == c->row_ptr.p) ? (double)c->live_rows / nrows : 1.0;
     for (int p0 = 0; p0 < np; p0 += chunk) {
         const int cnt = std::min(chunk, np - p0);
-        const cx<double>* rho_c = rho + (long long)p0 * rho_stride;
+        const cx<T>* rho_c = rho + (long long)p0 * rho_stride;
         cx<double>* V_c = V + (long long)p0 * v_stride;
         int slot = 0;
         for (int r = 0; r < 8; ++r) {
@@ -752,12 +754,21 @@ void run_rounds(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, 
     }
 }
 
-void run_rounds_mode(cl_ctx* c, const cx<double>* rho, long long rho_stride, int np, const int* row_ptr,
-                     const int* cell, cx<double>* V, long long v_stride, int round_mask = 0xFF) {
+// Pair densities are complex128 in the plain form and complex64 in the FP32 form (rounded
+// once from their FP64 sums); buffers are addressed in elements of the form's type.
+size_t rho_bytes(const cl_ctx* c) { return c->mode == CL_MODE_FP64_PLAIN ? sizeof(cx<double>) : sizeof(cx<float>); }
+void* rho_at(const cl_ctx* c, void* base, long long elems) {
+    return static_cast<unsigned char*>(base) + elems * (long long)rho_bytes(c);
+}
+
+void run_rounds_mode(cl_ctx* c, const void* rho, long long rho_stride, int np, const int* row_ptr, const int* cell,
+                     cx<double>* V, long long v_stride, int round_mask = 0xFF) {
     if (c->mode == CL_MODE_FP64_PLAIN)
-        run_rounds<double>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride, round_mask);
+        run_rounds<double>(c, static_cast<const cx<double>*>(rho), rho_stride, np, row_ptr, cell, V, v_stride,
+                           round_mask);
     else
-        run_rounds<float>(c, rho, rho_stride, np, row_ptr, cell, V, v_stride, round_mask);
+        run_rounds<float>(c, static_cast<const cx<float>*>(rho), rho_stride, np, row_ptr, cell, V, v_stride,
+                          round_mask);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -832,8 +843,8 @@ void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms) {
 }
 
 // out4[l][r] += {sum ac, bd, ad, bc} (out4 zeroed by the caller, error slot included).
-void gram_tc(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<double>* rho, long long r_stride,
-             const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
+void gram_tc(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const void* rho, bool rho_f32,
+             long long r_stride, const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
     using namespace clk::tc;
     const TcShape sh = tc_shape(c, nl, nr, n_atoms);
     if (sh.k_pad < BK) cl::fail(CL_ERR_STATE, "tensor-core Gram operands not reserved");
@@ -853,14 +864,19 @@ void gram_tc(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const c
         const int kt_total = (int)(kp / BK);
         cudaEvent_t e0 = prof_begin(c);
         const int xblocks = (int)std::min<long long>((kp + 255) / 256, 64);
-        clk::tc::k_tf32_split<<<dim3(xblocks, sh.rowsA / 2), 256, 0, c->stream>>>(V, v_stride, nullptr, nl, sh.rowsA,
-                                                                                 a0, na, sh.k_pad, A);
+        clk::tc::k_tf32_split<double><<<dim3(xblocks, sh.rowsA / 2), 256, 0, c->stream>>>(
+            V, v_stride, nullptr, nl, sh.rowsA, a0, na, sh.k_pad, A);
         CL_LAUNCHED();
-        clk::tc::k_tf32_split<<<dim3(xblocks, sh.rowsB / 2), 256, 0, c->stream>>>(rho, r_stride, ridx_dev, nr,
-                                                                                 sh.rowsB, a0, na, sh.k_pad, B);
+        if (rho_f32)
+            clk::tc::k_tf32_split<float><<<dim3(xblocks, sh.rowsB / 2), 256, 0, c->stream>>>(
+                static_cast<const cx<float>*>(rho), r_stride, ridx_dev, nr, sh.rowsB, a0, na, sh.k_pad, B);
+        else
+            clk::tc::k_tf32_split<double><<<dim3(xblocks, sh.rowsB / 2), 256, 0, c->stream>>>(
+                static_cast<const cx<double>*>(rho), r_stride, ridx_dev, nr, sh.rowsB, a0, na, sh.k_pad, B);
         CL_LAUNCHED();
         prof_end(c, e0, CL_KCLASS_GRAM_SPLIT,
-                 (double)(nl + nr) * na * 16.0 + (double)tc_bytes_per_atom(sh.rowsA, sh.rowsB) * kp);
+                 (double)na * (nl * 16.0 + nr * (rho_f32 ? 8.0 : 16.0)) +
+                     (double)tc_bytes_per_atom(sh.rowsA, sh.rowsB) * kp);
         // atom splits: whole waves of 148 blocks, each split at least 2 chunks long
         int best_s = 1;
         double best = -1e30;
@@ -895,11 +911,13 @@ void check_gram_slot(double slot) {
 // doubles, the last one an error slot.  The FP32 form runs the tensor-core Gram; the plain
 // form runs k_gram in FP64, whose register block IB (tile 16*IB) is the one that pads
 // max(nl, nr) least, preferring larger blocks.
-void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<double>* rho, long long r_stride,
-          const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
+// rho: the right densities, complex64 when rho_f32 (the FP32 form's pair densities), else
+// complex128 (the plain form's, and the grid API's caller-given density).
+void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const void* rho_any, bool rho_f32,
+          long long r_stride, const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
     CL_CUDA(cudaMemsetAsync(out4_dev, 0, sizeof(double) * (4 * (size_t)nl * nr + 1), c->stream));
     if (use_tc_gram(c)) {
-        gram_tc(c, V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, out4_dev);
+        gram_tc(c, V, v_stride, nl, rho_any, rho_f32, r_stride, ridx_dev, nr, n_atoms, out4_dev);
         return;
     }
     const int pmax = std::max(nl, nr);
@@ -921,14 +939,23 @@ void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const cx<d
     }
     cudaEvent_t e = prof_begin(c);
     const dim3 grid(tl, tr, (unsigned)splits);
-    switch (ib) {
-        case 1: clk::k_gram<1><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
-        case 2: clk::k_gram<2><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
-        case 3: clk::k_gram<3><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
-        default: clk::k_gram<4><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
-    }
+    // FP32 densities (the FP32 form with CL_NO_TC_GRAM) are widened as they are loaded
+    const auto launch = [&](auto tag) {
+        using RT = decltype(tag);
+        const cx<RT>* rho = static_cast<const cx<RT>*>(rho_any);
+        switch (ib) {
+            case 1: clk::k_gram<1, RT><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+            case 2: clk::k_gram<2, RT><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+            case 3: clk::k_gram<3, RT><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+            default: clk::k_gram<4, RT><<<grid, 256, 0, c->stream>>>(V, v_stride, nl, rho, r_stride, ridx_dev, nr, n_atoms, per, out4_dev); break;
+        }
+    };
+    if (rho_f32)
+        launch(float{});
+    else
+        launch(double{});
     CL_LAUNCHED();
-    prof_end(c, e, CL_KCLASS_GRAM, (double)(nl + nr) * n_atoms * 16.0);
+    prof_end(c, e, CL_KCLASS_GRAM, (double)n_atoms * (nl * 16.0 + nr * (rho_f32 ? 8.0 : 16.0)));
 }
 
 // Pair densities rho[p][atom] for products (fl[p], fr[p]) (0-based state indices): the
@@ -953,30 +980,39 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
     ps.prods.upload(local.data(), local.size(), c->stream);
     ps.states.upload(used.data(), used.size(), c->stream);
     ps.n_used = (int)used.size();
+    // two stages of `chunk` atoms, each up to 48 KB (about two blocks per SM)
     const int os = c->n_orb | 1;
     const size_t per_atom = sizeof(cx<double>) * (size_t)used.size() * os;
-    ps.chunk = (int)std::max<size_t>(1, std::min<size_t>(64, (40 * 1024) / per_atom));
-    ps.smem = per_atom * ps.chunk;
-    ensure_smem(clk::k_pair_density, ps.smem);
+    ps.chunk = (int)std::max<size_t>(1, std::min<size_t>(64, (48 * 1024) / per_atom));
+    ps.smem = 2 * per_atom * ps.chunk;
+    ensure_smem(clk::k_pair_density<double>, ps.smem);
+    ensure_smem(clk::k_pair_density<float>, ps.smem);
     const long long chunks = (c->n_sorted + ps.chunk - 1) / ps.chunk;
     ps.blocks = (int)std::min<long long>(chunks, 148LL * 8);
     CL_CUDA(cudaStreamSynchronize(c->stream));
 }
 
-void pair_launch(cl_ctx* c, const PairSetup& ps, cx<double>* rho) {
-    // the attribute is per kernel, so another setup (of another group or request) may have
-    // lowered it since this one was prepared
-    ensure_smem(clk::k_pair_density, ps.smem);
+void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
+    // the shared-memory attribute is per kernel, so another setup (of another group or
+    // request) may have lowered it since this one was prepared
     cudaEvent_t e = prof_begin(c);
-    clk::k_pair_density<<<ps.blocks, 256, ps.smem, c->stream>>>(c->coeff.p, c->n_atoms, c->n_orb,
-                                                               c->orig_sorted.p, c->n_sorted, ps.prods.p, ps.np,
-                                                               ps.states.p, ps.n_used, ps.chunk, rho);
+    if (c->mode == CL_MODE_FP64_PLAIN) {
+        ensure_smem(clk::k_pair_density<double>, ps.smem);
+        clk::k_pair_density<double><<<ps.blocks, 256, ps.smem, c->stream>>>(
+            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.prods.p, ps.np, ps.states.p,
+            ps.n_used, ps.chunk, static_cast<cx<double>*>(rho));
+    } else {
+        ensure_smem(clk::k_pair_density<float>, ps.smem);
+        clk::k_pair_density<float><<<ps.blocks, 256, ps.smem, c->stream>>>(
+            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.prods.p, ps.np, ps.states.p,
+            ps.n_used, ps.chunk, static_cast<cx<float>*>(rho));
+    }
     CL_LAUNCHED();
     prof_end(c, e, CL_KCLASS_DENSITY,
-             (double)ps.n_used * c->n_atoms * c->n_orb * 16.0 + (double)ps.np * c->n_sorted * 16.0);
+             (double)ps.n_used * c->n_atoms * c->n_orb * 16.0 + (double)ps.np * c->n_sorted * rho_bytes(c));
 }
 
-void pair_densities(cl_ctx* c, const std::vector<int2>& fl, cx<double>* rho) {
+void pair_densities(cl_ctx* c, const std::vector<int2>& fl, void* rho) {
     PairSetup ps;
     pair_setup(c, fl, ps);
     pair_launch(c, ps, rho);
@@ -1116,7 +1152,14 @@ int cl_prepare_grid(cl_ctx* c, const double* rho) {
         identity_atoms(c);
         c->grid_rho.upload(reinterpret_cast<const cx<double>*>(rho), c->M, c->stream);
         c->grid_V.alloc(c->M);
-        run_rounds_mode(c, c->grid_rho.p, c->M, 1, c->grid_row_ptr.p, c->grid_cell.p, c->grid_V.p, c->M);
+        const void* rho_in = c->grid_rho.p;
+        if (c->mode != CL_MODE_FP64_PLAIN) {  // the FP32 form's densities are complex64
+            c->grid_rho32.alloc(c->M);
+            clk::k_narrow<float><<<grid_for(c->M), 256, 0, c->stream>>>(c->grid_rho.p, c->grid_rho32.p, c->M);
+            CL_LAUNCHED();
+            rho_in = c->grid_rho32.p;
+        }
+        run_rounds_mode(c, rho_in, c->M, 1, c->grid_row_ptr.p, c->grid_cell.p, c->grid_V.p, c->M);
         CL_CUDA(cudaStreamSynchronize(c->stream));
         c->grid_prepared = true;
     });
@@ -1134,7 +1177,7 @@ int cl_calculate_grid(cl_ctx* c, const double* rho2, double out[2]) {
         int zero = 0;
         ridx.upload(&zero, 1, c->stream);
         tc_reserve(c, 1, 1, c->M);
-        gram(c, c->grid_V.p, c->M, 1, c->grid_rho2.p, c->M, ridx.p, 1, c->M, o4.p);
+        gram(c, c->grid_V.p, c->M, 1, c->grid_rho2.p, false, c->M, ridx.p, 1, c->M, o4.p);
         double h[5];
         CL_CUDA(cudaMemcpyAsync(h, o4.p, sizeof h, cudaMemcpyDeviceToHost, c->stream));
         CL_CUDA(cudaStreamSynchronize(c->stream));
@@ -1233,6 +1276,37 @@ int cl_set_states(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_o
 }  // extern "C"
 
 namespace {
+
+// Step values (coulombo.cpp:199-207): step s takes the Gram entry of its (left, right) pair,
+// combined for the pair's conjugation flags and conjugated when the left product is.  Long
+// integral lists are mapped on several host threads.
+void map_step_values(const std::vector<cl::PlanStep>& plan, const std::vector<int>& slot,
+                     const std::vector<int>& rcol, int nr, const double* h, double* out) {
+    const auto work = [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i) {
+            const auto& st = plan[i];
+            const int l = slot[st.left.product], r = rcol[st.right.product];
+            const double* q = &h[((size_t)l * nr + r) * 4];
+            const bool rconj = st.left.conjugate != st.right.conjugate;
+            const double re = rconj ? q[0] + q[1] : q[0] - q[1];
+            double im = rconj ? q[3] - q[2] : q[2] + q[3];
+            if (st.left.conjugate) im = -im;
+            out[2 * st.id] = re;
+            out[2 * st.id + 1] = im;
+        }
+    };
+    const size_t n = plan.size();
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 32), n / 65536 + 1);
+    if (nt <= 1) {
+        work(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t) pool.emplace_back([&, t] { work(n * t / nt, n * (t + 1) / nt); });
+    for (auto& th : pool) th.join();
+}
+
 void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, int round_mask) {
     {
         check_ctx(c);
@@ -1284,7 +1358,7 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
         run_rounds_mode(c, rho.p, As, nl, c->row_ptr.p, c->cell_sorted.p, V.p, As, round_mask);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
-        gram(c, V.p, As, nl, rho.p, As, dr.p, nr, As, o4.p);
+        gram(c, V.p, As, nl, rho.p, rho_bytes(c) == sizeof(cx<float>), As, dr.p, nr, As, o4.p);
         CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
         std::vector<double> h((size_t)4 * nl * nr + 1);
         CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1300,23 +1374,7 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         c->timings[2] = t23;
         c->timings[3] = t03;
         prof_collect(c);
-        // step values (coulombo.cpp:199-207)
-        for (const auto& s : plan) {
-            const int l = slot[s.left.product], r = rcol[s.right.product];
-            const double* q = &h[((size_t)l * nr + r) * 4];
-            const bool rconj = s.left.conjugate != s.right.conjugate;
-            double re, im;
-            if (rconj) {
-                re = q[0] + q[1];
-                im = q[3] - q[2];
-            } else {
-                re = q[0] - q[1];
-                im = q[2] + q[3];
-            }
-            if (s.left.conjugate) im = -im;
-            out[2 * s.id] = re;
-            out[2 * s.id + 1] = im;
-        }
+        map_step_values(plan, slot, rcol, nr, h.data(), out);
     }
 }
 
@@ -1446,15 +1504,16 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     for (auto& g : groups) {
         upload_through(g->last_state);
         CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[g->last_state], 0));
-        pair_launch(c, g->ps, rho.p + (long long)g->begin * As);
-        run_rounds_mode(c, rho.p + (long long)g->begin * As, As, g->end - g->begin, c->row_ptr.p, c->cell_sorted.p,
+        pair_launch(c, g->ps, rho_at(c, rho.p, (long long)g->begin * As));
+        run_rounds_mode(c, rho_at(c, rho.p, (long long)g->begin * As), As, g->end - g->begin, c->row_ptr.p,
+                        c->cell_sorted.p,
                         V.p + (long long)g->begin * As, As);
     }
     upload_through(n_states - 1);
     CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[n_states - 1], 0));
-    if (nu > nl) pair_launch(c, ps_right, rho.p + (long long)nl * As);
+    if (nu > nl) pair_launch(c, ps_right, rho_at(c, rho.p, (long long)nl * As));
     CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
-    gram(c, V.p, As, nl, rho.p, As, dr.p, nr, As, o4.p);
+    gram(c, V.p, As, nl, rho.p, rho_bytes(c) == sizeof(cx<float>), As, dr.p, nr, As, o4.p);
     CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
     std::vector<double> h((size_t)4 * nl * nr + 1);
     CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1469,16 +1528,7 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     c->timings[2] = t23;
     c->timings[3] = t03;
     prof_collect(c);
-    for (const auto& st : plan) {
-        const int l = slot[st.left.product], r = rcol[st.right.product];
-        const double* q = &h[((size_t)l * nr + r) * 4];
-        const bool rconj = st.left.conjugate != st.right.conjugate;
-        double re = rconj ? q[0] + q[1] : q[0] - q[1];
-        double im = rconj ? q[3] - q[2] : q[2] + q[3];
-        if (st.left.conjugate) im = -im;
-        out[2 * st.id] = re;
-        out[2 * st.id + 1] = im;
-    }
+    map_step_values(plan, slot, rcol, nr, h.data(), out);
 }
 }  // namespace
 
@@ -1617,23 +1667,14 @@ void request_enqueue(cl_request* r) {
     const long long As = c->n_sorted;
     pair_launch(c, r->ps, r->rho.p);
     run_rounds_mode(c, r->rho.p, As, r->nl, c->row_ptr.p, c->cell_sorted.p, r->V.p, As);
-    gram(c, r->V.p, As, r->nl, r->rho.p, As, r->ridx.p, r->nr, As, r->o4.p);
+    gram(c, r->V.p, As, r->nl, r->rho.p, rho_bytes(c) == sizeof(cx<float>), As, r->ridx.p, r->nr, As, r->o4.p);
     CL_CUDA(cudaMemcpyAsync(r->o4_host, r->o4.p, sizeof(double) * (4 * (size_t)r->nl * r->nr + 1),
                             cudaMemcpyDeviceToHost, c->stream));
 }
 
 void request_finish(cl_request* r, double* out) {
     check_gram_slot(r->o4_host[4 * (size_t)r->nl * r->nr]);
-    for (const auto& st : r->plan) {
-        const int l = r->slot[st.left.product], rr = r->rcol[st.right.product];
-        const double* q = &r->o4_host[((size_t)l * r->nr + rr) * 4];
-        const bool rconj = st.left.conjugate != st.right.conjugate;
-        double re = rconj ? q[0] + q[1] : q[0] - q[1];
-        double im = rconj ? q[3] - q[2] : q[2] + q[3];
-        if (st.left.conjugate) im = -im;
-        out[2 * st.id] = re;
-        out[2 * st.id + 1] = im;
-    }
+    map_step_values(r->plan, r->slot, r->rcol, r->nr, r->o4_host, out);
 }
 
 }  // namespace

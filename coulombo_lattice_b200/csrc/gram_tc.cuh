@@ -151,11 +151,12 @@ __device__ __forceinline__ float tf32_rn(float x) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Split pass: density d of `src` (row idx[d], or d) over atoms [a0, a0 + na) ->
+// Split pass: density d of `src` (row idx[d], or d; complex of S) over atoms [a0, a0 + na) ->
 //   dst[part][2d + {0: re, 1: im}][k], part 0 = hi, 1 = lo; rows >= 2n and k >= na are zero.
 // grid.y = rows_pad / 2 densities, grid.x strides over k.
 // ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_tf32_split(const cx<double>* __restrict__ src, long long stride,
+template <typename S>
+__global__ void __launch_bounds__(256) k_tf32_split(const cx<S>* __restrict__ src, long long stride,
                                                     const int* __restrict__ idx, int n, int rows_pad,
                                                     long long a0, long long na, long long k_pad,
                                                     float* __restrict__ dst) {
@@ -163,14 +164,14 @@ __global__ void __launch_bounds__(256) k_tf32_split(const cx<double>* __restrict
     const long long plane = (long long)rows_pad * k_pad;
     float* hre = dst + (long long)(2 * d) * k_pad;
     float* him = hre + k_pad;
-    const cx<double>* s = nullptr;
+    const cx<S>* s = nullptr;
     if (d < n) s = src + (long long)(idx ? idx[d] : d) * stride + a0;
     for (long long k = blockIdx.x * 256LL + threadIdx.x; k < k_pad; k += (long long)gridDim.x * 256) {
         double re = 0.0, im = 0.0;
         if (s && k < na) {
-            const cx<double> z = s[k];
-            re = z.re;
-            im = z.im;
+            const cx<S> z = s[k];
+            re = (double)z.re;
+            im = (double)z.im;
         }
         const float hr = tf32_rn((float)re), hi_ = tf32_rn((float)im);
         hre[k] = hr;

@@ -150,27 +150,56 @@ __global__ void k_khat(const double* __restrict__ ghat, int nx, int ny, int nz, 
 // Pair densities at atoms: rho_p(a) = sum_o conj(c_fl[a][o]) c_fr[a][o]  (Product.cpp:16-30).
 // coeff is [state][atom][orb] in input atom order; orig maps sorted -> input atom.
 // ---------------------------------------------------------------------------------------
-static __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms,
-                                                           int n_orb, const int* __restrict__ orig, long long n_sorted,
-                                                           const int2* __restrict__ prods, int n_prods,
-                                                           const int* __restrict__ states, int n_used, int chunk,
-                                                           cx<double>* __restrict__ rho) {
-    // A block stages the coefficients of `chunk` consecutive (cell-sorted) atoms for every
-    // used state in shared memory -- each coefficient is read from HBM once -- then forms every
-    // product of the chunk.  Atom pitch `os` is odd (in 16-byte units), so threads on
-    // consecutive atoms hit distinct banks.
+__device__ __forceinline__ void pd_cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                     static_cast<unsigned>(__cvta_generic_to_shared(smem_dst))),
+                 "l"(gmem_src));
+}
+
+// rho is written in the working precision RT of the form (rounded once from the FP64 sum).
+template <typename RT>
+__global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms,
+                                                    int n_orb, const int* __restrict__ orig, long long n_sorted,
+                                                    const int2* __restrict__ prods, int n_prods,
+                                                    const int* __restrict__ states, int n_used, int chunk,
+                                                    cx<RT>* __restrict__ rho) {
+    // A block stages the coefficients of `chunk` consecutive (cell-sorted) atoms for every used
+    // state in shared memory -- each coefficient is read from HBM once, a warp copying one
+    // (state, atom) row of orbitals with 16-byte cp.async -- and forms every product of the
+    // chunk while the next chunk is being copied (two stages).  Atom pitch `os` is odd (in
+    // 16-byte units), so threads on consecutive atoms hit distinct banks.
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<double>* sc = reinterpret_cast<cx<double>*>(smem_raw);
     const int os = n_orb | 1;
-    for (long long i0 = (long long)blockIdx.x * chunk; i0 < n_sorted; i0 += (long long)gridDim.x * chunk) {
+    const int stage = n_used * chunk * os;
+    cx<double>* sc0 = reinterpret_cast<cx<double>*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const long long n_chunks = (n_sorted + chunk - 1) / chunk;
+    const auto load = [&](long long ci, cx<double>* sc) {
+        const long long i0 = ci * chunk;
         const int ca = (int)min((long long)chunk, n_sorted - i0);
-        const int per_state = ca * n_orb;
-        for (int e = threadIdx.x; e < n_used * per_state; e += blockDim.x) {
-            const int su = e / per_state, rem = e - su * per_state;
-            const int a = rem / n_orb, k = rem - a * n_orb;
-            sc[(su * chunk + a) * os + k] = coeff[((long long)states[su] * n_atoms + orig[i0 + a]) * n_orb + k];
+        for (int row = warp; row < n_used * ca; row += nwarps) {
+            const int su = row / ca, a = row - su * ca;
+            const cx<double>* src = coeff + ((long long)states[su] * n_atoms + orig[i0 + a]) * n_orb;
+            cx<double>* dst = sc + (su * chunk + a) * os;
+            for (int k = lane; k < n_orb; k += 32) pd_cp_async16(dst + k, src + k);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    long long ci = blockIdx.x;
+    int buf = 0;
+    if (ci < n_chunks) load(ci, sc0);
+    for (; ci < n_chunks; ci += gridDim.x) {
+        cx<double>* sc = sc0 + buf * stage;
+        const long long next = ci + gridDim.x;
+        if (next < n_chunks) {
+            load(next, sc0 + (buf ^ 1) * stage);
+            asm volatile("cp.async.wait_group 1;\n" ::);
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::);
         }
         __syncthreads();
+        const long long i0 = ci * chunk;
+        const int ca = (int)min((long long)chunk, n_sorted - i0);
         for (int e = threadIdx.x; e < n_prods * ca; e += blockDim.x) {
             const int p = e / ca, a = e - p * ca;
             const int2 f = prods[p];  // indices into the used-state list
@@ -181,9 +210,10 @@ static __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* _
                 const cx<double> l = L[k], r = R[k];
                 acc = acc + mk(l.re * r.re + l.im * r.im, l.re * r.im - l.im * r.re);
             }
-            rho[(long long)p * n_sorted + i0 + a] = acc;
+            rho[(long long)p * n_sorted + i0 + a] = narrow<RT>(acc);
         }
-        __syncthreads();
+        __syncthreads();  // the stage is refilled by the load issued next iteration
+        buf ^= 1;
     }
 }
 
@@ -193,7 +223,7 @@ static __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* _
 // cell-sorted atom list.  Densities are processed one after another by the same block.
 // ---------------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_xfwd(const cx<double>* __restrict__ rho, long long rho_stride,
+__global__ void __launch_bounds__(256) k_xfwd(const cx<T>* __restrict__ rho, long long rho_stride,
                                              const int* __restrict__ row_ptr, const int* __restrict__ cell,
                                              cx<T>* __restrict__ out, long long out_stride, FftPlan plan,
                                              const cx<T>* __restrict__ tw_g, RoundPhase rp, int nx, int ny,
@@ -209,12 +239,12 @@ __global__ void __launch_bounds__(256) k_xfwd(const cx<double>* __restrict__ rho
     for (int p = 0; p < np; ++p) {
         for (int e = threadIdx.x; e < nx * ld; e += blockDim.x) a[e] = czero<T>();
         __syncthreads();
-        const cx<double>* rp_ = rho + (long long)p * rho_stride;
+        const cx<T>* rp_ = rho + (long long)p * rho_stride;
         for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
             const int c = cell[i];
             const int row = c / nx, x = c - row * nx;
             const int y = row % ny, z = row / ny;
-            a[x * ld + (row - r0)] = narrow<T>(cmulc(rp_[i], round_phase(rp, x, y, z)));
+            a[x * ld + (row - r0)] = narrow<T>(cmulc(widen(rp_[i]), round_phase(rp, x, y, z)));
         }
         __syncthreads();
         const cx<T>* res = fft_lines<-1>(a, b, tw, plan, rows, ld);
@@ -380,7 +410,7 @@ __global__ void __launch_bounds__(256) k_xinv(const cx<T>* __restrict__ buf, lon
 // conflicts.
 // ---------------------------------------------------------------------------------------
 template <typename T, int VALS>
-__global__ void __launch_bounds__(512, 1) k_xyfwd(const cx<double>* __restrict__ rho, long long rho_stride,
+__global__ void __launch_bounds__(512, 1) k_xyfwd(const cx<T>* __restrict__ rho, long long rho_stride,
                                               const int* __restrict__ row_ptr, const int* __restrict__ cell,
                                               cx<T>* __restrict__ out, long long out_stride, FftPlan px,
                                               FftPlan py, const cx<T>* __restrict__ twx_g,
@@ -397,12 +427,12 @@ __global__ void __launch_bounds__(512, 1) k_xyfwd(const cx<double>* __restrict__
     __syncthreads();
     const int r0 = z * ny;
     const int a0 = row_ptr[r0], a1 = row_ptr[r0 + ny];
-    const cx<double>* rp_ = rho + (long long)p * rho_stride;
+    const cx<T>* rp_ = rho + (long long)p * rho_stride;
     for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
         const int c = cell[i];
         const int row = c / nx, x = c - row * nx;
         const int y = row - r0;
-        pl[y * ld + x] = narrow<T>(cmulc(rp_[i], round_phase(rp, x, y, z)));
+        pl[y * ld + x] = narrow<T>(cmulc(widen(rp_[i]), round_phase(rp, x, y, z)));
     }
     __syncthreads();
     plane_axis<-1, VALS>(pl, twx, nx, ny, ld, 1);
@@ -499,9 +529,9 @@ __global__ void __launch_bounds__(256) k_round_sum(const cx<T>* __restrict__ t, 
 // 64x64 (l, r) tiles, 4x4 per thread, atoms staged 16 at a time; split over atoms with one
 // FP64 atomicAdd per result per block.
 // ---------------------------------------------------------------------------------------
-template <int IB>
+template <int IB, typename RT>
 __global__ void __launch_bounds__(256) k_gram(const cx<double>* __restrict__ V, long long v_stride, int nl,
-                                             const cx<double>* __restrict__ rho, long long r_stride,
+                                             const cx<RT>* __restrict__ rho, long long r_stride,
                                              const int* __restrict__ ridx, int nr, long long n_atoms,
                                              long long atoms_per_split, double* __restrict__ out) {
     // (16*IB) x (16*IB) tile of (left, right) pairs, IB x IB per thread; IB is chosen on the host
@@ -527,7 +557,7 @@ __global__ void __launch_bounds__(256) k_gram(const cx<double>* __restrict__ V, 
             const bool ok = atom < k_end;
             const int l = l0 + row, r = r0 + row;
             vs[k][row] = (ok && l < nl) ? V[(long long)l * v_stride + atom] : mk(0.0, 0.0);
-            rs[k][row] = (ok && r < nr) ? rho[(long long)ridx[r] * r_stride + atom] : mk(0.0, 0.0);
+            rs[k][row] = (ok && r < nr) ? widen(rho[(long long)ridx[r] * r_stride + atom]) : mk(0.0, 0.0);
         }
         __syncthreads();
 #pragma unroll 4

@@ -47,9 +47,10 @@ template <int S, typename T>
 bool ycol(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, int nx, int ny, int nz, int cnt,
           const int* row_ptr);
 
-// forward x pass: scatter of the atoms x conj(phase), FFT along x, rows stored.
+// forward x pass: scatter of the atoms x conj(phase), FFT along x, rows stored; the pair
+// densities rho are in the pass precision.
 template <typename T>
-bool xfwd(cudaStream_t s, Variant v, const cx<double>* rho, long long rho_stride, const int* row_ptr,
+bool xfwd(cudaStream_t s, Variant v, const cx<T>* rho, long long rho_stride, const int* row_ptr,
           const int* cell, cx<T>* buf, long long M, const cx<T>* tw, const clk::RoundPhase& rp, int nx, int ny,
           int nrows, int cnt, int skip_empty);
 

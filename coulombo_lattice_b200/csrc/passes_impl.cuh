@@ -81,7 +81,7 @@ bool ycol(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, i
 }
 
 template <typename T>
-bool xfwd(cudaStream_t s, Variant v, const cx<double>* rho, long long rho_stride, const int* row_ptr,
+bool xfwd(cudaStream_t s, Variant v, const cx<T>* rho, long long rho_stride, const int* row_ptr,
           const int* cell, cx<T>* buf, long long M, const cx<T>* tw, const clk::RoundPhase& rp, int nx, int ny,
           int nrows, int cnt, int skip_empty) {
     return clk::with_split2(

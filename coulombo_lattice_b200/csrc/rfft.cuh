@@ -343,7 +343,7 @@ struct XfwdTile {
 
 template <typename T, int R1, int R2, int LR, bool PAD>
 __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R2, LR * cmax<R1, R2>::value>::value)
-    k_xfwd_rf(const cx<double>* __restrict__ rho, long long rho_stride, const int* __restrict__ row_ptr,
+    k_xfwd_rf(const cx<T>* __restrict__ rho, long long rho_stride, const int* __restrict__ row_ptr,
               const int* __restrict__ cell, cx<T>* __restrict__ out, long long out_stride,
               const cx<T>* __restrict__ tw_g, RoundPhase rp, int ny, int nrows, int np, int skip_empty) {
     constexpr int N = R1 * R2;
@@ -390,26 +390,26 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
     __syncthreads();
     // the next density's atom values are loaded into registers while the current one is
     // transformed
-    cx<double> rv[KA], rn[KA];
-    const auto load = [&](int p, cx<double>(&v)[KA]) {
-        const cx<double>* src = rho + (long long)p * rho_stride + a0 + threadIdx.x;
+    cx<T> rv[KA], rn[KA];
+    const auto load = [&](int p, cx<T>(&v)[KA]) {
+        const cx<T>* src = rho + (long long)p * rho_stride + a0 + threadIdx.x;
 #pragma unroll
-        for (int k = 0; k < KA; ++k) v[k] = slot[k] >= 0 ? src[k * blockDim.x] : mk(0.0, 0.0);
+        for (int k = 0; k < KA; ++k) v[k] = slot[k] >= 0 ? src[k * blockDim.x] : mk(T(0), T(0));
     };
     if (pre && p_begin < p_end) load(p_begin, rv);
     for (int p = p_begin; p < p_end; ++p) {
-        const cx<double>* rp_ = rho + (long long)p * rho_stride;
+        const cx<T>* rp_ = rho + (long long)p * rho_stride;
         if (pre) {
             if (p + 1 < p_end) load(p + 1, rn);
 #pragma unroll
             for (int k = 0; k < KA; ++k)
-                if (slot[k] >= 0) tile[slot[k]] = narrow<T>(cmulc(rv[k], ph[k]));
+                if (slot[k] >= 0) tile[slot[k]] = narrow<T>(cmulc(widen(rv[k]), ph[k]));
         } else {
             for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
                 const int c = cell[i];
                 const int row = c / N, x = c - row * N;
                 const int y = row % ny, z = row / ny;
-                tile[Tile::pos(x) * LP + (row - r0)] = narrow<T>(cmulc(rp_[i], round_phase(rp, x, y, z)));
+                tile[Tile::pos(x) * LP + (row - r0)] = narrow<T>(cmulc(widen(rp_[i]), round_phase(rp, x, y, z)));
             }
         }
         __syncthreads();
