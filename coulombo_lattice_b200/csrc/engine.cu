@@ -571,6 +571,61 @@ void tune_pass(cl_ctx* c, int pass, bool fp32, int len, F&& launch) {
     tune_save(key, best);
 }
 
+// Fused plane passes against the separate passes they replace: times launch() like
+// tune_pass and records split = 1 (use the fused kernel) when it beats sep_ms, the sum of the
+// tuned separate passes' times on the same sample.
+template <typename F>
+void tune_plane(cl_ctx* c, int pass, bool fp32, double sep_ms, F&& launch) {
+    const TuneKey key{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]};
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        tune_load_locked();
+        if (g_tune.count(key)) return;
+    }
+    cudaEvent_t a, b;
+    CL_CUDA(cudaEventCreate(&a));
+    CL_CUDA(cudaEventCreate(&b));
+    launch();
+    CL_LAUNCHED();
+    CL_CUDA(cudaEventRecord(a, c->stream));
+    for (int k = 0; k < 3; ++k) launch();
+    CL_LAUNCHED();
+    CL_CUDA(cudaEventRecord(b, c->stream));
+    CL_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    CL_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    TuneEntry e;
+    e.candidates = 2;
+    e.ms = ms / 3.0;
+    e.ms_default = sep_ms;
+    e.v.split = (sep_ms <= 0 || e.ms < sep_ms) ? 1 : 0;
+    if (!e.v.split) e.ms = sep_ms;
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune[key] = e;
+    tune_save(key, e);
+}
+
+double tuned_ms(const cl_ctx* c, int pass, bool fp32) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(TuneKey{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]});
+    return it == g_tune.end() ? 0.0 : it->second.ms;
+}
+
+// Whether the fused plane pass replaces the separate ones: CL_XY_PLANE=0/1 decides outright;
+// with forced variants (CL_TUNE_FORCE) the separate passes run; otherwise the tuned choice,
+// and the fused pass when nothing was tuned.
+bool use_plane(const cl_ctx* c, int pass, bool fp32, bool supported) {
+    if (!supported) return false;
+    if (const char* e = std::getenv("CL_XY_PLANE")) return e[0] != '0';
+    if (std::getenv("CL_TUNE_FORCE")) return false;
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    tune_load_locked();
+    auto it = g_tune.find(TuneKey{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]});
+    return it == g_tune.end() ? true : it->second.v.split != 0;
+}
+
 // Number of atoms listed by a row CSR (host-side copy kept with the CSR).
 long long row_ptr_count(cl_ctx* c, const int* row_ptr) {
     return row_ptr == c->row_ptr.p ? c->n_sorted : c->M;
@@ -640,6 +695,7 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
     const bool reg_z = register_passes_enabled() && clp::split_variants(nz) > 0;
     const int skip_empty = (!pt.fits && reg_x && reg_y && !std::getenv("CL_NO_ROW_SKIP")) ? 1 : 0;
     const bool fp32 = sizeof(T) == 4;
+    const bool plane_ok = !pt.fits && reg_x && reg_y && clp::plane_supported(fp32, nx, ny);
 
     // Autotuning at the first eager request of this shape: the variants run on the first
     // densities of the request (about 512 MB of grids) in the work and rounds buffers, which
@@ -670,7 +726,17 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
             tune_pass(c, clp::kXInv, fp32, nx, [&](clp::Variant v) {
                 clp::xinv<T>(c->stream, v, buf, c->M, twx, row_ptr, cell, tr, n_at, nx, nrows, cnt_t);
             });
+        if (plane_ok && !std::getenv("CL_XY_PLANE")) {
+            tune_plane(c, clp::kXYFwd, fp32, tuned_ms(c, clp::kXFwd, fp32) + tuned_ms(c, clp::kYFwd, fp32), [&] {
+                clp::xyfwd<T>(c->stream, rho, rho_stride, row_ptr, cell, buf, c->M, twx, rp0, nx, ny, nz, cnt_t);
+            });
+            tune_plane(c, clp::kXYInv, fp32, tuned_ms(c, clp::kYInv, fp32) + tuned_ms(c, clp::kXInv, fp32), [&] {
+                clp::xyinv<T>(c->stream, buf, c->M, twx, row_ptr, cell, tr, n_at, nx, ny, nz, cnt_t);
+            });
+        }
     }
+    const bool xy_fwd = use_plane(c, clp::kXYFwd, fp32, plane_ok);
+    const bool xy_inv = use_plane(c, clp::kXYInv, fp32, plane_ok);
     const clp::Variant v_xf = tuned_variant(c, clp::kXFwd, fp32), v_yf = tuned_variant(c, clp::kYFwd, fp32),
                        v_z = tuned_variant(c, clp::kZConv, fp32), v_yi = tuned_variant(c, clp::kYInv, fp32),
                        v_xi = tuned_variant(c, clp::kXInv, fp32);
@@ -693,7 +759,9 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
                                (r >> 2) & 1};
             const T* kh = sizeof(T) == 4 ? (const T*)c->khat32[r].p : (const T*)c->khat64[r].p;
             cudaEvent_t e = prof_begin(c);
-            if (pt.fits) {
+            if (xy_fwd) {
+                clp::xyfwd<T>(c->stream, rho_c, rho_stride, row_ptr, cell, buf, c->M, twx, rp, nx, ny, nz, cnt);
+            } else if (pt.fits) {
                 clk::k_xyfwd<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
                     rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan, Y.plan, twx, twy, rp, nx, ny, pt.ld);
             } else if (!(reg_x && clp::xfwd<T>(c->stream, v_xf, rho_c, rho_stride, row_ptr, cell, buf, c->M, twx,
@@ -703,8 +771,9 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
                                                                      cnt);
             }
             CL_LAUNCHED();
-            prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * 16.0 + live * gbytes) + atoms * 4.0);
-            if (!pt.fits) {
+            prof_end(c, e, CL_KCLASS_XFWD,
+                     cnt * (atoms * (double)sizeof(cx<T>) + (xy_fwd ? 1.0 : live) * gbytes) + atoms * 4.0);
+            if (!pt.fits && !xy_fwd) {
                 e = prof_begin(c);
                 if (!(reg_y &&
                       clp::ycol<-1, T>(c->stream, v_yf, buf, c->M, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr)))
@@ -719,7 +788,7 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
                     buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W, cnt, 0);
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
-            if (!pt.fits) {
+            if (!pt.fits && !xy_inv) {
                 e = prof_begin(c);
                 if (!(reg_y &&
                       clp::ycol<+1, T>(c->stream, v_yi, buf, c->M, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr)))
@@ -729,7 +798,9 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
                 prof_end(c, e, CL_KCLASS_YPASS, cnt * (1.0 + live) * gbytes);
             }
             e = prof_begin(c);
-            if (pt.fits) {
+            if (xy_inv) {
+                clp::xyinv<T>(c->stream, buf, c->M, twx, row_ptr, cell, tr_r, n_at, nx, ny, nz, cnt);
+            } else if (pt.fits) {
                 clk::k_xyinv<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
                     buf, c->M, X.plan, Y.plan, twx, twy, row_ptr, cell, tr_r, n_at, nx, ny, pt.ld);
             } else if (!(reg_x && clp::xinv<T>(c->stream, v_xi, buf, c->M, twx, row_ptr, cell, tr_r, n_at, nx, nrows,
@@ -739,7 +810,7 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
             }
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_XINV,
-                     cnt * (row_side * gbytes + atoms * (double)sizeof(cx<T>)) + atoms * 4.0);
+                     cnt * ((xy_inv ? 1.0 : row_side) * gbytes + atoms * (double)sizeof(cx<T>)) + atoms * 4.0);
         }
         if (n_rounds > 0) {
             const clk::RoundPhase base{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
@@ -1857,13 +1928,27 @@ int cl_batch_last_ms(cl_batch* b, double* ms) {
 
 int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
     return cl::guarded([&] {
-        static const char* names[clp::kNumPasses] = {"x_forward", "y_forward", "z_pass", "y_inverse", "x_inverse"};
+        static const char* names[clp::kNumPasses] = {"x_forward", "y_forward", "z_pass",   "y_inverse",
+                                                     "x_inverse", "xy_forward", "xy_inverse"};
         std::string out;
         {
             std::lock_guard<std::mutex> g(g_tune_mu);
             for (const auto& kv : g_tune) {
                 char line[256];
                 const char* pn = names[kv.first.pass];
+                if (kv.first.pass == clp::kXYFwd || kv.first.pass == clp::kXYInv) {
+                    const char* ch = kv.second.v.split ? "fused plane pass" : "separate passes";
+                    if (kv.second.candidates == 0)
+                        std::snprintf(line, sizeof line, "%s %s %dx%dx%d: %s, from CL_TUNE_FILE\n", pn,
+                                      kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny, kv.first.nz, ch);
+                    else
+                        std::snprintf(line, sizeof line,
+                                      "%s %s %dx%dx%d: %s, 2 candidates, %.4f ms (separate passes %.4f ms)\n", pn,
+                                      kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny, kv.first.nz, ch,
+                                      kv.second.ms, kv.second.ms_default);
+                    out += line;
+                    continue;
+                }
                 const char* pr = kv.first.fp32 ? "fp32" : "fp64";
                 const char* sp = kv.second.v.split ? "swapped" : "balanced";
                 const char* ln = kv.second.v.half ? "half" : "default";

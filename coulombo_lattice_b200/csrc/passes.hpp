@@ -27,7 +27,9 @@ struct Variant {
     bool operator==(const Variant& o) const { return split == o.split && half == o.half && pad == o.pad; }
 };
 
-enum Pass { kXFwd = 0, kYFwd = 1, kZConv = 2, kYInv = 3, kXInv = 4, kNumPasses = 5 };
+// kXYFwd / kXYInv: the fused plane passes in place of x+y forward / y+x inverse (tuned
+// choice: Variant::split = 1 uses them).
+enum Pass { kXFwd = 0, kYFwd = 1, kZConv = 2, kYInv = 3, kXInv = 4, kXYFwd = 5, kXYInv = 6, kNumPasses = 7 };
 
 // Number of distinct split variants compiled for a line length: 0 (no register pass), 1
 // (square split) or 2.
@@ -58,5 +60,17 @@ bool xfwd(cudaStream_t s, Variant v, const cx<T>* rho, long long rho_stride, con
 template <typename T>
 bool xinv(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, const int* row_ptr,
           const int* cell, cx<T>* out, long long o_stride, int nx, int nrows, int cnt);
+
+// Fused xy passes on whole planes (plane_rf.cuh), for the square plane shapes compiled there
+// (false otherwise, nothing launched).  Forward: the atoms' pair densities x conj(phase) are
+// transformed along x and y and every plane is stored; inverse: planes are transformed back
+// along y and x and the round's values at the atoms are written to out.
+bool plane_supported(bool fp32, int nx, int ny);
+template <typename T>
+bool xyfwd(cudaStream_t s, const cx<T>* rho, long long rho_stride, const int* row_ptr, const int* cell, cx<T>* buf,
+           long long M, const cx<T>* tw, const clk::RoundPhase& rp, int nx, int ny, int nz, int cnt);
+template <typename T>
+bool xyinv(cudaStream_t s, cx<T>* buf, long long M, const cx<T>* tw, const int* row_ptr, const int* cell,
+           cx<T>* out, long long o_stride, int nx, int ny, int nz, int cnt);
 
 }  // namespace clp

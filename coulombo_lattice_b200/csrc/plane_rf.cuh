@@ -1,0 +1,428 @@
+// Fused x+y passes on whole xy-planes held in shared memory, with the register two-factor
+// line FFTs of rfft.cuh.
+//
+// A block owns one z-plane (N x N points, N = R1*R2) and a run of densities.  Every stage of
+// both line transforms runs in place in the plane buffer:
+//   phase A  item t < R2 of a line reads points t + R2*m (m < R1), does an R1-point DFT and
+//            writes output j back to point t + R2*j;
+//   phase B  item j < R1 reads points R2*j + t (t < R2), multiplies by W_N^(t j), does an
+//            R2-point DFT and writes output s back to point R2*j + s, which then holds
+//            frequency j + R1*s ("digit order", dig(k) below).
+// Each thread rewrites only the points it read, so a stage needs one barrier, before the
+// next stage reads.  The inverse stages run the same patterns in the opposite order
+// (B, then A), which takes a line from digit order back to natural order.
+//
+// Forward (per density): scatter the plane's atoms x conj(phase_kappa) into the zeroed plane,
+// x transform of the rows with atoms only (natural order in, digit order out), y transform of
+// every column (natural order in), and the phase-B outputs go straight to HBM in natural order
+// (consecutive threads on consecutive x); the points a thread read in the last stage are
+// zeroed as it goes, so the plane is clear for the next density.  One HBM write per point.
+// Inverse: the y transform loads its columns straight from HBM (natural order in, digit-order
+// rows out; only rows with atoms are kept), the x transform of those rows (digit order in,
+// natural order out), and the round's values at the plane's atoms are gathered to
+// out[p][atom] with consecutive threads on consecutive atoms.  One HBM read per point.
+//
+// Shared-memory layout: point n of a row at pos(n) = n + P*(n / R2) (P pad elements after
+// every R2 points), physical row pr at pr*LDP + cls(pr)*D with cls(pr) = (pr >> 1) & 1.  The
+// x-stage phase A serves 16 lanes per row and phase B 8 lanes per row, two rows of distinct
+// classes in one 16-lane group (the pair list of plane_rows); with P and D below, the row
+// accesses of both phases and the column accesses of the y stage (lanes on consecutive
+// frequencies kx, points pos(dig(kx))) are free of bank conflicts -- checked at compile time
+// by PlaneLayout::kConflictFree.
+#pragma once
+
+#include <type_traits>
+
+#include "rfft.cuh"
+
+namespace clk {
+
+template <typename T, int R1, int R2>
+struct PlaneLayout {
+    static constexpr int N = R1 * R2;
+    static constexpr int W = 128 / (int)sizeof(cx<T>);  // elements served by one wavefront
+    static constexpr int P = sizeof(T) == 4 ? 2 : 1;
+    static constexpr int D = sizeof(T) == 4 ? 1 : 0;
+    __host__ __device__ static constexpr int pos(int n) { return n + P * (n / R2); }
+    __host__ __device__ static constexpr int dig(int k) { return R2 * (k % R1) + k / R1; }
+    __host__ __device__ static constexpr int cls(int pr) { return (pr >> 1) & 1; }
+    // row pitch a multiple of W, so that a row's slot offset is cls(pr) * D whatever pr
+    static constexpr int LDP = (pos(N - 1) + 1 + D + W - 1) / W * W;
+    __host__ __device__ static constexpr int rowbase(int pr) { return pr * LDP + cls(pr) * D; }
+
+    // Bank model: a wavefront serves W consecutive lanes; the degree is the largest number of
+    // lanes of one group that hit the same W-element slot.
+    static constexpr int deg_a() {  // x phase A: lanes t of one row, points t + R2*m
+        int worst = 0;
+        for (int m = 0; m < R1; ++m)
+            for (int g0 = 0; g0 < 16; g0 += W) {
+                int cnt[16] = {};
+                for (int l = g0; l < g0 + W; ++l)
+                    if (l < R2) {
+                        const int s = pos(l + R2 * m) % W;
+                        if (++cnt[s] > worst) worst = cnt[s];
+                    }
+            }
+        return worst;
+    }
+    static constexpr int deg_b() {  // x phase B: 8 lanes j of a class-0 row, 8 of a class-1 row
+        int worst = 0;
+        for (int t = 0; t < R2; ++t)
+            for (int g0 = 0; g0 < 16; g0 += W) {
+                int cnt[16] = {};
+                for (int l = g0; l < g0 + W; ++l) {
+                    const int j = l & 7, off = (l >> 3) ? D : 0;
+                    if (j >= R1) continue;
+                    const int s = (off + pos(R2 * j + t)) % W;
+                    if (++cnt[s] > worst) worst = cnt[s];
+                }
+            }
+        return worst;
+    }
+    static constexpr int deg_c() {  // y stage: lanes on consecutive kx of one row
+        int worst = 0;
+        for (int g0 = 0; g0 < N; g0 += W) {
+            int cnt[16] = {};
+            for (int k = g0; k < g0 + W && k < N; ++k) {
+                const int s = pos(dig(k)) % W;
+                if (++cnt[s] > worst) worst = cnt[s];
+            }
+        }
+        return worst;
+    }
+    static constexpr bool kConflictFree = deg_a() == 1 && deg_b() == 1 && deg_c() == 1;
+};
+
+// Shared memory of the plane kernels: the plane, the twiddles W_N^e, the atom phases (forward)
+// and the row tables.
+template <typename T, int R1, int R2, int THREADS, bool FWD>
+struct PlaneSmem {
+    using L = PlaneLayout<T, R1, R2>;
+    static constexpr int KA = 4;  // atoms a thread keeps in registers (slots) across densities
+    static constexpr size_t elems = (size_t)L::N * L::LDP + L::N + (FWD ? (size_t)KA * THREADS : 0);
+    static constexpr size_t bytes = sizeof(cx<T>) * elems + sizeof(short) * (3 * (size_t)L::N + 2);
+};
+
+// Row tables of the block's plane (rp = the plane's slice of the row CSR): the physical rows
+// (pr = y, or dig(y) for digit-order rows) of the rows with atoms, paired class 0 with class 1
+// and flattened (prl[2q], prl[2q+1]; -1 where a pair has one row), and the live-row bit mask
+// by natural y.  Returns the number of pairs.  Called by every thread of the block.
+template <typename L>
+__device__ int plane_rows(const int* __restrict__ rp, bool digit_rows, short* prl, short* lst, unsigned* live_mask,
+                          int* cnt_sh) {
+    constexpr int N = L::N;
+    constexpr int NW = (N + 31) / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    bool live = false;
+    int pr = 0, g = 0;
+    if (tid < N) {
+        live = rp[tid + 1] > rp[tid];
+        pr = digit_rows ? L::dig(tid) : tid;
+        g = L::cls(pr);
+    }
+    unsigned b0 = 0, b1 = 0;
+    if (warp < NW) {
+        b0 = __ballot_sync(0xffffffffu, live && g == 0);
+        b1 = __ballot_sync(0xffffffffu, live && g == 1);
+        if (lane == 0) {
+            cnt_sh[warp] = __popc(b0);
+            cnt_sh[NW + warp] = __popc(b1);
+            live_mask[warp] = b0 | b1;
+        }
+    }
+    __syncthreads();
+    if (tid < N && live) {
+        int before = __popc((g ? b1 : b0) & ((1u << lane) - 1u));
+        for (int w = 0; w < warp; ++w) before += cnt_sh[g * NW + w];
+        lst[g * N + before] = (short)pr;
+    }
+    int n0 = 0, n1 = 0;
+    for (int w = 0; w < NW; ++w) {
+        n0 += cnt_sh[w];
+        n1 += cnt_sh[NW + w];
+    }
+    __syncthreads();
+    const int mn = min(n0, n1), nbig = max(n0, n1), big = n0 > n1 ? 0 : 1;
+    const int npairs = mn + (nbig - mn + 1) / 2;
+    for (int q = tid; q < npairs; q += blockDim.x) {
+        short a, b;
+        if (q < mn) {
+            a = lst[q];
+            b = lst[N + q];
+        } else {  // rows left over in the longer class, paired among themselves
+            const int u = mn + 2 * (q - mn);
+            a = lst[big * N + u];
+            b = (u + 1 < nbig) ? lst[big * N + u + 1] : (short)-1;
+        }
+        prl[2 * q] = a;
+        prl[2 * q + 1] = b;
+    }
+    __syncthreads();
+    return npairs;
+}
+
+template <typename T, int R1, int R2, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_xyfwd_plane(const cx<T>* __restrict__ rho, long long rho_stride, const int* __restrict__ row_ptr,
+                  const int* __restrict__ cell, cx<T>* __restrict__ out, long long out_stride,
+                  const cx<T>* __restrict__ tw_g, RoundPhase rp, int np) {
+    using L = PlaneLayout<T, R1, R2>;
+    using Sm = PlaneSmem<T, R1, R2, THREADS, true>;
+    static_assert(R1 <= 8 && R2 <= 16, "plane stages serve 16 lanes a row (phase A) and 8 (phase B)");
+    static_assert(L::kConflictFree, "plane layout has bank conflicts");
+    constexpr int N = L::N, KA = Sm::KA, NW = (N + 31) / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* plane = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* tw = plane + N * L::LDP;
+    cx<T>* phs = tw + N;  // [KA][THREADS]
+    short* prl = reinterpret_cast<short*>(phs + KA * THREADS);
+    short* lst = prl + N + 2;
+    __shared__ unsigned live_mask[NW];
+    __shared__ int cnt_sh[2 * NW];
+    const int tid = threadIdx.x, z = blockIdx.x, r0 = z * N;
+    for (int i = tid; i < N; i += THREADS) tw[i] = tw_g[i];
+    for (int e = tid; e < N * L::LDP; e += THREADS) plane[e] = mk(T(0), T(0));
+    const int npairs = plane_rows<L>(row_ptr + r0, false, prl, lst, live_mask, cnt_sh);
+    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + N];
+    const bool pre = (a1 - a0) <= KA * THREADS;
+    int slot[KA];
+#pragma unroll
+    for (int k = 0; k < KA; ++k) {
+        const int i = a0 + tid + k * THREADS;
+        slot[k] = -1;
+        if (pre && i < a1) {
+            const int c = cell[i];
+            const int row = c / N, x = c - row * N, y = row - r0;
+            slot[k] = L::rowbase(y) + L::pos(x);
+            phs[k * THREADS + tid] = narrow<T>(round_phase(rp, x, y, z));
+        }
+    }
+    const int per = (np + gridDim.y - 1) / gridDim.y;
+    const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
+    cx<T> rv[KA], rn[KA];
+    const auto load = [&](int p, cx<T>(&v)[KA]) {
+        const cx<T>* src = rho + (long long)p * rho_stride + a0 + tid;
+#pragma unroll
+        for (int k = 0; k < KA; ++k) v[k] = slot[k] >= 0 ? src[k * THREADS] : mk(T(0), T(0));
+    };
+    if (pre && p_begin < p_end) load(p_begin, rv);
+    __syncthreads();
+    for (int p = p_begin; p < p_end; ++p) {
+        if (pre) {
+#pragma unroll
+            for (int k = 0; k < KA; ++k)
+                if (slot[k] >= 0) plane[slot[k]] = cmulc(rv[k], phs[k * THREADS + tid]);
+            if (p + 1 < p_end) load(p + 1, rn);
+        } else {
+            const cx<T>* rp_ = rho + (long long)p * rho_stride;
+            for (int i = a0 + tid; i < a1; i += THREADS) {
+                const int c = cell[i];
+                const int row = c / N, x = c - row * N, y = row - r0;
+                plane[L::rowbase(y) + L::pos(x)] = narrow<T>(cmulc(widen(rp_[i]), round_phase(rp, x, y, z)));
+            }
+        }
+        __syncthreads();
+        // x, phase A: rows with atoms, 16 lanes a row
+        for (int i = tid; i < npairs * 32; i += THREADS) {
+            const int t = i & 15, pr = prl[i >> 4];
+            if (pr >= 0 && t < R2) {
+                cx<T>* row = plane + L::rowbase(pr);
+                cx<T> v[R1];
+#pragma unroll
+                for (int m = 0; m < R1; ++m) v[m] = row[L::pos(t + R2 * m)];
+                dft<R1, -1>(v);
+#pragma unroll
+                for (int m = 0; m < R1; ++m) row[L::pos(t + R2 * m)] = v[m];
+            }
+        }
+        __syncthreads();
+        // x, phase B: 8 lanes a row, two rows a 16-lane group
+        for (int i = tid; i < npairs * 16; i += THREADS) {
+            const int j = i & 7, pr = prl[i >> 3];
+            if (pr >= 0 && j < R1) {
+                cx<T>* row = plane + L::rowbase(pr);
+                cx<T> u[R2];
+#pragma unroll
+                for (int t = 0; t < R2; ++t) u[t] = row[L::pos(R2 * j + t)];
+#pragma unroll
+                for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * j]);
+                dft<R2, -1>(u);
+#pragma unroll
+                for (int s = 0; s < R2; ++s) row[L::pos(R2 * j + s)] = u[s];
+            }
+        }
+        __syncthreads();
+        // y, phase A: every column, lanes on consecutive kx
+#pragma unroll 1
+        for (int i = tid; i < N * R2; i += THREADS) {
+            const int kx = i % N, t = i / N;
+            cx<T>* col = plane + L::pos(L::dig(kx));
+            cx<T> v[R1];
+#pragma unroll
+            for (int m = 0; m < R1; ++m) v[m] = col[L::rowbase(t + R2 * m)];
+            dft<R1, -1>(v);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[m];
+        }
+        __syncthreads();
+        // y, phase B: outputs to HBM in natural order; the points read are cleared
+        cx<T>* o = out + (long long)p * out_stride + (long long)z * N * N;
+#pragma unroll 1
+        for (int i = tid; i < N * R1; i += THREADS) {
+            const int kx = i % N, j = i / N;
+            cx<T>* col = plane + L::pos(L::dig(kx));
+            cx<T> u[R2];
+#pragma unroll
+            for (int t = 0; t < R2; ++t) {
+                u[t] = col[L::rowbase(R2 * j + t)];
+                col[L::rowbase(R2 * j + t)] = mk(T(0), T(0));
+            }
+#pragma unroll
+            for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * j]);
+            dft<R2, -1>(u);
+#pragma unroll
+            for (int s = 0; s < R2; ++s) o[(long long)(j + R1 * s) * N + kx] = u[s];
+        }
+        __syncthreads();
+        if (pre) {
+#pragma unroll
+            for (int k = 0; k < KA; ++k) rv[k] = rn[k];
+        }
+    }
+}
+
+template <typename T, int R1, int R2, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_xyinv_plane(const cx<T>* __restrict__ buf, long long stride, const cx<T>* __restrict__ tw_g,
+                  const int* __restrict__ row_ptr, const int* __restrict__ cell, cx<T>* __restrict__ out,
+                  long long o_stride, int np) {
+    using L = PlaneLayout<T, R1, R2>;
+    using Sm = PlaneSmem<T, R1, R2, THREADS, false>;
+    static_assert(R1 <= 8 && R2 <= 16, "plane stages serve 16 lanes a row (phase A) and 8 (phase B)");
+    static_assert(L::kConflictFree, "plane layout has bank conflicts");
+    constexpr int N = L::N, KA = Sm::KA, NW = (N + 31) / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* plane = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* tw = plane + N * L::LDP;
+    short* prl = reinterpret_cast<short*>(tw + N);
+    short* lst = prl + N + 2;
+    __shared__ unsigned live_mask[NW];
+    __shared__ int cnt_sh[2 * NW];
+    const int tid = threadIdx.x, z = blockIdx.x, r0 = z * N;
+    for (int i = tid; i < N; i += THREADS) tw[i] = tw_g[i];
+    const int npairs = plane_rows<L>(row_ptr + r0, true, prl, lst, live_mask, cnt_sh);
+    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + N];
+    const bool pre = (a1 - a0) <= KA * THREADS;
+    int slot[KA];
+#pragma unroll
+    for (int k = 0; k < KA; ++k) {
+        const int i = a0 + tid + k * THREADS;
+        slot[k] = -1;
+        if (pre && i < a1) {
+            const int c = cell[i];
+            const int row = c / N, x = c - row * N, y = row - r0;
+            slot[k] = L::rowbase(L::dig(y)) + L::pos(x);
+        }
+    }
+    const int per = (np + gridDim.y - 1) / gridDim.y;
+    const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
+    for (int p = p_begin; p < p_end; ++p) {
+        const cx<T>* src = buf + (long long)p * stride + (long long)z * N * N;
+        // y, phase A: columns loaded from HBM (lanes on consecutive kx), natural order in
+#pragma unroll 1
+        for (int i = tid; i < N * R2; i += THREADS) {
+            const int kx = i % N, t = i / N;
+            cx<T> v[R1];
+#pragma unroll
+            for (int m = 0; m < R1; ++m) v[m] = src[(long long)(t + R2 * m) * N + kx];
+            dft<R1, +1>(v);
+            cx<T>* col = plane + L::pos(L::dig(kx));
+#pragma unroll
+            for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[m];
+        }
+        __syncthreads();
+        // y, phase B: digit-order rows out, kept only for the rows with atoms
+#pragma unroll 1
+        for (int i = tid; i < N * R1; i += THREADS) {
+            const int kx = i % N, j = i / N;
+            cx<T>* col = plane + L::pos(L::dig(kx));
+            cx<T> u[R2];
+#pragma unroll
+            for (int t = 0; t < R2; ++t) u[t] = col[L::rowbase(R2 * j + t)];
+#pragma unroll
+            for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * j]);
+            dft<R2, +1>(u);
+#pragma unroll
+            for (int s = 0; s < R2; ++s) {
+                const int y = j + R1 * s;
+                if ((live_mask[y >> 5] >> (y & 31)) & 1u) col[L::rowbase(R2 * j + s)] = u[s];
+            }
+        }
+        __syncthreads();
+        // x, phase B pattern first: digit order in
+        for (int i = tid; i < npairs * 16; i += THREADS) {
+            const int j = i & 7, pr = prl[i >> 3];
+            if (pr >= 0 && j < R1) {
+                cx<T>* row = plane + L::rowbase(pr);
+                cx<T> u[R2];
+#pragma unroll
+                for (int s = 0; s < R2; ++s) u[s] = row[L::pos(R2 * j + s)];
+                dft<R2, +1>(u);
+#pragma unroll
+                for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * j]);
+#pragma unroll
+                for (int t = 0; t < R2; ++t) row[L::pos(R2 * j + t)] = u[t];
+            }
+        }
+        __syncthreads();
+        // x, phase A pattern: natural order out
+        for (int i = tid; i < npairs * 32; i += THREADS) {
+            const int t = i & 15, pr = prl[i >> 4];
+            if (pr >= 0 && t < R2) {
+                cx<T>* row = plane + L::rowbase(pr);
+                cx<T> v[R1];
+#pragma unroll
+                for (int j = 0; j < R1; ++j) v[j] = row[L::pos(t + R2 * j)];
+                dft<R1, +1>(v);
+#pragma unroll
+                for (int m = 0; m < R1; ++m) row[L::pos(t + R2 * m)] = v[m];
+            }
+        }
+        __syncthreads();
+        cx<T>* op = out + (long long)p * o_stride;
+        if (pre) {
+#pragma unroll
+            for (int k = 0; k < KA; ++k)
+                if (slot[k] >= 0) op[a0 + tid + k * THREADS] = plane[slot[k]];
+        } else {
+            for (int i = a0 + tid; i < a1; i += THREADS) {
+                const int c = cell[i];
+                const int row = c / N, x = c - row * N, y = row - r0;
+                op[i] = plane[L::rowbase(L::dig(y)) + L::pos(x)];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Compiled plane shapes (square planes): N = R1*R2 with R1 <= 8, R2 <= 16; threads per block
+// and resident blocks per SM chosen so that the plane (and, forward, the atom phases) fits:
+// FP32 96^2 (99.6 KB forward, two blocks an SM), FP32 128^2 (165.6 KB), FP64 96^2 (186 KB).
+template <typename T, typename F>
+bool with_plane(int nx, int ny, F&& f) {
+    if (nx != ny) return false;
+    if constexpr (sizeof(T) == 4) {
+        switch (nx) {
+            case 96: f(SplitTag<8, 12>{}, std::integral_constant<int, 384>{}, std::integral_constant<int, 2>{}); return true;
+            case 128: f(SplitTag<8, 16>{}, std::integral_constant<int, 512>{}, std::integral_constant<int, 1>{}); return true;
+            default: return false;
+        }
+    } else {
+        switch (nx) {
+            case 96: f(SplitTag<8, 12>{}, std::integral_constant<int, 384>{}, std::integral_constant<int, 1>{}); return true;
+            default: return false;
+        }
+    }
+}
+
+}  // namespace clk
