@@ -93,14 +93,17 @@ struct PlaneLayout {
     static constexpr bool kConflictFree = deg_a() == 1 && deg_b() == 1 && deg_c() == 1;
 };
 
-// Shared memory of the plane kernels: the plane, the twiddles W_N^e, the atom phases (forward)
-// and the row tables.
+// Shared memory of the plane kernels: the plane, the twiddles W_N^e, the atom phases (forward),
+// the atom masks and the row and item tables.
 template <typename T, int R1, int R2, int THREADS, bool FWD>
 struct PlaneSmem {
     using L = PlaneLayout<T, R1, R2>;
-    static constexpr int KA = 4;  // atoms a thread keeps in registers (slots) across densities
+    static constexpr int KA = 4;                   // atoms a thread keeps (slots) across densities
+    static constexpr int NI = L::N * R2;           // phase-A items of the x stage
+    static constexpr int AW = (NI + 3) / 4;        // words of the byte masks amask
     static constexpr size_t elems = (size_t)L::N * L::LDP + L::N + (FWD ? (size_t)KA * THREADS : 0);
-    static constexpr size_t bytes = sizeof(cx<T>) * elems + sizeof(short) * (3 * (size_t)L::N + 2);
+    static constexpr size_t shorts = 4 * (size_t)L::N + 2 + NI;  // prl, lst, tmask, items
+    static constexpr size_t bytes = sizeof(cx<T>) * elems + 4 * (size_t)AW + 2 * shorts;
 };
 
 // Row tables of the block's plane (rp = the plane's slice of the row CSR): the physical rows
@@ -161,6 +164,91 @@ __device__ int plane_rows(const int* __restrict__ rp, bool digit_rows, short* pr
     return npairs;
 }
 
+// Atom tables of the block's plane (atoms a0..a1 of the sorted cell list, rows r0..r0+N):
+// amask byte y*R2 + t has bit m set when an atom sits at x = t + R2*m of row y; tmask[y] has
+// bit t set when that byte is nonzero; items[] lists y*16 + t for the nonzero bytes in
+// row-major order.  Returns the item count.  Called by every thread of the block.
+template <typename L, int R2, int THREADS>
+__device__ int plane_items(const int* __restrict__ cell, int a0, int a1, int r0, unsigned* amask_w,
+                           unsigned short* tmask, short* items, int* scan_sh) {
+    constexpr int N = L::N, NI = N * R2, AW = (NI + 3) / 4, K = (NI + THREADS - 1) / THREADS;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int w = tid; w < AW; w += THREADS) amask_w[w] = 0u;
+    __syncthreads();
+    for (int i = a0 + tid; i < a1; i += THREADS) {
+        const int c = cell[i];
+        const int row = c / N, x = c - row * N, y = row - r0;
+        const int e = y * R2 + x % R2;
+        atomicOr(&amask_w[e >> 2], (1u << (x / R2)) << (8 * (e & 3)));
+    }
+    __syncthreads();
+    const unsigned char* am = reinterpret_cast<const unsigned char*>(amask_w);
+    for (int y = tid; y < N; y += THREADS) {
+        unsigned tm = 0;
+        for (int t = 0; t < R2; ++t)
+            if (am[y * R2 + t]) tm |= 1u << t;
+        tmask[y] = (unsigned short)tm;
+    }
+    // compaction: thread tid owns candidates [tid*K, tid*K + K); exclusive scan of the counts
+    int cnt = 0;
+    for (int k = 0; k < K; ++k) {
+        const int e = tid * K + k;
+        if (e < NI && am[e]) ++cnt;
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) scan_sh[warp] = incl;
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < THREADS / 32; ++w) {
+        const int v = scan_sh[w];
+        if (w < warp) before += v;
+        total += v;
+    }
+    int o = before + incl - cnt;
+    for (int k = 0; k < K; ++k) {
+        const int e = tid * K + k;
+        if (e < NI && am[e]) items[o++] = (short)((e / R2) * 16 + e % R2);
+    }
+    __syncthreads();
+    return total;
+}
+
+// Bit y of the block's live-row mask, held in registers (planes of up to 128 rows).
+__device__ __forceinline__ unsigned live_bit(const unsigned (&lw)[4], int y) {
+    const unsigned w = y < 64 ? (y < 32 ? lw[0] : lw[1]) : (y < 96 ? lw[2] : lw[3]);
+    return (w >> (y & 31)) & 1u;
+}
+
+// Carves the plane kernels' shared memory.
+template <typename T, int R1, int R2, int THREADS, bool FWD>
+struct PlaneTables {
+    using Sm = PlaneSmem<T, R1, R2, THREADS, FWD>;
+    static constexpr int N = Sm::L::N;
+    cx<T>* plane;
+    cx<T>* tw;
+    cx<T>* phs;
+    unsigned* amask_w;
+    short* prl;
+    short* lst;
+    unsigned short* tmask;
+    short* items;
+    __device__ explicit PlaneTables(unsigned char* raw) {
+        plane = reinterpret_cast<cx<T>*>(raw);
+        tw = plane + N * Sm::L::LDP;
+        phs = tw + N;
+        amask_w = reinterpret_cast<unsigned*>(phs + (FWD ? Sm::KA * THREADS : 0));
+        prl = reinterpret_cast<short*>(amask_w + Sm::AW);
+        lst = prl + N + 2;
+        tmask = reinterpret_cast<unsigned short*>(lst + 2 * N);
+        items = reinterpret_cast<short*>(tmask + N);
+    }
+};
+
 template <typename T, int R1, int R2, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_xyfwd_plane(const cx<T>* __restrict__ rho, long long rho_stride, const int* __restrict__ row_ptr,
@@ -168,22 +256,25 @@ __global__ void __launch_bounds__(THREADS, MINB)
                   const cx<T>* __restrict__ tw_g, RoundPhase rp, int np) {
     using L = PlaneLayout<T, R1, R2>;
     using Sm = PlaneSmem<T, R1, R2, THREADS, true>;
-    static_assert(R1 <= 8 && R2 <= 16, "plane stages serve 16 lanes a row (phase A) and 8 (phase B)");
+    static_assert(R1 <= 8 && R2 <= 16 && L::N <= 128, "plane stages serve 16 lanes a row (phase A) and 8 (phase B)");
     static_assert(L::kConflictFree, "plane layout has bank conflicts");
     constexpr int N = L::N, KA = Sm::KA, NW = (N + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<T>* plane = reinterpret_cast<cx<T>*>(smem_raw);
-    cx<T>* tw = plane + N * L::LDP;
-    cx<T>* phs = tw + N;  // [KA][THREADS]
-    short* prl = reinterpret_cast<short*>(phs + KA * THREADS);
-    short* lst = prl + N + 2;
-    __shared__ unsigned live_mask[NW];
+    const PlaneTables<T, R1, R2, THREADS, true> tb(smem_raw);
+    cx<T>* const plane = tb.plane;
+    const cx<T>* const tw = tb.tw;
+    __shared__ unsigned live_mask[4];
     __shared__ int cnt_sh[2 * NW];
+    __shared__ int scan_sh[THREADS / 32];
     const int tid = threadIdx.x, z = blockIdx.x, r0 = z * N;
-    for (int i = tid; i < N; i += THREADS) tw[i] = tw_g[i];
-    for (int e = tid; e < N * L::LDP; e += THREADS) plane[e] = mk(T(0), T(0));
-    const int npairs = plane_rows<L>(row_ptr + r0, false, prl, lst, live_mask, cnt_sh);
+    for (int i = tid; i < N; i += THREADS) tb.tw[i] = tw_g[i];
+    if (tid < 4) live_mask[tid] = 0u;
+    __syncthreads();
+    const int npairs = plane_rows<L>(row_ptr + r0, false, tb.prl, tb.lst, live_mask, cnt_sh);
     const int a0 = row_ptr[r0], a1 = row_ptr[r0 + N];
+    const int n_items = plane_items<L, R2, THREADS>(cell, a0, a1, r0, tb.amask_w, tb.tmask, tb.items, scan_sh);
+    const unsigned char* am = reinterpret_cast<const unsigned char*>(tb.amask_w);
+    const unsigned lw[4] = {live_mask[0], live_mask[1], live_mask[2], live_mask[3]};
     const bool pre = (a1 - a0) <= KA * THREADS;
     int slot[KA];
 #pragma unroll
@@ -194,7 +285,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             const int c = cell[i];
             const int row = c / N, x = c - row * N, y = row - r0;
             slot[k] = L::rowbase(y) + L::pos(x);
-            phs[k * THREADS + tid] = narrow<T>(round_phase(rp, x, y, z));
+            tb.phs[k * THREADS + tid] = narrow<T>(round_phase(rp, x, y, z));
         }
     }
     const int per = (np + gridDim.y - 1) / gridDim.y;
@@ -207,11 +298,13 @@ __global__ void __launch_bounds__(THREADS, MINB)
     };
     if (pre && p_begin < p_end) load(p_begin, rv);
     __syncthreads();
+    // The plane is never cleared: every read below takes only points written for the current
+    // density (atom points, masked by amask / tmask / the live rows) and zero for the rest.
     for (int p = p_begin; p < p_end; ++p) {
         if (pre) {
 #pragma unroll
             for (int k = 0; k < KA; ++k)
-                if (slot[k] >= 0) plane[slot[k]] = cmulc(rv[k], phs[k * THREADS + tid]);
+                if (slot[k] >= 0) plane[slot[k]] = cmulc(rv[k], tb.phs[k * THREADS + tid]);
             if (p + 1 < p_end) load(p + 1, rn);
         } else {
             const cx<T>* rp_ = rho + (long long)p * rho_stride;
@@ -222,28 +315,29 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
         }
         __syncthreads();
-        // x, phase A: rows with atoms, 16 lanes a row
-        for (int i = tid; i < npairs * 32; i += THREADS) {
-            const int t = i & 15, pr = prl[i >> 4];
-            if (pr >= 0 && t < R2) {
-                cx<T>* row = plane + L::rowbase(pr);
-                cx<T> v[R1];
+        // x, phase A: the items (row, t) with atoms, their atom points only
+        for (int i = tid; i < n_items; i += THREADS) {
+            const int code = tb.items[i];
+            const int y = code >> 4, t = code & 15;
+            const unsigned mm = am[y * R2 + t];
+            cx<T>* row = plane + L::rowbase(y);
+            cx<T> v[R1];
 #pragma unroll
-                for (int m = 0; m < R1; ++m) v[m] = row[L::pos(t + R2 * m)];
-                dft<R1, -1>(v);
+            for (int m = 0; m < R1; ++m) v[m] = ((mm >> m) & 1u) ? row[L::pos(t + R2 * m)] : mk(T(0), T(0));
+            dft<R1, -1>(v);
 #pragma unroll
-                for (int m = 0; m < R1; ++m) row[L::pos(t + R2 * m)] = v[m];
-            }
+            for (int m = 0; m < R1; ++m) row[L::pos(t + R2 * m)] = v[m];
         }
         __syncthreads();
-        // x, phase B: 8 lanes a row, two rows a 16-lane group
+        // x, phase B: rows with atoms, 8 lanes a row, two rows a 16-lane group
         for (int i = tid; i < npairs * 16; i += THREADS) {
-            const int j = i & 7, pr = prl[i >> 3];
+            const int j = i & 7, pr = tb.prl[i >> 3];
             if (pr >= 0 && j < R1) {
+                const unsigned tm = tb.tmask[pr];
                 cx<T>* row = plane + L::rowbase(pr);
                 cx<T> u[R2];
 #pragma unroll
-                for (int t = 0; t < R2; ++t) u[t] = row[L::pos(R2 * j + t)];
+                for (int t = 0; t < R2; ++t) u[t] = ((tm >> t) & 1u) ? row[L::pos(R2 * j + t)] : mk(T(0), T(0));
 #pragma unroll
                 for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * j]);
                 dft<R2, -1>(u);
@@ -252,20 +346,21 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
         }
         __syncthreads();
-        // y, phase A: every column, lanes on consecutive kx
+        // y, phase A: every column, lanes on consecutive kx; rows without atoms read as zero
 #pragma unroll 1
         for (int i = tid; i < N * R2; i += THREADS) {
             const int kx = i % N, t = i / N;
             cx<T>* col = plane + L::pos(L::dig(kx));
             cx<T> v[R1];
 #pragma unroll
-            for (int m = 0; m < R1; ++m) v[m] = col[L::rowbase(t + R2 * m)];
+            for (int m = 0; m < R1; ++m)
+                v[m] = live_bit(lw, t + R2 * m) ? col[L::rowbase(t + R2 * m)] : mk(T(0), T(0));
             dft<R1, -1>(v);
 #pragma unroll
             for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[m];
         }
         __syncthreads();
-        // y, phase B: outputs to HBM in natural order; the points read are cleared
+        // y, phase B: outputs to HBM in natural order
         cx<T>* o = out + (long long)p * out_stride + (long long)z * N * N;
 #pragma unroll 1
         for (int i = tid; i < N * R1; i += THREADS) {
@@ -273,10 +368,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             cx<T>* col = plane + L::pos(L::dig(kx));
             cx<T> u[R2];
 #pragma unroll
-            for (int t = 0; t < R2; ++t) {
-                u[t] = col[L::rowbase(R2 * j + t)];
-                col[L::rowbase(R2 * j + t)] = mk(T(0), T(0));
-            }
+            for (int t = 0; t < R2; ++t) u[t] = col[L::rowbase(R2 * j + t)];
 #pragma unroll
             for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * j]);
             dft<R2, -1>(u);
@@ -298,20 +390,25 @@ __global__ void __launch_bounds__(THREADS, MINB)
                   long long o_stride, int np) {
     using L = PlaneLayout<T, R1, R2>;
     using Sm = PlaneSmem<T, R1, R2, THREADS, false>;
-    static_assert(R1 <= 8 && R2 <= 16, "plane stages serve 16 lanes a row (phase A) and 8 (phase B)");
+    static_assert(R1 <= 8 && R2 <= 16 && L::N <= 128, "plane stages serve 16 lanes a row (phase A) and 8 (phase B)");
     static_assert(L::kConflictFree, "plane layout has bank conflicts");
     constexpr int N = L::N, KA = Sm::KA, NW = (N + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<T>* plane = reinterpret_cast<cx<T>*>(smem_raw);
-    cx<T>* tw = plane + N * L::LDP;
-    short* prl = reinterpret_cast<short*>(tw + N);
-    short* lst = prl + N + 2;
-    __shared__ unsigned live_mask[NW];
+    const PlaneTables<T, R1, R2, THREADS, false> tb(smem_raw);
+    cx<T>* const plane = tb.plane;
+    const cx<T>* const tw = tb.tw;
+    __shared__ unsigned live_mask[4];
     __shared__ int cnt_sh[2 * NW];
+    __shared__ int scan_sh[THREADS / 32];
     const int tid = threadIdx.x, z = blockIdx.x, r0 = z * N;
-    for (int i = tid; i < N; i += THREADS) tw[i] = tw_g[i];
-    const int npairs = plane_rows<L>(row_ptr + r0, true, prl, lst, live_mask, cnt_sh);
+    for (int i = tid; i < N; i += THREADS) tb.tw[i] = tw_g[i];
+    if (tid < 4) live_mask[tid] = 0u;
+    __syncthreads();
+    const int npairs = plane_rows<L>(row_ptr + r0, true, tb.prl, tb.lst, live_mask, cnt_sh);
     const int a0 = row_ptr[r0], a1 = row_ptr[r0 + N];
+    const int n_items = plane_items<L, R2, THREADS>(cell, a0, a1, r0, tb.amask_w, tb.tmask, tb.items, scan_sh);
+    const unsigned char* am = reinterpret_cast<const unsigned char*>(tb.amask_w);
+    const unsigned lw[4] = {live_mask[0], live_mask[1], live_mask[2], live_mask[3]};
     const bool pre = (a1 - a0) <= KA * THREADS;
     int slot[KA];
 #pragma unroll
@@ -353,16 +450,15 @@ __global__ void __launch_bounds__(THREADS, MINB)
             for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * j]);
             dft<R2, +1>(u);
 #pragma unroll
-            for (int s = 0; s < R2; ++s) {
-                const int y = j + R1 * s;
-                if ((live_mask[y >> 5] >> (y & 31)) & 1u) col[L::rowbase(R2 * j + s)] = u[s];
-            }
+            for (int s = 0; s < R2; ++s)
+                if (live_bit(lw, j + R1 * s)) col[L::rowbase(R2 * j + s)] = u[s];
         }
         __syncthreads();
-        // x, phase B pattern first: digit order in
+        // x, phase B pattern first (digit order in); only the points of items with atoms kept
         for (int i = tid; i < npairs * 16; i += THREADS) {
-            const int j = i & 7, pr = prl[i >> 3];
+            const int j = i & 7, pr = tb.prl[i >> 3];
             if (pr >= 0 && j < R1) {
+                const unsigned tm = tb.tmask[(pr % R2) * R1 + pr / R2];  // natural row of pr = dig(y)
                 cx<T>* row = plane + L::rowbase(pr);
                 cx<T> u[R2];
 #pragma unroll
@@ -371,22 +467,24 @@ __global__ void __launch_bounds__(THREADS, MINB)
 #pragma unroll
                 for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * j]);
 #pragma unroll
-                for (int t = 0; t < R2; ++t) row[L::pos(R2 * j + t)] = u[t];
+                for (int t = 0; t < R2; ++t)
+                    if ((tm >> t) & 1u) row[L::pos(R2 * j + t)] = u[t];
             }
         }
         __syncthreads();
-        // x, phase A pattern: natural order out
-        for (int i = tid; i < npairs * 32; i += THREADS) {
-            const int t = i & 15, pr = prl[i >> 4];
-            if (pr >= 0 && t < R2) {
-                cx<T>* row = plane + L::rowbase(pr);
-                cx<T> v[R1];
+        // x, phase A pattern (natural order out): the items with atoms, their atom points only
+        for (int i = tid; i < n_items; i += THREADS) {
+            const int code = tb.items[i];
+            const int y = code >> 4, t = code & 15;
+            const unsigned mm = am[y * R2 + t];
+            cx<T>* row = plane + L::rowbase(L::dig(y));
+            cx<T> v[R1];
 #pragma unroll
-                for (int j = 0; j < R1; ++j) v[j] = row[L::pos(t + R2 * j)];
-                dft<R1, +1>(v);
+            for (int j = 0; j < R1; ++j) v[j] = row[L::pos(R2 * j + t)];
+            dft<R1, +1>(v);
 #pragma unroll
-                for (int m = 0; m < R1; ++m) row[L::pos(t + R2 * m)] = v[m];
-            }
+            for (int m = 0; m < R1; ++m)
+                if ((mm >> m) & 1u) row[L::pos(t + R2 * m)] = v[m];
         }
         __syncthreads();
         cx<T>* op = out + (long long)p * o_stride;
