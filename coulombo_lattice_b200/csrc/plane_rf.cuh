@@ -346,18 +346,48 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
         }
         __syncthreads();
-        // y, phase A: every column, lanes on consecutive kx; rows without atoms read as zero
+        // y, phase A: every column, lanes on consecutive kx; rows without atoms read as zero.
+        // Where the launch leaves a thread 128 registers or more (FP32), the loads of all of its
+        // items are issued before the first transform; otherwise one item at a time (measured:
+        // batching spills at 80 registers and is slower there).
+        constexpr bool kBatch = sizeof(T) == 4 && 65536 / (THREADS * MINB) >= 128;
+        if constexpr (kBatch) {
+            constexpr int IA = (N * R2 + THREADS - 1) / THREADS;
+            cx<T> v[IA][R1];
+#pragma unroll
+            for (int a = 0; a < IA; ++a) {
+                const int i = tid + a * THREADS;
+                const int kx = i % N, t = i / N;
+                const cx<T>* col = plane + L::pos(L::dig(kx));
+#pragma unroll
+                for (int m = 0; m < R1; ++m)
+                    v[a][m] = (i < N * R2 && live_bit(lw, t + R2 * m)) ? col[L::rowbase(t + R2 * m)]
+                                                                       : mk(T(0), T(0));
+            }
+#pragma unroll
+            for (int a = 0; a < IA; ++a) {
+                const int i = tid + a * THREADS;
+                if (i < N * R2) {
+                    const int kx = i % N, t = i / N;
+                    dft<R1, -1>(v[a]);
+                    cx<T>* col = plane + L::pos(L::dig(kx));
+#pragma unroll
+                    for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[a][m];
+                }
+            }
+        } else {
 #pragma unroll 1
-        for (int i = tid; i < N * R2; i += THREADS) {
-            const int kx = i % N, t = i / N;
-            cx<T>* col = plane + L::pos(L::dig(kx));
-            cx<T> v[R1];
+            for (int i = tid; i < N * R2; i += THREADS) {
+                const int kx = i % N, t = i / N;
+                cx<T>* col = plane + L::pos(L::dig(kx));
+                cx<T> v[R1];
 #pragma unroll
-            for (int m = 0; m < R1; ++m)
-                v[m] = live_bit(lw, t + R2 * m) ? col[L::rowbase(t + R2 * m)] : mk(T(0), T(0));
-            dft<R1, -1>(v);
+                for (int m = 0; m < R1; ++m)
+                    v[m] = live_bit(lw, t + R2 * m) ? col[L::rowbase(t + R2 * m)] : mk(T(0), T(0));
+                dft<R1, -1>(v);
 #pragma unroll
-            for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[m];
+                for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[m];
+            }
         }
         __syncthreads();
         // y, phase B: outputs to HBM in natural order
@@ -425,17 +455,28 @@ __global__ void __launch_bounds__(THREADS, MINB)
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
     for (int p = p_begin; p < p_end; ++p) {
         const cx<T>* src = buf + (long long)p * stride + (long long)z * N * N;
-        // y, phase A: columns loaded from HBM (lanes on consecutive kx), natural order in
-#pragma unroll 1
-        for (int i = tid; i < N * R2; i += THREADS) {
+        // y, phase A: columns loaded from HBM (lanes on consecutive kx), natural order in; the
+        // loads of all of a thread's items are issued before the first transform
+        constexpr int IA = (N * R2 + THREADS - 1) / THREADS;
+        cx<T> v[IA][R1];
+#pragma unroll
+        for (int a = 0; a < IA; ++a) {
+            const int i = tid + a * THREADS;
             const int kx = i % N, t = i / N;
-            cx<T> v[R1];
 #pragma unroll
-            for (int m = 0; m < R1; ++m) v[m] = src[(long long)(t + R2 * m) * N + kx];
-            dft<R1, +1>(v);
-            cx<T>* col = plane + L::pos(L::dig(kx));
+            for (int m = 0; m < R1; ++m)
+                v[a][m] = i < N * R2 ? src[(long long)(t + R2 * m) * N + kx] : mk(T(0), T(0));
+        }
 #pragma unroll
-            for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[m];
+        for (int a = 0; a < IA; ++a) {
+            const int i = tid + a * THREADS;
+            if (i < N * R2) {
+                const int kx = i % N, t = i / N;
+                dft<R1, +1>(v[a]);
+                cx<T>* col = plane + L::pos(L::dig(kx));
+#pragma unroll
+                for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[a][m];
+            }
         }
         __syncthreads();
         // y, phase B: digit-order rows out, kept only for the rows with atoms
