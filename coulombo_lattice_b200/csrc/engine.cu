@@ -1033,9 +1033,9 @@ void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const void
 // device lists and launch shape are set up once (setup synchronises), the launch itself only
 // enqueues (it can be captured in a CUDA graph).
 struct PairSetup {
-    DevBuf<int2> prods;  // indices into `states`
+    DevBuf<clk::PairSeg> segs;  // products grouped by left state, indices into `states`
     DevBuf<int> states;
-    int np = 0, n_used = 0, chunk = 1, blocks = 1;
+    int np = 0, n_segs = 0, n_used = 0, chunk = 1, blocks = 1;
     size_t smem = 0;
 };
 
@@ -1046,15 +1046,41 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
     for (const auto& f : fl)
         for (int s : {f.x, f.y})
             if (where[s] < 0) { where[s] = (int)used.size(); used.push_back(s); }
-    std::vector<int2> local(ps.np);
-    for (int p = 0; p < ps.np; ++p) local[p] = make_int2(where[fl[p].x], where[fl[p].y]);
-    ps.prods.upload(local.data(), local.size(), c->stream);
+    // segments: the products of each left state, kPairSeg at a time (product order kept)
+    std::vector<std::vector<int>> by_left(used.size());
+    for (int p = 0; p < ps.np; ++p) by_left[where[fl[p].x]].push_back(p);
+    std::vector<clk::PairSeg> segs;
+    for (int u = 0; u < (int)used.size(); ++u)
+        for (size_t k0 = 0; k0 < by_left[u].size(); k0 += clk::kPairSeg) {
+            clk::PairSeg sg{};
+            sg.left = u;
+            sg.cnt = (int)std::min<size_t>(clk::kPairSeg, by_left[u].size() - k0);
+            for (int j = 0; j < sg.cnt; ++j) {
+                const int p = by_left[u][k0 + j];
+                sg.right[j] = where[fl[p].y];
+                sg.prod[j] = p;
+            }
+            segs.push_back(sg);
+        }
+    ps.n_segs = (int)segs.size();
+    ps.segs.upload(segs.data(), segs.size(), c->stream);
     ps.states.upload(used.data(), used.size(), c->stream);
     ps.n_used = (int)used.size();
     // two stages of `chunk` atoms, each up to 48 KB (about two blocks per SM)
     const int os = c->n_orb | 1;
     const size_t per_atom = sizeof(cx<double>) * (size_t)used.size() * os;
-    ps.chunk = (int)std::max<size_t>(1, std::min<size_t>(64, (48 * 1024) / per_atom));
+    // the chunk (at most the 48 KB stage) whose item rounds -- segments x atoms over the 256
+    // threads of a block -- cost least per atom
+    const int max_chunk = (int)std::max<size_t>(1, std::min<size_t>(64, (48 * 1024) / per_atom));
+    ps.chunk = max_chunk;
+    double best = 1e300;
+    for (int ch = max_chunk; ch >= std::max(1, max_chunk / 2); --ch) {
+        const double rounds = (double)(((long long)ps.n_segs * ch + 255) / 256);
+        if (rounds / ch < best - 1e-12) {
+            best = rounds / ch;
+            ps.chunk = ch;
+        }
+    }
     ps.smem = 2 * per_atom * ps.chunk;
     ensure_smem(clk::k_pair_density<double>, ps.smem);
     ensure_smem(clk::k_pair_density<float>, ps.smem);
@@ -1070,12 +1096,12 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
     if (c->mode == CL_MODE_FP64_PLAIN) {
         ensure_smem(clk::k_pair_density<double>, ps.smem);
         clk::k_pair_density<double><<<ps.blocks, 256, ps.smem, c->stream>>>(
-            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.prods.p, ps.np, ps.states.p,
+            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<double>*>(rho));
     } else {
         ensure_smem(clk::k_pair_density<float>, ps.smem);
         clk::k_pair_density<float><<<ps.blocks, 256, ps.smem, c->stream>>>(
-            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.prods.p, ps.np, ps.states.p,
+            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<float>*>(rho));
     }
     CL_LAUNCHED();

@@ -156,18 +156,28 @@ __device__ __forceinline__ void pd_cp_async16(void* smem_dst, const void* gmem_s
                  "l"(gmem_src));
 }
 
+// Products of one left state, up to kPairSeg of them: rho_prod[k] = conj(c_left) c_right[k].
+constexpr int kPairSeg = 4;
+struct PairSeg {
+    int left, cnt;              // indices into the used-state list; products in this segment
+    int right[kPairSeg];        // right state of each product (used-state index)
+    int prod[kPairSeg];         // product index (row of rho)
+};
+
 // rho is written in the working precision RT of the form (rounded once from the FP64 sum).
 template <typename RT>
 __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restrict__ coeff, long long n_atoms,
                                                     int n_orb, const int* __restrict__ orig, long long n_sorted,
-                                                    const int2* __restrict__ prods, int n_prods,
+                                                    const PairSeg* __restrict__ segs, int n_segs,
                                                     const int* __restrict__ states, int n_used, int chunk,
                                                     cx<RT>* __restrict__ rho) {
     // A block stages the coefficients of `chunk` consecutive (cell-sorted) atoms for every used
     // state in shared memory -- each coefficient is read from HBM once, a warp copying one
     // (state, atom) row of orbitals with 16-byte cp.async -- and forms every product of the
-    // chunk while the next chunk is being copied (two stages).  Atom pitch `os` is odd (in
-    // 16-byte units), so threads on consecutive atoms hit distinct banks.
+    // chunk while the next chunk is being copied (two stages).  A thread takes one segment
+    // (a left state and up to kPairSeg right states) at one atom, so each orbital of the left
+    // state is read from shared memory once for all the segment's products.  Atom pitch `os`
+    // is odd (in 16-byte units), so threads on consecutive atoms hit distinct banks.
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int os = n_orb | 1;
     const int stage = n_used * chunk * os;
@@ -200,17 +210,31 @@ __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restri
         __syncthreads();
         const long long i0 = ci * chunk;
         const int ca = (int)min((long long)chunk, n_sorted - i0);
-        for (int e = threadIdx.x; e < n_prods * ca; e += blockDim.x) {
-            const int p = e / ca, a = e - p * ca;
-            const int2 f = prods[p];  // indices into the used-state list
-            const cx<double>* L = sc + (f.x * chunk + a) * os;
-            const cx<double>* R = sc + (f.y * chunk + a) * os;
-            cx<double> acc = mk(0.0, 0.0);
+        for (int e = threadIdx.x; e < n_segs * ca; e += blockDim.x) {
+            const int q = e / ca, a = e - q * ca;
+            const PairSeg& sg = segs[q];
+            const cx<double>* L = sc + (sg.left * chunk + a) * os;
+            const cx<double>* R[kPairSeg];
+#pragma unroll
+            for (int j = 0; j < kPairSeg; ++j) R[j] = sc + ((j < sg.cnt ? sg.right[j] : sg.left) * chunk + a) * os;
+            cx<double> acc[kPairSeg];
+#pragma unroll
+            for (int j = 0; j < kPairSeg; ++j) acc[j] = mk(0.0, 0.0);
+            // four orbitals in flight: the chain of shared-memory loads, not their bandwidth,
+            // bounds this loop at the occupancy the staged chunks allow
+#pragma unroll 4
             for (int k = 0; k < n_orb; ++k) {
-                const cx<double> l = L[k], r = R[k];
-                acc = acc + mk(l.re * r.re + l.im * r.im, l.re * r.im - l.im * r.re);
+                const cx<double> l = L[k];
+#pragma unroll
+                for (int j = 0; j < kPairSeg; ++j)
+                    if (j < sg.cnt) {
+                        const cx<double> r = R[j][k];
+                        acc[j] = acc[j] + mk(l.re * r.re + l.im * r.im, l.re * r.im - l.im * r.re);
+                    }
             }
-            rho[(long long)p * n_sorted + i0 + a] = narrow<RT>(acc);
+#pragma unroll
+            for (int j = 0; j < kPairSeg; ++j)
+                if (j < sg.cnt) rho[(long long)sg.prod[j] * n_sorted + i0 + a] = narrow<RT>(acc[j]);
         }
         __syncthreads();  // the stage is refilled by the load issued next iteration
         buf ^= 1;
