@@ -49,6 +49,11 @@ struct PlaneLayout {
     // row pitch a multiple of W, so that a row's slot offset is cls(pr) * D whatever pr
     static constexpr int LDP = (pos(N - 1) + 1 + D + W - 1) / W * W;
     __host__ __device__ static constexpr int rowbase(int pr) { return pr * LDP + cls(pr) * D; }
+    // With R2 a multiple of 4 (or no class shift), rows r + R2*k share the class of r, so the
+    // rows a y-stage item touches are one base plus compile-time multiples of R2*LDP:
+    // rowbase(r + R2*k) = rowbase(r) + k*RSTEP.
+    static_assert(R2 % 4 == 0 || D == 0, "rows R2 apart must share their class");
+    static constexpr int RSTEP = R2 * LDP;
 
     // Bank model: a wavefront serves W consecutive lanes; the degree is the largest number of
     // lanes of one group that hit the same W-element slot.
@@ -361,7 +366,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 const cx<T>* col = plane + L::pos(L::dig(kx));
 #pragma unroll
                 for (int m = 0; m < R1; ++m)
-                    v[a][m] = (i < N * R2 && live_bit(lw, t + R2 * m)) ? col[L::rowbase(t + R2 * m)]
+                    v[a][m] = (i < N * R2 && live_bit(lw, t + R2 * m)) ? col[L::rowbase(t) + m * L::RSTEP]
                                                                        : mk(T(0), T(0));
             }
 #pragma unroll
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                     dft<R1, -1>(v[a]);
                     cx<T>* col = plane + L::pos(L::dig(kx));
 #pragma unroll
-                    for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[a][m];
+                    for (int m = 0; m < R1; ++m) col[L::rowbase(t) + m * L::RSTEP] = v[a][m];
                 }
             }
         } else {
@@ -383,10 +388,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 cx<T> v[R1];
 #pragma unroll
                 for (int m = 0; m < R1; ++m)
-                    v[m] = live_bit(lw, t + R2 * m) ? col[L::rowbase(t + R2 * m)] : mk(T(0), T(0));
+                    v[m] = live_bit(lw, t + R2 * m) ? col[L::rowbase(t) + m * L::RSTEP] : mk(T(0), T(0));
                 dft<R1, -1>(v);
 #pragma unroll
-                for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[m];
+                for (int m = 0; m < R1; ++m) col[L::rowbase(t) + m * L::RSTEP] = v[m];
             }
         }
         __syncthreads();
@@ -398,7 +403,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             cx<T>* col = plane + L::pos(L::dig(kx));
             cx<T> u[R2];
 #pragma unroll
-            for (int t = 0; t < R2; ++t) u[t] = col[L::rowbase(R2 * j + t)];
+            for (int t = 0; t < R2; ++t) u[t] = col[j * L::RSTEP + L::rowbase(t)];
 #pragma unroll
             for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * j]);
             dft<R2, -1>(u);
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 dft<R1, +1>(v[a]);
                 cx<T>* col = plane + L::pos(L::dig(kx));
 #pragma unroll
-                for (int m = 0; m < R1; ++m) col[L::rowbase(t + R2 * m)] = v[a][m];
+                for (int m = 0; m < R1; ++m) col[L::rowbase(t) + m * L::RSTEP] = v[a][m];
             }
         }
         __syncthreads();
@@ -486,13 +491,13 @@ __global__ void __launch_bounds__(THREADS, MINB)
             cx<T>* col = plane + L::pos(L::dig(kx));
             cx<T> u[R2];
 #pragma unroll
-            for (int t = 0; t < R2; ++t) u[t] = col[L::rowbase(R2 * j + t)];
+            for (int t = 0; t < R2; ++t) u[t] = col[j * L::RSTEP + L::rowbase(t)];
 #pragma unroll
             for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * j]);
             dft<R2, +1>(u);
 #pragma unroll
             for (int s = 0; s < R2; ++s)
-                if (live_bit(lw, j + R1 * s)) col[L::rowbase(R2 * j + s)] = u[s];
+                if (live_bit(lw, j + R1 * s)) col[j * L::RSTEP + L::rowbase(s)] = u[s];
         }
         __syncthreads();
         // x, phase B pattern first (digit order in); only the points of items with atoms kept
