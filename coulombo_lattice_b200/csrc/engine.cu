@@ -600,8 +600,7 @@ void tune_plane(cl_ctx* c, int pass, bool fp32, double sep_ms, F&& launch) {
     e.candidates = 2;
     e.ms = ms / 3.0;
     e.ms_default = sep_ms;
-    e.v.split = (sep_ms <= 0 || e.ms < sep_ms) ? 1 : 0;
-    if (!e.v.split) e.ms = sep_ms;
+    e.v.split = (sep_ms <= 0 || e.ms < sep_ms) ? 1 : 0;  // ms: the fused pass; ms_default: separate
     std::lock_guard<std::mutex> g(g_tune_mu);
     g_tune[key] = e;
     tune_save(key, e);
@@ -1969,7 +1968,7 @@ int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
                                       kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny, kv.first.nz, ch);
                     else
                         std::snprintf(line, sizeof line,
-                                      "%s %s %dx%dx%d: %s, 2 candidates, %.4f ms (separate passes %.4f ms)\n", pn,
+                                      "%s %s %dx%dx%d: %s, 2 candidates, fused %.4f ms, separate %.4f ms\n", pn,
                                       kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny, kv.first.nz, ch,
                                       kv.second.ms, kv.second.ms_default);
                     out += line;
