@@ -1,14 +1,17 @@
-// Launchers of the register-FFT passes (rfft.cuh) for every compiled variant.
+// Launchers of the register-FFT passes (rfft.cuh) for every compiled variant, and of the
+// fused xy plane passes (plane_rf.cuh).
 //
 // A variant picks the radix split of the line length (the balanced split, or its two factors
 // swapped), the lines per block (the default -- 16 for FP32, 8 for FP64 -- or half) and, for
-// the forward x pass, the layout of its tile.  The
-// autotuner in engine.cu times the variants of each pass on the request's own shapes and
-// keeps the fastest.  Each launcher returns false (nothing launched) when the length has no
-// compiled two-factor split; launch errors surface through cudaGetLastError.
+// the forward x pass, the layout of its tile.  The autotuner in engine.cu times the variants
+// of each pass on the request's own shapes and keeps the fastest, then times the fused plane
+// passes (where compiled) against the separate passes they replace.  Each launcher returns
+// false (nothing launched) when the length has no compiled kernel; launch errors surface
+// through cudaGetLastError.
 //
 // The launchers are instantiated in passes_xfwd.cu, passes_xinv.cu, passes_yfwd.cu,
-// passes_yinv.cu and passes_z.cu (one translation unit per pass, compiled in parallel).
+// passes_yinv.cu, passes_z.cu and passes_xy.cu (one translation unit per pass, compiled in
+// parallel).
 #pragma once
 
 #include <cuda_runtime.h>
