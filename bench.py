@@ -45,7 +45,7 @@ DIELECTRIC = 10.89
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -111,7 +111,7 @@ class ClockSampler:
     def __init__(self, device_uuid=None):
         self.samples = []
         self.proc = None
-        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200"]
+        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "50"]
         if device_uuid:
             cmd += ["-i", device_uuid]
         try:
@@ -233,7 +233,9 @@ def run_reference(args):
         return
     d = build_workload(args.config, cells=cells_arg(args))
     threads = os.cpu_count() or 1
-    n_left = {"c1": 2, "c2": 2, "c3": 1, "c4": 1}[args.config]
+    # one step's sample shrinks with the step count, so that --steps K --warmup W ends within a
+    # few minutes (C2: about 0.9 s a step with one prepared density)
+    n_left = {"c1": 2, "c2": 2, "c3": 1, "c4": 1}[args.config] if args.steps <= 20 else 1
     for _ in range(args.warmup):
         cpu_sample(d, n_left, threads)
     vals, secs = [], []
