@@ -551,18 +551,21 @@ __global__ void __launch_bounds__(THREADS, MINB)
 
 // Compiled plane shapes (square planes): N = R1*R2 with R1 <= 8, R2 <= 16; threads per block
 // and resident blocks per SM chosen so that the plane (and, forward, the atom phases) fits:
-// FP32 96^2 (99.6 KB forward, two blocks an SM), FP32 128^2 (165.6 KB), FP64 96^2 (186 KB).
+// FP32 64^2 (52 KB forward, three blocks an SM), FP32 96^2 (101 KB, two blocks), FP32 128^2
+// (168 KB), FP64 64^2 (91 KB, two blocks), FP64 96^2 (186 KB).
 template <typename T, typename F>
 bool with_plane(int nx, int ny, F&& f) {
     if (nx != ny) return false;
     if constexpr (sizeof(T) == 4) {
         switch (nx) {
+            case 64: f(SplitTag<8, 8>{}, std::integral_constant<int, 256>{}, std::integral_constant<int, 3>{}); return true;
             case 96: f(SplitTag<8, 12>{}, std::integral_constant<int, 384>{}, std::integral_constant<int, 2>{}); return true;
             case 128: f(SplitTag<8, 16>{}, std::integral_constant<int, 512>{}, std::integral_constant<int, 1>{}); return true;
             default: return false;
         }
     } else {
         switch (nx) {
+            case 64: f(SplitTag<8, 8>{}, std::integral_constant<int, 256>{}, std::integral_constant<int, 2>{}); return true;
             case 96: f(SplitTag<8, 12>{}, std::integral_constant<int, 384>{}, std::integral_constant<int, 1>{}); return true;
             default: return false;
         }

@@ -1,5 +1,5 @@
-"""The fused xy plane passes (a whole xy-plane in shared memory per block: 96^2 in FP32 and
-FP64, 128^2 in FP32) against the oracle and against the separate x and y passes, on
+"""The fused xy plane passes (a whole xy-plane in shared memory per block: 64^2 and 96^2 in
+FP32 and FP64, 128^2 in FP32) against the oracle and against the separate x and y passes, on
 zinc-blende atoms, on scattered atoms (rows of every parity, a plane with more atoms than a
 block keeps in registers) and on the grid API (every cell an atom)."""
 import numpy as np
@@ -48,13 +48,15 @@ def _check(d, mode, monkeypatch):
     assert np.abs(got - sep).max() <= tol * np.abs(sep).max()
 
 
-@pytest.mark.parametrize("mode,cells", [(FP32, (24, 24, 3)), (FP64, (24, 24, 3)), (FP32, (32, 32, 2))],
-                         ids=["fp32-96", "fp64-96", "fp32-128"])
+@pytest.mark.parametrize("mode,cells", [(FP32, (24, 24, 3)), (FP64, (24, 24, 3)), (FP32, (32, 32, 2)),
+                                        (FP32, (16, 16, 3)), (FP64, (16, 16, 3))],
+                         ids=["fp32-96", "fp64-96", "fp32-128", "fp32-64", "fp64-64"])
 def test_plane_passes_on_zincblende_atoms(mode, cells, monkeypatch):
     _check(synth.build("c1", cells=cells), mode, monkeypatch)
 
 
-@pytest.mark.parametrize("mode,n", [(FP32, 96), (FP64, 96), (FP32, 128)], ids=["fp32-96", "fp64-96", "fp32-128"])
+@pytest.mark.parametrize("mode,n", [(FP32, 96), (FP64, 96), (FP32, 128), (FP32, 64), (FP64, 64)],
+                         ids=["fp32-96", "fp64-96", "fp32-128", "fp32-64", "fp64-64"])
 def test_plane_passes_on_scattered_atoms(mode, n, monkeypatch):
     """Atoms on random distinct cells: live rows of both classes in every plane, unpaired rows,
     and a first plane holding more atoms (2,100) than a block keeps in registers."""
@@ -68,8 +70,9 @@ def test_plane_passes_on_scattered_atoms(mode, n, monkeypatch):
     _check(d, mode, monkeypatch)
 
 
-@pytest.mark.parametrize("mode,dims", [(FP32, (96, 96, 10)), (FP64, (96, 96, 10)), (FP32, (128, 128, 6))],
-                         ids=["fp32-96", "fp64-96", "fp32-128"])
+@pytest.mark.parametrize("mode,dims", [(FP32, (96, 96, 10)), (FP64, (96, 96, 10)), (FP32, (128, 128, 6)),
+                                       (FP32, (64, 64, 12)), (FP64, (64, 64, 12))],
+                         ids=["fp32-96", "fp64-96", "fp32-128", "fp32-64", "fp64-64"])
 def test_plane_passes_on_grid_api(mode, dims, monkeypatch):
     rng = np.random.default_rng(dims[0] + dims[2])
     nx, ny, nz = dims
