@@ -215,23 +215,6 @@ LTile l_tile(int n, bool with_khat) {
     return LTile{W, bytes(W)};
 }
 
-// Whole xy-plane in shared memory ([y][ld], ld odd) plus both twiddle tables.
-struct PlaneTile {
-    bool fits;
-    int ld;
-    size_t smem;
-};
-template <typename T>
-PlaneTile plane_tile(int nx, int ny) {
-    const int ld = (nx % 2 == 0) ? nx + 1 : nx;
-    const size_t smem = sizeof(cx<T>) * ((size_t)nx + ny + (size_t)ny * ld);
-    // Off unless CL_XY_FUSION is set: measured on B200 at 96^3, the register row/column passes
-    // (two HBM sweeps more) run 1.5x faster than this whole-plane kernel.
-    const bool fits = smem <= 220 * 1024 && clk::plane_size_supported(nx) && clk::plane_size_supported(ny) &&
-                      std::getenv("CL_XY_FUSION") != nullptr;
-    return PlaneTile{fits, ld, smem};
-}
-
 unsigned zgroups(long long zblocks, int cnt) { return clp::density_groups(zblocks, cnt); }
 
 // Bytes of grids a chunk may hold so that consecutive passes meet in L2 (CL_L2_CHUNK_MB;
@@ -672,17 +655,10 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
     const XTile xt = x_tile<T>(nx, nrows);
     const LTile yt = l_tile<T>(ny, false);
     const LTile zt = l_tile<T>(nz, true);
-    const PlaneTile pt = plane_tile<T>(nx, ny);
-    constexpr int VALS = sizeof(T) == 4 ? 8 : 4;
-    if (pt.fits) {
-        ensure_smem(clk::k_xyfwd<T, VALS>, pt.smem);
-        ensure_smem(clk::k_xyinv<T, VALS>, pt.smem);
-    } else {
-        ensure_smem(clk::k_xfwd<T>, xt.smem);
-        ensure_smem(clk::k_xinv<T>, xt.smem);
-        ensure_smem(clk::k_ypass<-1, T>, yt.smem);
-        ensure_smem(clk::k_ypass<+1, T>, yt.smem);
-    }
+    ensure_smem(clk::k_xfwd<T>, xt.smem);
+    ensure_smem(clk::k_xinv<T>, xt.smem);
+    ensure_smem(clk::k_ypass<-1, T>, yt.smem);
+    ensure_smem(clk::k_ypass<+1, T>, yt.smem);
     ensure_smem(clk::k_zpass<T>, zt.smem);
     const int xblocks = (nrows + xt.rows - 1) / xt.rows;
     const int ychunks = (nx + yt.W - 1) / yt.W;
@@ -692,9 +668,9 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
     const bool reg_x = register_passes_enabled() && clp::split_variants(nx) > 0;
     const bool reg_y = register_passes_enabled() && clp::split_variants(ny) > 0;
     const bool reg_z = register_passes_enabled() && clp::split_variants(nz) > 0;
-    const int skip_empty = (!pt.fits && reg_x && reg_y && !std::getenv("CL_NO_ROW_SKIP")) ? 1 : 0;
+    const int skip_empty = (reg_x && reg_y && !std::getenv("CL_NO_ROW_SKIP")) ? 1 : 0;
     const bool fp32 = sizeof(T) == 4;
-    const bool plane_ok = !pt.fits && reg_x && reg_y && clp::plane_supported(fp32, nx, ny);
+    const bool plane_ok = reg_x && reg_y && clp::plane_supported(fp32, nx, ny);
 
     // Autotuning at the first eager request of this shape: the variants run on the first
     // densities of the request (about 512 MB of grids) in the work and rounds buffers, which
@@ -704,12 +680,12 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
         const clk::RoundPhase rp0{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
         const T* kh0 = sizeof(T) == 4 ? (const T*)c->khat32[0].p : (const T*)c->khat64[0].p;
         const int* rp_skip = skip_empty ? row_ptr : nullptr;
-        if (!pt.fits && reg_x)
+        if (reg_x)
             tune_pass(c, clp::kXFwd, fp32, nx, [&](clp::Variant v) {
                 clp::xfwd<T>(c->stream, v, rho, rho_stride, row_ptr, cell, buf, c->M, twx, rp0, nx, ny, nrows, cnt_t,
                              skip_empty);
             });
-        if (!pt.fits && reg_y) {
+        if (reg_y) {
             tune_pass(c, clp::kYFwd, fp32, ny, [&](clp::Variant v) {
                 clp::ycol<-1, T>(c->stream, v, buf, c->M, twy, nx, ny, nz, cnt_t, rp_skip);
             });
@@ -721,7 +697,7 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
             tune_pass(c, clp::kZConv, fp32, nz, [&](clp::Variant v) {
                 clp::zconv<T>(c->stream, v, buf, c->M, twz, kh0, nxy, nz, cnt_t);
             });
-        if (!pt.fits && reg_x)
+        if (reg_x)
             tune_pass(c, clp::kXInv, fp32, nx, [&](clp::Variant v) {
                 clp::xinv<T>(c->stream, v, buf, c->M, twx, row_ptr, cell, tr, n_at, nx, nrows, cnt_t);
             });
@@ -760,9 +736,6 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
             cudaEvent_t e = prof_begin(c);
             if (xy_fwd) {
                 clp::xyfwd<T>(c->stream, rho_c, rho_stride, row_ptr, cell, buf, c->M, twx, rp, nx, ny, nz, cnt);
-            } else if (pt.fits) {
-                clk::k_xyfwd<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
-                    rho_c, rho_stride, row_ptr, cell, buf, c->M, X.plan, Y.plan, twx, twy, rp, nx, ny, pt.ld);
             } else if (!(reg_x && clp::xfwd<T>(c->stream, v_xf, rho_c, rho_stride, row_ptr, cell, buf, c->M, twx,
                                                 rp, nx, ny, nrows, cnt, skip_empty))) {
                 clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, c->M,
@@ -772,7 +745,7 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_XFWD,
                      cnt * (atoms * (double)sizeof(cx<T>) + (xy_fwd ? 1.0 : live) * gbytes) + atoms * 4.0);
-            if (!pt.fits && !xy_fwd) {
+            if (!xy_fwd) {
                 e = prof_begin(c);
                 if (!(reg_y &&
                       clp::ycol<-1, T>(c->stream, v_yf, buf, c->M, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr)))
@@ -787,7 +760,7 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
                     buf, c->M, Z.plan, twz, kh, nxy, nz, zt.W, cnt, 0);
             CL_LAUNCHED();
             prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + (double)c->M * sizeof(T));
-            if (!pt.fits && !xy_inv) {
+            if (!xy_inv) {
                 e = prof_begin(c);
                 if (!(reg_y &&
                       clp::ycol<+1, T>(c->stream, v_yi, buf, c->M, twy, nx, ny, nz, cnt, skip_empty ? row_ptr : nullptr)))
@@ -799,9 +772,6 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
             e = prof_begin(c);
             if (xy_inv) {
                 clp::xyinv<T>(c->stream, buf, c->M, twx, row_ptr, cell, tr_r, n_at, nx, ny, nz, cnt);
-            } else if (pt.fits) {
-                clk::k_xyinv<T, VALS><<<dim3(nz, cnt), 512, pt.smem, c->stream>>>(
-                    buf, c->M, X.plan, Y.plan, twx, twy, row_ptr, cell, tr_r, n_at, nx, ny, pt.ld);
             } else if (!(reg_x && clp::xinv<T>(c->stream, v_xi, buf, c->M, twx, row_ptr, cell, tr_r, n_at, nx, nrows,
                                                 cnt))) {
                 clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, c->M, X.plan, twx, row_ptr, cell, tr_r,

@@ -463,154 +463,4 @@ __device__ cx<T>* fft_lines(cx<T>* a, cx<T>* b, const cx<T>* __restrict__ tw, co
     return a;
 }
 
-// ---------------------------------------------------------------------------------------
-// In-place variant: element (line, idx) at buf[line*ls + idx*is].  Within a stage every
-// thread first loads all of its butterflies' inputs into registers, the block synchronises,
-// and only then are outputs written, so a single buffer serves as both source and
-// destination.  Lines are processed in groups small enough that a group's elements fit in
-// VALS registers per thread.
-// ---------------------------------------------------------------------------------------
-template <int R, int S, int VALS, typename T>
-__device__ __forceinline__ void stage_ip(cx<T>* buf, const cx<T>* __restrict__ tw, int n, int ns, unsigned ns_m,
-                                         int l0, int lines, unsigned lines_m, int ls, int is) {
-    constexpr int B = (VALS + R - 1) / R;
-    const int nb = n / R;
-    const int total = nb * lines;
-    const int twstep = n / (ns * R);
-    cx<T> v[B][R];
-#pragma unroll
-    for (int i = 0; i < B; ++i) {
-        const int b = threadIdx.x + i * blockDim.x;
-        if (b < total) {
-            const int j = fdiv(b, lines_m);
-            const int line = b - j * lines;
-            const int k = j - fdiv(j, ns_m) * ns;
-            const cx<T>* base = buf + (l0 + line) * ls;
-#pragma unroll
-            for (int r = 0; r < R; ++r) v[i][r] = base[(j + r * nb) * is];
-            if (ns > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    cx<T> w = tw[r * k * twstep];
-                    v[i][r] = S < 0 ? cmul(v[i][r], w) : cmulc(v[i][r], w);
-                }
-            }
-            dft<R, S>(v[i]);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < B; ++i) {
-        const int b = threadIdx.x + i * blockDim.x;
-        if (b < total) {
-            const int j = fdiv(b, lines_m);
-            const int line = b - j * lines;
-            const int k = j - fdiv(j, ns_m) * ns;
-            cx<T>* base = buf + (l0 + line) * ls;
-            const int o = (j - k) * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r) base[(o + r * ns) * is] = v[i][r];
-        }
-    }
-    __syncthreads();
-}
-
-// Transforms `lines` lines in place.  Requires blockDim.x * VALS >= n (one line per group
-// at least); the caller synchronises before the call.  Ends synchronised.
-template <int S, int VALS, typename T>
-__device__ __forceinline__ void fft_lines_ip(cx<T>* buf, const cx<T>* __restrict__ tw, const FftPlan& p,
-                                             int lines, int ls, int is) {
-    const int group = max(1, min(lines, (int)(blockDim.x * VALS) / p.n));
-    for (int l0 = 0; l0 < lines; l0 += group) {
-        const int cnt = min(group, lines - l0);
-        const unsigned lm = fdiv_magic(cnt);
-        int ns = 1;
-        for (int s = 0; s < p.nst; ++s) {
-            const int R = p.radix[s];
-            const unsigned nm = p.ns_magic[s];
-            switch (R) {
-                case 2: stage_ip<2, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                case 3: stage_ip<3, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                case 4: stage_ip<4, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                case 5: stage_ip<5, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                case 6: stage_ip<6, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                case 10: stage_ip<10, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                case 12: stage_ip<12, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                case 16: stage_ip<16, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-                default: stage_ip<8, S, VALS>(buf, tw, p.n, ns, nm, l0, cnt, lm, ls, is); break;
-            }
-            ns *= R;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------------------
-// Compile-time stage chains for the in-place plane transforms: with the length N and every
-// radix known at compile time, each stage is straight-line code (divisions by constants),
-// and the kernel's register allocation is that of its largest single stage.
-// ---------------------------------------------------------------------------------------
-template <int R, int S, int VALS, int N, int NS, typename T>
-__device__ __forceinline__ void stage_ct(cx<T>* buf, const cx<T>* __restrict__ tw, int l0, int lines,
-                                         unsigned lines_m, int ls, int is) {
-    constexpr int B = (VALS + R - 1) / R;
-    constexpr int NB = N / R;
-    constexpr int TWSTEP = N / (NS * R);
-    const int total = NB * lines;
-    cx<T> v[B][R];
-#pragma unroll
-    for (int i = 0; i < B; ++i) {
-        const int b = threadIdx.x + i * blockDim.x;
-        if (b < total) {
-            const int j = fdiv(b, lines_m);
-            const int line = b - j * lines;
-            const int k = j % NS;
-            const cx<T>* base = buf + (l0 + line) * ls;
-#pragma unroll
-            for (int r = 0; r < R; ++r) v[i][r] = base[(j + r * NB) * is];
-            if (NS > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    cx<T> w = tw[r * k * TWSTEP];
-                    v[i][r] = S < 0 ? cmul(v[i][r], w) : cmulc(v[i][r], w);
-                }
-            }
-            dft<R, S>(v[i]);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < B; ++i) {
-        const int b = threadIdx.x + i * blockDim.x;
-        if (b < total) {
-            const int j = fdiv(b, lines_m);
-            const int line = b - j * lines;
-            const int k = j % NS;
-            cx<T>* base = buf + (l0 + line) * ls;
-            const int o = (j - k) * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r) base[(o + r * NS) * is] = v[i][r];
-        }
-    }
-    __syncthreads();
-}
-
-template <int S, int VALS, int N, int NS, typename T, int R, int... Rest>
-__device__ __forceinline__ void chain_ct(cx<T>* buf, const cx<T>* __restrict__ tw, int l0, int lines,
-                                         unsigned lines_m, int ls, int is) {
-    stage_ct<R, S, VALS, N, NS>(buf, tw, l0, lines, lines_m, ls, is);
-    if constexpr (sizeof...(Rest) > 0) chain_ct<S, VALS, N, NS * R, T, Rest...>(buf, tw, l0, lines, lines_m, ls, is);
-}
-
-// All `lines` lines of length N = product(Rs), in place, in groups that fit VALS registers
-// per thread.  Caller synchronises before; ends synchronised.
-template <int S, int VALS, typename T, int... Rs>
-__device__ __forceinline__ void axis_ct(cx<T>* buf, const cx<T>* __restrict__ tw, int lines, int ls, int is) {
-    constexpr int N = (Rs * ...);
-    const int group = max(1, min(lines, (int)(blockDim.x * VALS) / N));
-    for (int l0 = 0; l0 < lines; l0 += group) {
-        const int cnt = min(group, lines - l0);
-        chain_ct<S, VALS, N, 1, T, Rs...>(buf, tw, l0, cnt, fdiv_magic(cnt), ls, is);
-    }
-}
-
 }  // namespace clk

@@ -18,7 +18,6 @@
 #pragma once
 
 #include "fft.cuh"
-#include "plane_fft.cuh"
 
 namespace clk {
 
@@ -422,81 +421,6 @@ __global__ void __launch_bounds__(256) k_xinv(const cx<T>* __restrict__ buf, lon
             op[i] = res[x * ld + (row - r0)];
         }
         __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------------------
-// Fused x+y passes for planes that fit in shared memory: block = (z-plane, density).
-// Forward: scatter the plane's atoms x conj(phase), FFT along x then y in place, store the
-// plane (one HBM write).  Inverse: load the plane, inverse FFT along y then x, and write the
-// round's value at the plane's atoms (one HBM read).  The plane sits in shared
-// memory as [y][ld] with ld odd, so row and column transforms are both free of bank
-// conflicts.
-// ---------------------------------------------------------------------------------------
-template <typename T, int VALS>
-__global__ void __launch_bounds__(512, 1) k_xyfwd(const cx<T>* __restrict__ rho, long long rho_stride,
-                                              const int* __restrict__ row_ptr, const int* __restrict__ cell,
-                                              cx<T>* __restrict__ out, long long out_stride, FftPlan px,
-                                              FftPlan py, const cx<T>* __restrict__ twx_g,
-                                              const cx<T>* __restrict__ twy_g, RoundPhase rp, int nx, int ny,
-                                              int ld) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<T>* twx = reinterpret_cast<cx<T>*>(smem_raw);
-    cx<T>* twy = twx + nx;
-    cx<T>* pl = twy + ny;
-    const int z = blockIdx.x, p = blockIdx.y;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = twx_g[i];
-    for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = twy_g[i];
-    for (int e = threadIdx.x; e < ny * ld; e += blockDim.x) pl[e] = czero<T>();
-    __syncthreads();
-    const int r0 = z * ny;
-    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + ny];
-    const cx<T>* rp_ = rho + (long long)p * rho_stride;
-    for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
-        const int c = cell[i];
-        const int row = c / nx, x = c - row * nx;
-        const int y = row - r0;
-        pl[y * ld + x] = narrow<T>(cmulc(widen(rp_[i]), round_phase(rp, x, y, z)));
-    }
-    __syncthreads();
-    plane_axis<-1, VALS>(pl, twx, nx, ny, ld, 1);
-    plane_axis<-1, VALS>(pl, twy, ny, nx, 1, ld);
-    cx<T>* o = out + (long long)p * out_stride + (long long)z * nx * ny;
-    for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
-        const int y = e / nx, x = e - y * nx;
-        o[e] = pl[y * ld + x];
-    }
-}
-
-template <typename T, int VALS>
-__global__ void __launch_bounds__(512, 1) k_xyinv(const cx<T>* __restrict__ buf, long long stride, FftPlan px,
-                                              FftPlan py, const cx<T>* __restrict__ twx_g,
-                                              const cx<T>* __restrict__ twy_g, const int* __restrict__ row_ptr,
-                                              const int* __restrict__ cell, cx<T>* __restrict__ out,
-                                              long long o_stride, int nx, int ny, int ld) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<T>* twx = reinterpret_cast<cx<T>*>(smem_raw);
-    cx<T>* twy = twx + nx;
-    cx<T>* pl = twy + ny;
-    const int z = blockIdx.x, p = blockIdx.y;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = twx_g[i];
-    for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = twy_g[i];
-    const cx<T>* src = buf + (long long)p * stride + (long long)z * nx * ny;
-    for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
-        const int y = e / nx, x = e - y * nx;
-        pl[y * ld + x] = src[e];
-    }
-    __syncthreads();
-    plane_axis<+1, VALS>(pl, twy, ny, nx, 1, ld);
-    plane_axis<+1, VALS>(pl, twx, nx, ny, ld, 1);
-    const int r0 = z * ny;
-    const int a0 = row_ptr[r0], a1 = row_ptr[r0 + ny];
-    cx<T>* op = out + (long long)p * o_stride;
-    for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
-        const int c = cell[i];
-        const int row = c / nx, x = c - row * nx;
-        const int y = row - r0;
-        op[i] = pl[y * ld + x];
     }
 }
 

@@ -135,11 +135,12 @@ def test_compute_requires_states_and_kernel():
 
 
 @pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
-@pytest.mark.parametrize("env", [{"CL_XY_FUSION": "1"}, {"CL_NO_REGISTER_FFT": "1"}, {"CL_L2_CHUNK_MB": "4"}])
+@pytest.mark.parametrize("env", [{"CL_XY_PLANE": "0"}, {"CL_NO_REGISTER_FFT": "1"}, {"CL_L2_CHUNK_MB": "4"}])
 def test_pass_variants_agree(mode, env, monkeypatch):
-    """The whole-plane xy kernels, the register row/column passes, the generic passes and every
-    chunking of the densities compute the same integrals."""
-    d = synth.build("c1", cells=(8, 8, 6))
+    """The register row/column passes (with the fused plane passes off), the generic passes and
+    every chunking of the densities compute the same integrals as the default passes (a 64^2
+    plane, so the default is the fused plane pass)."""
+    d = synth.build("c1", cells=(16, 16, 3))
     step = (synth.A_ZB / 4,) * 3
     specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
 
