@@ -96,7 +96,7 @@ bool xfwd(cudaStream_t s, Variant v, const cx<T>* rho, long long rho_stride, con
                     constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
                     auto kern = clk::k_xfwd_rf<T, Tag::r1, Tag::r2, LR, PAD>;
                     const size_t smem =
-                        sizeof(cx<T>) * ((size_t)N + (size_t)(clk::XfwdTile<N, PAD>::points + N) * (LR + 1));
+                        sizeof(cx<T>) * clk::XfwdPitch<Tag::r1, Tag::r2, LR, PAD, sizeof(cx<T>)>::elems;
                     set_smem(kern, smem);
                     const long long blocks = (nrows + LR - 1) / LR;
                     kern<<<dim3((unsigned)blocks, density_groups(blocks, cnt)), LR * Q, smem, s>>>(

@@ -341,18 +341,103 @@ struct XfwdTile {
     static constexpr int points = pos(N - 1) + 1;
 };
 
+// Pitches of the forward row pass, chosen at compile time by simulating the bank mapping
+// (W-element slots, one wavefront per group of W lanes; cost = the wavefronts of all of a
+// block's accesses):
+//   tile     T[pos(x)*TP + row]: phase A reads (lanes: LR rows fastest, then t) and the atom
+//            scatter (consecutive lanes on atoms 1, 2 or 4 points apart along a row);
+//   exchange item t's output r at t*EP + r*XP + row: phase A writes it (lanes as above),
+//            phase B reads position j + r*R1, i.e. item r's output j (lanes: j fastest, then
+//            rows).  The item pitch EP is separate from R1*XP so that items t do not all start
+//            on the same bank.
+template <int R1, int R2, int LR, bool PAD, int ES>
+struct XfwdPitch {
+    static constexpr int N = R1 * R2;
+    static constexpr int Q = R1 > R2 ? R1 : R2;
+    static constexpr int TH = LR * Q;
+    static constexpr int W = 128 / ES;
+    using Tile = XfwdTile<N, PAD>;
+    template <typename F>
+    static constexpr int groups(F addr) {  // sum over W-lane groups of the worst slot count
+        int total = 0;
+        for (int g0 = 0; g0 < TH; g0 += W) {
+            int cnt[32] = {};
+            int worst = 0;
+            for (int tid = g0; tid < g0 + W && tid < TH; ++tid) {
+                const int a = addr(tid);
+                if (a < 0) continue;
+                const int sl = a % W;
+                if (++cnt[sl] > worst) worst = cnt[sl];
+            }
+            total += worst;
+        }
+        return total;
+    }
+    static constexpr int tile_cost(int tp) {
+        int c = 0;
+        for (int j = 0; j < R1; ++j)
+            c += groups([&](int tid) {
+                const int lr = tid % LR, t = tid / LR;
+                return t < R2 ? Tile::pos(t + R2 * j) * tp + lr : -1;
+            });
+        for (int s = 1; s <= 4; s *= 2)  // scatter of atoms s points apart, one row
+            c += groups([&](int tid) { return tid * s < N ? Tile::pos(tid * s) * tp : -1; });
+        return c;
+    }
+    static constexpr int ex_cost(int xp, int ep) {
+        const int w = groups([&](int tid) {
+            const int lr = tid % LR, t = tid / LR;
+            return t < R2 ? t * ep + lr : -1;
+        });
+        const int r = groups([&](int tid) {
+            const int j = tid % R1, lr = tid / R1;
+            return lr < LR ? j * xp + lr : -1;
+        });
+        return R1 * w + R2 * r;
+    }
+    static constexpr int pick_tp() {
+        int best = LR, bc = 1 << 30;
+        for (int tp = LR; tp < LR + W; ++tp) {
+            const int c = tile_cost(tp);
+            if (c < bc) {
+                bc = c;
+                best = tp;
+            }
+        }
+        return best;
+    }
+    static constexpr int pick_ex(int which) {  // 0: XP, 1: EP
+        int bx = LR, be = R1 * LR, bc = 1 << 30;
+        for (int xp = LR; xp < LR + W; ++xp)
+            for (int ep = R1 * xp; ep < R1 * xp + W; ++ep) {
+                const int c = ex_cost(xp, ep);
+                if (c < bc) {
+                    bc = c;
+                    bx = xp;
+                    be = ep;
+                }
+            }
+        return which ? be : bx;
+    }
+    static constexpr int TP = pick_tp();
+    static constexpr int XP = pick_ex(0);
+    static constexpr int EP = pick_ex(1);
+    static constexpr size_t elems = (size_t)N + (size_t)Tile::points * TP + (size_t)R2 * EP;
+};
+
 template <typename T, int R1, int R2, int LR, bool PAD>
 __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R2, LR * cmax<R1, R2>::value>::value)
     k_xfwd_rf(const cx<T>* __restrict__ rho, long long rho_stride, const int* __restrict__ row_ptr,
               const int* __restrict__ cell, cx<T>* __restrict__ out, long long out_stride,
               const cx<T>* __restrict__ tw_g, RoundPhase rp, int ny, int nrows, int np, int skip_empty) {
     constexpr int N = R1 * R2;
-    constexpr int LP = LR + 1;
+    using Pitch = XfwdPitch<R1, R2, LR, PAD, sizeof(cx<T>)>;
+    constexpr int TP = Pitch::TP, XP = Pitch::XP, EP = Pitch::EP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using Tile = XfwdTile<N, PAD>;
     cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* tile = tw + N;
-    cx<T>* ex = tile + Tile::points * LP;
+    cx<T>* ex = tile + Tile::points * TP;
     const int r0 = blockIdx.x * LR;
     const int nr = min(LR, nrows - r0);
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
@@ -380,13 +465,13 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             if (i < a1) {
                 const int c = cell[i];
                 const int row = c / N, x = c - row * N;
-                slot[k] = Tile::pos(x) * LP + (row - r0);
+                slot[k] = Tile::pos(x) * TP + (row - r0);
                 ph[k] = round_phase(rp, x, row % ny, row / ny);
             }
         }
     }
     // cells without an atom stay zero for every density: the tile is cleared once
-    for (int e = threadIdx.x; e < Tile::points * LP; e += blockDim.x) tile[e] = mk(T(0), T(0));
+    for (int e = threadIdx.x; e < Tile::points * TP; e += blockDim.x) tile[e] = mk(T(0), T(0));
     __syncthreads();
     // the next density's atom values are loaded into registers while the current one is
     // transformed
@@ -409,7 +494,7 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
                 const int c = cell[i];
                 const int row = c / N, x = c - row * N;
                 const int y = row % ny, z = row / ny;
-                tile[Tile::pos(x) * LP + (row - r0)] = narrow<T>(cmulc(widen(rp_[i]), round_phase(rp, x, y, z)));
+                tile[Tile::pos(x) * TP + (row - r0)] = narrow<T>(cmulc(widen(rp_[i]), round_phase(rp, x, y, z)));
             }
         }
         __syncthreads();
@@ -418,10 +503,10 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             if (t < R2) {
                 cx<T> v[R1];
 #pragma unroll
-                for (int j = 0; j < R1; ++j) v[j] = tile[Tile::pos(t + R2 * j) * LP + lr];
+                for (int j = 0; j < R1; ++j) v[j] = tile[Tile::pos(t + R2 * j) * TP + lr];
                 dft<R1, -1>(v);
 #pragma unroll
-                for (int r = 0; r < R1; ++r) ex[(t * R1 + r) * LP + lr] = v[r];
+                for (int r = 0; r < R1; ++r) ex[t * EP + r * XP + lr] = v[r];
             }
         }
         __syncthreads();
@@ -430,7 +515,7 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
             if (store_row) {
                 cx<T> u[R2];
 #pragma unroll
-                for (int r = 0; r < R2; ++r) u[r] = ex[(j + r * R1) * LP + lr];
+                for (int r = 0; r < R2; ++r) u[r] = ex[r * EP + j * XP + lr];
 #pragma unroll
                 for (int r = 1; r < R2; ++r) u[r] = cmul(u[r], tw[r * j]);
                 dft<R2, -1>(u);
