@@ -98,7 +98,7 @@ struct PlaneLayout {
     static constexpr bool kConflictFree = deg_a() == 1 && deg_b() == 1 && deg_c() == 1;
 };
 
-// Shared memory of the plane kernels: the plane, the twiddles W_N^e, the atom phases (forward),
+// Shared memory of the plane kernels: the plane, the twiddles W_N^(t j) laid out [t][j], the atom phases (forward),
 // the atom masks and the row and item tables.
 template <typename T, int R1, int R2, int THREADS, bool FWD>
 struct PlaneSmem {
@@ -272,7 +272,9 @@ __global__ void __launch_bounds__(THREADS, MINB)
     __shared__ int cnt_sh[2 * NW];
     __shared__ int scan_sh[THREADS / 32];
     const int tid = threadIdx.x, z = blockIdx.x, r0 = z * N;
-    for (int i = tid; i < N; i += THREADS) tb.tw[i] = tw_g[i];
+    // twiddles laid out [t][j] = W_N^(t j): the x stage's phase-B lanes on consecutive j read
+    // consecutive words (the y stage's lanes share j: one broadcast)
+    for (int i = tid; i < N; i += THREADS) tb.tw[i] = tw_g[(i / R1) * (i % R1)];
     if (tid < 4) live_mask[tid] = 0u;
     __syncthreads();
     const int npairs = plane_rows<L>(row_ptr + r0, false, tb.prl, tb.lst, live_mask, cnt_sh);
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 #pragma unroll
                 for (int t = 0; t < R2; ++t) u[t] = ((tm >> t) & 1u) ? row[L::pos(R2 * j + t)] : mk(T(0), T(0));
 #pragma unroll
-                for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * j]);
+                for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * R1 + j]);
                 dft<R2, -1>(u);
 #pragma unroll
                 for (int s = 0; s < R2; ++s) row[L::pos(R2 * j + s)] = u[s];
@@ -405,7 +407,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 #pragma unroll
             for (int t = 0; t < R2; ++t) u[t] = col[j * L::RSTEP + L::rowbase(t)];
 #pragma unroll
-            for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * j]);
+            for (int t = 1; t < R2; ++t) u[t] = cmul(u[t], tw[t * R1 + j]);
             dft<R2, -1>(u);
 #pragma unroll
             for (int s = 0; s < R2; ++s) o[(long long)(j + R1 * s) * N + kx] = u[s];
@@ -436,7 +438,9 @@ __global__ void __launch_bounds__(THREADS, MINB)
     __shared__ int cnt_sh[2 * NW];
     __shared__ int scan_sh[THREADS / 32];
     const int tid = threadIdx.x, z = blockIdx.x, r0 = z * N;
-    for (int i = tid; i < N; i += THREADS) tb.tw[i] = tw_g[i];
+    // twiddles laid out [t][j] = W_N^(t j): the x stage's phase-B lanes on consecutive j read
+    // consecutive words (the y stage's lanes share j: one broadcast)
+    for (int i = tid; i < N; i += THREADS) tb.tw[i] = tw_g[(i / R1) * (i % R1)];
     if (tid < 4) live_mask[tid] = 0u;
     __syncthreads();
     const int npairs = plane_rows<L>(row_ptr + r0, true, tb.prl, tb.lst, live_mask, cnt_sh);
@@ -493,7 +497,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 #pragma unroll
             for (int t = 0; t < R2; ++t) u[t] = col[j * L::RSTEP + L::rowbase(t)];
 #pragma unroll
-            for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * j]);
+            for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * R1 + j]);
             dft<R2, +1>(u);
 #pragma unroll
             for (int s = 0; s < R2; ++s)
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 for (int s = 0; s < R2; ++s) u[s] = row[L::pos(R2 * j + s)];
                 dft<R2, +1>(u);
 #pragma unroll
-                for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * j]);
+                for (int t = 1; t < R2; ++t) u[t] = cmulc(u[t], tw[t * R1 + j]);
 #pragma unroll
                 for (int t = 0; t < R2; ++t)
                     if ((tm >> t) & 1u) row[L::pos(R2 * j + t)] = u[t];

@@ -440,7 +440,9 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
     cx<T>* ex = tile + Tile::points * TP;
     const int r0 = blockIdx.x * LR;
     const int nr = min(LR, nrows - r0);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
+    // twiddles laid out [r][j] = W_N^(r j), so that phase B's lanes on consecutive j read
+    // consecutive words
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[(i / R1) * (i % R1)];
     const int a0 = row_ptr[r0], a1 = row_ptr[r0 + nr];
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
@@ -517,7 +519,7 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
 #pragma unroll
                 for (int r = 0; r < R2; ++r) u[r] = ex[r * EP + j * XP + lr];
 #pragma unroll
-                for (int r = 1; r < R2; ++r) u[r] = cmul(u[r], tw[r * j]);
+                for (int r = 1; r < R2; ++r) u[r] = cmul(u[r], tw[r * R1 + j]);
                 dft<R2, -1>(u);
                 cx<T>* o = out + (long long)p * out_stride + (long long)(r0 + lr) * N + j;
 #pragma unroll
@@ -625,7 +627,9 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
     cx<T>* rows = ex + LR * PP;  // [LR][NP], natural order
     const int r0 = blockIdx.x * LR;
     const int nr = min(LR, nrows - r0);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
+    // twiddles laid out [r][j] = W_N^(r j), so that phase B's lanes on consecutive j read
+    // consecutive words
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[(i / R1) * (i % R1)];
     const int a0 = row_ptr[r0], a1 = row_ptr[r0 + nr];
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
@@ -655,7 +659,7 @@ __global__ void __launch_bounds__(LR * cmax<R1, R2>::value, col_min_blocks<R1, R
 #pragma unroll
             for (int r = 0; r < R2; ++r) u[r] = ex[lb * PP + jb + r * (R1 + 1)];
 #pragma unroll
-            for (int r = 1; r < R2; ++r) u[r] = cmulc(u[r], tw[r * jb]);
+            for (int r = 1; r < R2; ++r) u[r] = cmulc(u[r], tw[r * R1 + jb]);
             dft<R2, +1>(u);
 #pragma unroll
             for (int r = 0; r < R2; ++r) rows[lb * NP + Pitch::pos(jb + r * R1)] = u[r];
