@@ -1,16 +1,17 @@
 #!/usr/bin/env python
-"""Throughput of the Coulomb-integral path on one node: integrals/s of the FP32 form
-(FP32 transforms, FP64 kernel/twiddles/reductions/round sum), every integral checked against
-the all-FP64 plain path within max(1e-6 |I|, 1e-9 eV).
+"""Throughput of the Coulomb-integral path on one node: integrals/s of the FP32 form, every
+integral checked against the all-FP64 plain path within max(1e-6 |I|, 1e-9 eV), and a bounded
+sample of integrals against the FP64 oracle.
 
 A step is one full request over one synthetic zinc-blende structure: pair densities, the
-8-round convolution of every prepared density and the real-space reductions of every
-requested integral (split-precision tensor-core Gram with FP64 accumulation).  `value` is the
-device time (CUDA events) of one CUDA-graph replay of the prepared request per step, with the
-inputs resident in HBM; `e2e` runs the public C ABI from pinned host buffers (coefficient and
-cell upload, compute, result download) every step.
+convolution of every prepared density and the real-space reductions of every requested
+integral (split-precision tensor-core Gram with FP64 accumulation).  `value` is the device
+time (CUDA events) of one CUDA-graph replay of the prepared request per step, with the inputs
+resident in HBM; `e2e` runs the public C ABI from pinned host buffers (coefficient and cell
+upload, compute, result download) every step.  The default workload is the 2.1M-atom box
+(64^3 zinc-blende cells, 256^3 grid, 20 orbitals, 4 e + 4 h, 1,024 integrals).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c3|c1] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c1|c2|c3|c4|c5] [--impl ours|reference]
 
 With N > 1 (torchrun) each rank computes an independent structure of the same size (seeded
 by rank; structures are independent objects), so the work per GPU is fixed: weak scaling.
@@ -40,6 +41,12 @@ WORKLOADS = {
           "orbitals, 4e+4h each, eeee,hhhh,ehhe,eheh (16 x 1024 integrals), one CUDA-graph launch per batch",
 }
 DIELECTRIC = 10.89
+HEADLINE_MODE = 1  # coulombo_lattice_b200.MODE_FP32_ROUNDS
+FORM_TEXT = {
+    0: "all-FP64: 8 rounds of N-point FFTs (the reference's method), FP64 Gram",
+    1: "FP32 transforms in 8 rounds; FP64 kernel, twiddles, V accumulation and round sum; split-precision "
+       "(3xTF32) tensor-core reductions accumulated in FP64",
+}
 
 
 def parse_args():
@@ -47,7 +54,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--config", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", default=None,
@@ -146,14 +153,27 @@ class ClockSampler:
 # ----------------------------------------------------------------------------------------
 # workload
 # ----------------------------------------------------------------------------------------
-def build_workload(config, seed_index=None, cells=None):
+def build_workload(config, seed_index=None, cells=None, with_library=True):
+    """Synthetic structure, states and integral list.  The reference arm enumerates the
+    integrals with the oracle's restatement of Pattern (with_library=False), so that its
+    process never loads this repository's library."""
     from coulombo_lattice_b200 import synth
-    import coulombo_lattice_b200 as cl
     d = synth.build(config, cells=cells, seed_index=seed_index)
     n = d["states"].shape[0]
-    d["specs"] = np.ascontiguousarray(cl.enumerate_integrals(d["integrals"], n, d["holes"]))
+    if with_library:
+        import coulombo_lattice_b200 as cl
+        d["specs"] = np.ascontiguousarray(cl.enumerate_integrals(d["integrals"], n, d["holes"]))
+    else:
+        from oracle import host as H
+        d["specs"] = np.array(H.enumerate_integrals(H.Pattern(d["integrals"], d["holes"]), n),
+                              dtype=np.int16).reshape(-1, 4)
     d["step"] = (synth.A_ZB / 4,) * 3
     return d
+
+
+def config_of(args, n_int):
+    """The `config` object of both arms' JSON lines (identical by construction)."""
+    return {"workload": workload_name(args), "integrals_per_step": int(n_int)}
 
 
 def gpu_local_cpus(device):
@@ -175,84 +195,133 @@ def gpu_local_cpus(device):
         return None
 
 
-def cpu_sample(d, n_left, threads):
-    """The oracle's FP64 reference-structured loop (Planner order, 8-round prepare per left
-    density, real-space calculate per right density) over the first n_left prepared
-    densities; returns (seconds, integrals covered, integrals/s extrapolated to the request)."""
-    from oracle import coulomb as C
-    from oracle import host as H
-    specs = [tuple(int(v) for v in s) for s in d["specs"]]
-    n = d["states"].shape[0]
-    plan = H.compute_plan(specs, n * (n + 1) // 2)
-    lefts = sorted({s[1][0] for s in plan})
-    chosen = set(lefts[:n_left])
-    t0 = time.perf_counter()
-    ghat = C.kernel_spectrum(C.kernel_octant(d["dims"], d["step"], DIELECTRIC), d["dims"])
-    t_init = time.perf_counter() - t0
+class OracleLoop:
+    """The oracle's FP64 restatement of the reference's integral loop, structured like the
+    reference (coulombo.cpp:186-209): in plan order, a dense zeroed pair-density grid per
+    product (Product.cpp:16-30), 8 rounds of N-point FFTs per new left density
+    (CoulombCalculator.cpp:105-163) and a dense sum over the grid per right density
+    (CoulombCalculator.cpp:165-172).  SciPy's pocketfft runs on every host thread.
 
-    def density(prod, conj):
-        fl, fr = H.product_states(prod)
-        rho = C.pair_density_atoms(d["states"][fl - 1], d["states"][fr - 1], conj)
-        return C.scatter_density(rho, d["cells_idx"], d["dims"])
+    Large integral lists (more than 50,000) are planned over the integrals of their first two
+    left products only, which is all a bounded sample reaches."""
 
-    t0 = time.perf_counter()
-    covered = 0
-    last_left, last_right, last_rc = -1, -1, None
-    V = None
-    for (sid, left, right) in plan:
-        if left[0] not in chosen:
-            continue
-        if left[0] != last_left:
-            V = C.prepare(density(left[0], False), ghat)
-            last_left, last_right = left[0], -1
-        rc = left[1] != right[1]
-        if right[0] != last_right or rc != last_rc:
-            C.calculate(V, density(right[0], rc))
-            last_right, last_rc = right[0], rc
-        covered += 1
-    t_loop = time.perf_counter() - t0
-    frac = len(chosen) / len(lefts)
-    est_total = t_init + t_loop / frac
-    return t_loop + t_init, covered, len(specs) / est_total, len(chosen), len(lefts)
+    def __init__(self, d):
+        from oracle import coulomb as C
+        from oracle import host as H
+        self.C, self.H, self.d = C, H, d
+        specs = d["specs"]
+        n = d["states"].shape[0]
+        ids = np.arange(len(specs))
+        if len(specs) > 50000:
+            lp = np.array([H.product_of(int(a), int(b))[0] for a, b in zip(specs[:, 0], specs[:, 3])])
+            keep = np.isin(lp, np.unique(lp)[:2])
+            ids = ids[keep]
+        sub = [tuple(int(v) for v in specs[i]) for i in ids]
+        plan = H.compute_plan(sub, n * (n + 1) // 2)
+        self.groups = []  # [(left, [(spec id, left, right), ...])] in plan order
+        for (sid, left, right) in plan:
+            if not self.groups or self.groups[-1][0] != left[0]:
+                self.groups.append((left[0], []))
+            self.groups[-1][1].append((int(ids[sid]), left, right))
+        t0 = time.perf_counter()
+        self.ghat = C.kernel_spectrum(C.kernel_octant(d["dims"], d["step"], DIELECTRIC), d["dims"])
+        self.init_s = time.perf_counter() - t0
+        self.next_group = 0
+
+    def _density(self, prod, conj):
+        fl, fr = self.H.product_states(prod)
+        rho = self.C.pair_density_atoms(self.d["states"][fl - 1], self.d["states"][fr - 1], conj)
+        return self.C.scatter_density(rho, self.d["cells_idx"], self.d["dims"])
+
+    def run(self, budget_s=None, groups=1):
+        """Runs the next `groups` left densities (cycling) with all their steps, or stops after
+        the step that crosses budget_s.  Returns (seconds, {spec id: value})."""
+        C = self.C
+        values = {}
+        t0 = time.perf_counter()
+        for _ in range(groups):
+            left, steps = self.groups[self.next_group % len(self.groups)]
+            self.next_group += 1
+            V = C.prepare(self._density(left, False), self.ghat)
+            last_right, last_rc, val = -1, None, 0j
+            for (sid, lf, right) in steps:
+                rc = lf[1] != right[1]
+                if right[0] != last_right or rc != last_rc:
+                    val = C.calculate(V, self._density(right[0], rc))
+                    last_right, last_rc = right[0], rc
+                values[sid] = np.conj(val) if lf[1] else val
+                if budget_s is not None and time.perf_counter() - t0 > budget_s:
+                    return time.perf_counter() - t0, values
+        return time.perf_counter() - t0, values
 
 
-def cpu_baseline_entry(d, budget_lefts, threads, kind="port"):
-    secs, covered, ips, k, P = cpu_sample(d, budget_lefts, threads)
-    return {"value": ips, "unit": "integrals/s", "cores": threads, "kind": kind,
-            "sample": "CPU restatement (NumPy/SciPy pocketfft FP64, workers=%d), not the reference binary: "
-                      "%d of %d prepared densities with their calculate() calls (%d integrals) in %.1f s, "
-                      "extrapolated x%d/%d to the full request" % (threads, k, P, covered, secs, P, k)}
+def accuracy_vs_oracle(values, got, fp64):
+    """Worst error over the gate of `got` (full integral vector) on the oracle's sample."""
+    ids = np.array(sorted(values), dtype=np.int64)
+    want = np.array([values[i] for i in ids])
+    err = np.abs(got[ids] - want)
+    lim = (1e-10 * np.abs(want) + 1e-16) if fp64 else np.maximum(1e-6 * np.abs(want), 1e-9)
+    return {"integrals": int(len(ids)), "worst_err_over_gate": float((err / lim).max()),
+            "max_abs_err_eV": float(err.max()),
+            "max_rel_err": float((err / np.maximum(np.abs(want), 1e-300)).max()), "pass": bool(np.all(err <= lim)),
+            "gate": "1e-10 relative" if fp64 else "max(1e-6 |I|, 1e-9 eV)"}
 
 
 # ----------------------------------------------------------------------------------------
 # arms
 # ----------------------------------------------------------------------------------------
 def run_reference(args):
+    """The reference's CPU path on the host cores: the oracle's reference-structured FP64 loop
+    (no repository library is loaded).  One step = the next prepared left density with all of
+    its calculate() calls; value = integrals computed / seconds over the timed steps."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    d = build_workload(args.config, cells=cells_arg(args))
-    threads = os.cpu_count() or 1
-    # one step's sample shrinks with the step count, so that --steps K --warmup W ends within a
-    # few minutes (C2: about 0.9 s a step with one prepared density)
-    n_left = {"c1": 2, "c2": 2, "c3": 1, "c4": 1}[args.config] if args.steps <= 20 else 1
+    threads = len(os.sched_getaffinity(0))
+    if args.config == "c5":
+        # the sixteen structures in turn, one left density of the next structure per step
+        from coulombo_lattice_b200 import synth
+        loops, n_req = [], 0
+        for i in range(len(synth.C5_CELLS)):
+            dd = synth.build_c5(i)
+            from oracle import host as H
+            dd["specs"] = np.array(H.enumerate_integrals(H.Pattern(dd["integrals"], dd["holes"]),
+                                                         dd["states"].shape[0]), dtype=np.int16).reshape(-1, 4)
+            dd["step"] = (synth.A_ZB / 4,) * 3
+            n_req += len(dd["specs"])
+            loops.append(OracleLoop(dd))
+        budget = None
+    else:
+        d = build_workload(args.config, cells=cells_arg(args), with_library=False)
+        n_req = len(d["specs"])
+        loops = [OracleLoop(d)]
+        budget = {"c4": 8.0}.get(args.config)  # a C4 left density has ~3,200 dense steps
+    k = 0
     for _ in range(args.warmup):
-        cpu_sample(d, n_left, threads)
-    vals, secs = [], []
+        loops[k % len(loops)].run(budget)
+        k += 1
+    secs, covered = [], 0
     for _ in range(args.steps):
-        s, covered, ips, k, P = cpu_sample(d, n_left, threads)
-        vals.append(ips)
+        s, vals = loops[k % len(loops)].run(budget)
+        k += 1
         secs.append(s)
-    value = float(np.median(vals))
+        covered += len(vals)
+    loop = loops[0]
+    value = covered / sum(secs)
     line = {
         "impl": "reference", "metric": "integrals/s", "value": value, "unit": "integrals/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * len(d["specs"]) / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args), "integrals_per_step": int(len(d["specs"]))},
+        "config": config_of(args, n_req),
         "cpu_baseline": {"value": value, "unit": "integrals/s", "cores": threads, "kind": "port",
-                         "sample": "each step: %d of %d prepared densities of the oracle's reference-structured "
-                                   "FP64 loop, extrapolated to the full request; median of %d steps"
-                                   % (n_left, P, args.steps)},
+                         "sample": "the oracle's FP64 restatement of the reference's loop (dense pair-density grids, "
+                                   "8 rounds of SciPy pocketfft FFTs on %d threads per left density, dense calculate "
+                                   "per step), not the reference binary (MPI/FFTW/Armadillo are not installed): each "
+                                   "step is the next of %d left densities%s, %d integrals in %.1f s over %d steps; the "
+                                   "one-time kernel spectrum (%.2f s) is excluded like the GPU arm's"
+                                   % (threads, sum(len(lp.groups) for lp in loops),
+                                      " (cut at %.0f s)" % budget if budget else "", covered, sum(secs), args.steps,
+                                      sum(lp.init_s for lp in loops))},
         "e2e": {"value": value, "unit": "integrals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -283,7 +352,7 @@ def run_batch(args):
         plain.set_states(d["states"], d["cells_idx"], d["holes"])
         v64 = plain.compute(specs)
         plain.close()
-        cc = cl.CoulombCalculator(d["dims"], step, cl.MODE_FP32_FOURIER)
+        cc = cl.CoulombCalculator(d["dims"], step, HEADLINE_MODE)
         cc.initialize(dielectric=DIELECTRIC)
         cc.set_states(d["states"], d["cells_idx"], d["holes"])
         r = cc.request(specs)
@@ -328,8 +397,8 @@ def run_batch(args):
         "metric": "integrals/s", "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOADS["c5"], "integrals_per_step": int(n_int_total),
-                   "grids": [list(map(int, d["dims"])) for d, _ in structs]},
+        "config": config_of(args, n_int_total),
+        "details": {"grids": [list(map(int, d["dims"])) for d, _ in structs], "form": FORM_TEXT[HEADLINE_MODE]},
         "accuracy": {"worst_err_over_gate": accuracy_worst, "pass": accuracy_worst <= 1.0,
                      "gate": "max(1e-6|I|, 1e-9 eV) vs the all-FP64 plain path"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": fft[dom][2] / (fft[dom][0] / 1e3) / 1e9,
@@ -396,7 +465,7 @@ def run_ours(args):
     plain.close()
     plain_ms = max_over_ranks(min(plain_ms))
 
-    calc = cl.CoulombCalculator(d["dims"], d["step"], cl.MODE_FP32_FOURIER)
+    calc = cl.CoulombCalculator(d["dims"], d["step"], HEADLINE_MODE)
     t0 = time.perf_counter()
     calc.initialize(dielectric=DIELECTRIC)
     init_ms = 1e3 * (time.perf_counter() - t0)
@@ -406,9 +475,11 @@ def run_ours(args):
 
     err = np.abs(v32 - v64)
     lim = np.maximum(1e-6 * np.abs(v64), 1e-9)
-    accuracy = {"max_rel_err": float(np.max(err / np.maximum(np.abs(v64), 1e-300))),
-                "max_abs_err_eV": float(err.max()), "worst_err_over_gate": float((err / lim).max()),
-                "gate": "max(1e-6|I|, 1e-9 eV) vs the all-FP64 plain path", "pass": bool(np.all(err <= lim))}
+    accuracy = {"vs_plain_fp64": {
+        "integrals": int(n_int), "max_rel_err": float(np.max(err / np.maximum(np.abs(v64), 1e-300))),
+        "max_abs_err_eV": float(err.max()), "worst_err_over_gate": float((err / lim).max()),
+        "gate": "max(1e-6|I|, 1e-9 eV) vs the all-FP64 plain path on every integral",
+        "pass": bool(np.all(err <= lim))}}
 
     # ---- timed region: resident inputs, one CUDA-graph replay of the prepared request per
     # step (pair densities, 8 rounds, reductions, results to pinned host), device time ---------
@@ -525,17 +596,17 @@ def run_ours(args):
         "metric": "integrals/s", "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(args), "integrals_per_step": int(n_int),
-                   "form": "FP32 transforms; FP64 kernel, twiddles, V accumulation and round sum; split-precision "
-                           "(3xTF32) tensor-core reductions accumulated in FP64",
-                   "l2": "inputs larger than L2 (126 MB): %.0f MB of transformed grids per request, "
-                         "streamed in chunks" % buf_mb, "prepared_densities": n_prepared,
-                   "init_ms_kernel_build": init_ms, "wall_ms_per_step": wall_ms / args.steps,
-                   "timing": "device time (CUDA events) of one CUDA-graph replay of the prepared request per "
-                             "step; per-kernel times from the same graph captured with an event pair around "
-                             "every launch (%.3f ms per step)" % (prof_dev_ms / args.steps)},
+        "config": config_of(args, n_int),
+        "details": {"form": FORM_TEXT[HEADLINE_MODE],
+                    "l2": "inputs larger than L2 (126 MB): %.0f MB of transformed grids per request, "
+                          "streamed in chunks" % buf_mb, "prepared_densities": n_prepared,
+                    "init_ms_kernel_build": init_ms, "wall_ms_per_step": wall_ms / args.steps,
+                    "timing": "device time (CUDA events) of one CUDA-graph replay of the prepared request per "
+                              "step; per-kernel times from the same graph captured with an event pair around "
+                              "every launch (%.3f ms per step)" % (prof_dev_ms / args.steps)},
         "accuracy": accuracy,
         "plain_fp64": {"value": world * n_int / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                       "form": FORM_TEXT[cl.MODE_FP64_PLAIN],
                        "timing": "device time of a CUDA-graph replay of the prepared request, best of 3",
                        "speedup_of_fp32_form": plain_ms / ms_per_step},
         "e2e": {"value": world * n_int / (e2e_ms / 1e3), "unit": "integrals/s", "h2d_bytes_per_step": int(h2d),
@@ -564,9 +635,24 @@ def run_ours(args):
         "clocks": clock_info,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        n_left = {"c1": 2, "c2": 4, "c3": 1, "c4": 1}[args.config]
-        line["cpu_baseline"] = cpu_baseline_entry(d, n_left, threads)
+        # the oracle's reference-structured FP64 loop on a bounded sample (about 20 s) of this
+        # workload's left densities: the CPU baseline, and the per-integral check of both forms
+        loop = OracleLoop(d)
+        budget = {"c1": 5.0}.get(args.config, 20.0)
+        secs, vals = 0.0, {}
+        while secs < budget and loop.next_group < len(loop.groups):
+            s_, v_ = loop.run(budget - secs)
+            secs += s_
+            vals.update(v_)
+        threads = len(os.sched_getaffinity(0))
+        line["cpu_baseline"] = {
+            "value": len(vals) / secs, "unit": "integrals/s", "cores": threads, "kind": "port",
+            "sample": "the oracle's FP64 restatement of the reference's loop (dense pair-density grids, 8 rounds of "
+                      "SciPy pocketfft FFTs on %d threads, dense calculate per step), not the reference binary: "
+                      "%d of the request's %d integrals (%d left densities) in %.1f s, not extrapolated"
+                      % (threads, len(vals), n_int, loop.next_group, secs)}
+        line["accuracy"]["vs_oracle"] = {"fp32_form": accuracy_vs_oracle(vals, v32, False),
+                                         "plain_fp64": accuracy_vs_oracle(vals, v64, True)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     calc.close()

@@ -21,8 +21,16 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcoulombo_lattice.so")
 BIN_DIR = os.path.join(_HERE, "bin")
 
-MODE_FP64_PLAIN = 0
-MODE_FP32_FOURIER = 1
+# precision / algorithm forms (include/coulombo_lattice.h CL_MODE_*)
+MODE_FP64_PLAIN = 0   # all-FP64, 8 rounds of N-point transforms (the reference's method)
+MODE_FP32_ROUNDS = 1  # FP32 transforms, FP64 kernel/twiddles/round sum/reductions, 8 rounds
+MODE_FP32_FOURIER = MODE_FP32_ROUNDS  # former name of MODE_FP32_ROUNDS
+ALL_MODES = [MODE_FP64_PLAIN, MODE_FP32_ROUNDS]
+
+
+def mode_is_fp64(mode):
+    """True for the all-FP64 forms (parity gate 1e-10 relative)."""
+    return mode in (MODE_FP64_PLAIN,)
 
 # kernel classes of cl_kernel_profile (include/coulombo_lattice.h CL_KCLASS_*)
 KERNEL_CLASSES = ["pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram", "kernel_build", "gram_split",

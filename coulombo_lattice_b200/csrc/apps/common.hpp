@@ -42,7 +42,7 @@ inline void parse_common_options(const clio::ParseResults& pr, Inputs& in) {
         if (value == "fp64")
             in.mode = CL_MODE_FP64_PLAIN;
         else if (value == "fp32")
-            in.mode = CL_MODE_FP32_FOURIER;
+            in.mode = CL_MODE_FP32_ROUNDS;
         else
             clio::throwfr("invalid value for precision: %s", value.c_str());
     }

@@ -814,7 +814,7 @@ void run_rounds_mode(cl_ctx* c, const void* rho, long long rho_stride, int np, c
 // ---------------------------------------------------------------------------------------
 // Tensor-core Gram (FP32 form): TF32 split pass + tcgen05 GEMM, see gram_tc.cuh.
 // ---------------------------------------------------------------------------------------
-bool use_tc_gram(const cl_ctx* c) { return c->mode == CL_MODE_FP32_FOURIER && !std::getenv("CL_NO_TC_GRAM"); }
+bool use_tc_gram(const cl_ctx* c) { return c->mode == CL_MODE_FP32_ROUNDS && !std::getenv("CL_NO_TC_GRAM"); }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -1125,7 +1125,7 @@ int cl_create(cl_ctx** out, int nx, int ny, int nz, double sx, double sy, double
     int st = cl::guarded([&] {
         if (!out) cl::fail(CL_ERR_ARGUMENT, "null output pointer");
         if (nx <= 0 || ny <= 0 || nz <= 0) cl::fail(CL_ERR_ARGUMENT, "dimensions must be positive");
-        if (mode != CL_MODE_FP64_PLAIN && mode != CL_MODE_FP32_FOURIER) cl::fail(CL_ERR_ARGUMENT, "unknown mode %d", mode);
+        if (mode != CL_MODE_FP64_PLAIN && mode != CL_MODE_FP32_ROUNDS) cl::fail(CL_ERR_ARGUMENT, "unknown mode %d", mode);
         const int dims[3] = {nx, ny, nz};
         for (int d = 0; d < 3; ++d) {
             if (!smooth235(dims[d]))
@@ -1473,6 +1473,24 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
         CL_CUDA(cudaStreamSynchronize(c->stream));
         return;
     }
+    // The integral list is checked (and planned) before any copy reads the caller's buffer.
+    std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
+    for (int64_t i = 0; i < n_int; ++i)
+        for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
+    const auto plan = cl::orient_steps(n_states, specs);
+    // On every error path below, the copies already queued from the caller's buffer (and the
+    // work waiting on them) finish before the call returns, so the buffer is free for reuse
+    // once the call has returned, whatever its status.
+    struct DrainOnError {
+        cudaStream_t a, b;
+        bool armed = true;
+        ~DrainOnError() {
+            if (!armed) return;
+            cudaStreamSynchronize(a);
+            cudaStreamSynchronize(b);
+            cudaGetLastError();
+        }
+    } drain{c->copy_stream, c->stream};
     // Uploads, one state at a time on the copy stream.  From pinned memory they are all enqueued
     // now and overlap the planning below; from pageable memory a copy returns only once staged,
     // so they are interleaved with the groups that need them (the groups already enqueued run
@@ -1493,10 +1511,6 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
             upload_through(n_states - 1);
         cudaGetLastError();  // pageable memory is not an error
     }
-    std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
-    for (int64_t i = 0; i < n_int; ++i)
-        for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
-    const auto plan = cl::orient_steps(n_states, specs);
     const int P = n_states * (n_states + 1) / 2;
     std::vector<int> is_left(P, 0), is_right(P, 0);
     for (const auto& st : plan) {
@@ -1583,7 +1597,8 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
     std::vector<double> h((size_t)4 * nl * nr + 1);
     CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CL_CUDA(cudaStreamSynchronize(c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));  // after the wait on the last upload: all copies done
+    drain.armed = false;
     check_gram_slot(h.back());
     float t02, t23, t03;
     CL_CUDA(cudaEventElapsedTime(&t02, c->ev[0], c->ev[2]));
@@ -1980,7 +1995,7 @@ int cl_fft3d(int nx, int ny, int nz, int batch, int sign, int fp32, double* data
         if (nx <= 0 || ny <= 0 || nz <= 0 || batch <= 0 || !data || (sign != -1 && sign != 1))
             cl::fail(CL_ERR_ARGUMENT, "invalid FFT arguments");
         cl_ctx* raw = nullptr;
-        if (cl_create(&raw, nx, ny, nz, 1, 1, 1, fp32 ? CL_MODE_FP32_FOURIER : CL_MODE_FP64_PLAIN) != CL_OK)
+        if (cl_create(&raw, nx, ny, nz, 1, 1, 1, fp32 ? CL_MODE_FP32_ROUNDS : CL_MODE_FP64_PLAIN) != CL_OK)
             cl::fail(CL_ERR_ARGUMENT, "%s", cl_last_error());
         std::unique_ptr<cl_ctx> c(raw);
         const long long M = c->M;
@@ -2013,24 +2028,29 @@ int cl_fft3d(int nx, int ny, int nz, int batch, int sign, int fp32, double* data
             const int ychunks = (nx + yt.W - 1) / yt.W;
             const long long nxy = (long long)nx * ny;
             const long long zblocks = (nxy + zt.W - 1) / zt.W;
-            if (sign < 0) {
-                ensure_smem(clk::k_xpass<-1, T>, xt.smem);
-                ensure_smem(clk::k_ypass<-1, T>, yt.smem);
-                clk::k_xpass<-1, T><<<dim3(xblocks, batch), 256, xt.smem, c->stream>>>(buf, M, X.plan, twx, nx, nrows,
-                                                                                      xt.rows, xt.ld);
-                CL_LAUNCHED();
-                clk::k_ypass<-1, T><<<dim3(ychunks * nz, batch), 256, yt.smem, c->stream>>>(buf, M, Y.plan, twy, nx,
-                                                                                           ny, yt.W, ychunks);
-                CL_LAUNCHED();
-            } else {
-                ensure_smem(clk::k_xpass<+1, T>, xt.smem);
-                ensure_smem(clk::k_ypass<+1, T>, yt.smem);
-                clk::k_xpass<+1, T><<<dim3(xblocks, batch), 256, xt.smem, c->stream>>>(buf, M, X.plan, twx, nx, nrows,
-                                                                                      xt.rows, xt.ld);
-                CL_LAUNCHED();
-                clk::k_ypass<+1, T><<<dim3(ychunks * nz, batch), 256, yt.smem, c->stream>>>(buf, M, Y.plan, twy, nx,
-                                                                                           ny, yt.W, ychunks);
-                CL_LAUNCHED();
+            // the x and y passes take the grid index from blockIdx.y (at most 65535): slices of grids
+            for (int b0 = 0; b0 < batch; b0 += 65535) {
+                const int nb = std::min(65535, batch - b0);
+                cx<T>* slice = buf + (long long)b0 * M;
+                if (sign < 0) {
+                    ensure_smem(clk::k_xpass<-1, T>, xt.smem);
+                    ensure_smem(clk::k_ypass<-1, T>, yt.smem);
+                    clk::k_xpass<-1, T><<<dim3(xblocks, nb), 256, xt.smem, c->stream>>>(slice, M, X.plan, twx, nx,
+                                                                                       nrows, xt.rows, xt.ld);
+                    CL_LAUNCHED();
+                    clk::k_ypass<-1, T><<<dim3(ychunks * nz, nb), 256, yt.smem, c->stream>>>(slice, M, Y.plan, twy,
+                                                                                            nx, ny, yt.W, ychunks);
+                    CL_LAUNCHED();
+                } else {
+                    ensure_smem(clk::k_xpass<+1, T>, xt.smem);
+                    ensure_smem(clk::k_ypass<+1, T>, yt.smem);
+                    clk::k_xpass<+1, T><<<dim3(xblocks, nb), 256, xt.smem, c->stream>>>(slice, M, X.plan, twx, nx,
+                                                                                       nrows, xt.rows, xt.ld);
+                    CL_LAUNCHED();
+                    clk::k_ypass<+1, T><<<dim3(ychunks * nz, nb), 256, yt.smem, c->stream>>>(slice, M, Y.plan, twy,
+                                                                                            nx, ny, yt.W, ychunks);
+                    CL_LAUNCHED();
+                }
             }
             ensure_smem(clk::k_zpass<T>, zt.smem);
             clk::k_zpass<T><<<(unsigned)zblocks, 256, zt.smem, c->stream>>>(buf, M, Z.plan, twz, nullptr, nxy, nz,

@@ -13,9 +13,12 @@
 // loads the library holds it until the process exits.  In host code its name is only a
 // host-side stand-in; the device address is obtained once per device with
 // cudaGetSymbolAddress, on the first call made with that device current (so make that first
-// call before any stream capture).  Every call rewrites all table entries it reads, so
-// nothing has to start at zero; but all calls share the one array, so calls that overlap on
-// the GPU (e.g. from threads using per-thread default streams) race on it.
+// call before any stream capture).  The address is kept for the life of the process: after a
+// cudaDeviceReset the module is loaded again and the array may move, so a process that resets
+// a device must not call this entry point on it afterwards.  Every call rewrites all table
+// entries it reads, so nothing has to start at zero; but all calls share the one array, so
+// calls that overlap on the GPU (e.g. from threads using per-thread default streams) race on
+// it.
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
@@ -122,10 +125,16 @@ void run(int nx, int ny, int nz, int batch, clk::cx<double>* data, const clk::cx
     const clk::FftPlan px = plan_for(nx), py = plan_for(ny), pz = plan_for(nz);
     const int ychunks = (nx + wy - 1) / wy;
     const long long nxy = (long long)nx * ny;
-    clk::k_xpass<S, double><<<dim3((nrows + rows - 1) / rows, batch), 256, xs>>>(data, M, px, twx, nx, nrows, rows, ld);
-    NA_CUDA(cudaGetLastError());
-    clk::k_ypass<S, double><<<dim3(ychunks * nz, batch), 256, ys>>>(data, M, py, twy, nx, ny, wy, ychunks);
-    NA_CUDA(cudaGetLastError());
+    // the x and y passes take the grid index from blockIdx.y (at most 65535): slices of grids
+    for (int b0 = 0; b0 < batch; b0 += 65535) {
+        const int nb = std::min(65535, batch - b0);
+        C* slice = data + (long long)b0 * M;
+        clk::k_xpass<S, double><<<dim3((nrows + rows - 1) / rows, nb), 256, xs>>>(slice, M, px, twx, nx, nrows, rows,
+                                                                                  ld);
+        NA_CUDA(cudaGetLastError());
+        clk::k_ypass<S, double><<<dim3(ychunks * nz, nb), 256, ys>>>(slice, M, py, twy, nx, ny, wy, ychunks);
+        NA_CUDA(cudaGetLastError());
+    }
     clk::k_zpass<double><<<(unsigned)((nxy + wz - 1) / wz), 256, zs>>>(data, M, pz, twz, nullptr, nxy, nz, wz, batch, S);
     NA_CUDA(cudaGetLastError());
 }

@@ -36,7 +36,9 @@ extern "C" {
 
 /* precision / algorithm forms */
 #define CL_MODE_FP64_PLAIN   0  /* all-FP64: 8 rounds of FFT -> x Ghat -> iFFT, real-space dot */
-#define CL_MODE_FP32_FOURIER 1  /* FP32 FFT stages, FP64 kernel/twiddles/reductions/round sum */
+#define CL_MODE_FP32_ROUNDS  1  /* the same 8 rounds with FP32 FFT stages; FP64 kernel, twiddles,
+                                   round sum and reductions (split-precision tensor-core Gram) */
+#define CL_MODE_FP32_FOURIER CL_MODE_FP32_ROUNDS /* former name of CL_MODE_FP32_ROUNDS */
 
 typedef struct cl_ctx cl_ctx;
 
@@ -205,8 +207,9 @@ int cl_fft3d(int nx, int ny, int nz, int batch, int sign, int fp32, double* data
  * after the transform has finished.  It allocates nothing: the twiddle tables live in a
  * fixed 192 KiB array inside the library (held by every GPU that loads it until exit), so
  * each axis is limited to 4096 points and longer axes are rejected.  The first call on a
- * device looks up that array's device address; make it before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race. */
+ * device looks up that array's device address; make it before any stream capture.  That
+ * address is kept until the process exits, so do not call this again on a device after
+ * cudaDeviceReset.  All calls share the array: calls that overlap on the GPU race. */
 int cl_fft3d_noalloc(int nx, int ny, int nz, int batch, int sign, double* data);
 
 /* ---------------------------------------------------------------------------------------

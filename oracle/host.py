@@ -302,6 +302,86 @@ def compute_integrals(states, cells, dims, step, specs, dielectric=1.0, onsite=0
     return values
 
 
+def compute_integrals_sampled(states, cells, dims, step, specs, lefts=None, dielectric=1.0, onsite=0.0,
+                              tf_lattice=None, ghat=None, timer=None):
+    """The same plan loop as ``compute_integrals`` restricted to the steps whose (oriented)
+    left product is in ``lefts`` (all of them when None), for workloads too large for the
+    dense per-step grids.
+
+    Each prepared left density is convolved on the dense grid exactly as in the reference
+    (8 rounds, CoulombCalculator.cpp:105-163).  ``calculate`` (CoulombCalculator.cpp:165-172)
+    is the sum of V(r) F(r) over the grid; F is zero except at atom cells (Product.cpp:16-30,
+    where a later atom in a shared cell overwrites an earlier one), so the sum is taken over
+    the occupied cells only -- the same terms without the zeros.
+
+    Returns (values, covered): complex values per spec (0 where not covered) and the boolean
+    mask of covered specs.  ``timer`` (optional) receives the seconds spent per prepared left
+    density, for CPU-baseline timing."""
+    import time as _time
+    n = len(states)
+    product_count = n * (n + 1) // 2
+    plan = compute_plan(specs, product_count)
+    if ghat is None:
+        ghat = C.kernel_spectrum(C.kernel_octant(dims, step, dielectric, onsite, tf_lattice), dims)
+    cells = np.asarray(cells, dtype=np.int64)
+    # occupied cells and the atom that ends up in each (the last one in input order)
+    rev = cells[::-1]
+    uniq, first_in_rev = np.unique(rev, return_index=True)
+    owner = (len(cells) - 1 - first_in_rev).astype(np.int64)
+    chosen = None if lefts is None else set(int(v) for v in lefts)
+    values = np.zeros(len(specs), dtype=np.complex128)
+    covered = np.zeros(len(specs), dtype=bool)
+    right_cache = {}
+    # keep every right density while they fit in a few GB, else only the current left's
+    keep_all = 2 * product_count * len(uniq) * 16 < (4 << 30)
+    owned = [None] * n
+    identity = len(owner) == len(cells) and bool(np.all(owner == np.arange(len(cells))))
+
+    def rho_at(prod, conj):
+        key = (prod, conj)
+        if key not in right_cache:
+            fl, fr = product_states(prod)
+            for f in (fl, fr):
+                if owned[f - 1] is None:
+                    owned[f - 1] = states[f - 1] if identity else np.ascontiguousarray(states[f - 1][owner])
+            right_cache[key] = C.pair_density_atoms(owned[fl - 1], owned[fr - 1], conj)
+        return right_cache[key]
+
+    V_at = None
+    last_left = -1
+    t0 = None
+    for (sid, left, right) in plan:
+        if chosen is not None and left[0] not in chosen:
+            continue
+        if left[0] != last_left:
+            if timer is not None and t0 is not None:
+                timer.append(_time.perf_counter() - t0)
+            t0 = _time.perf_counter()
+            if not keep_all:
+                right_cache.clear()
+            F = C.scatter_density(rho_at(left[0], False), uniq, dims)
+            V_at = C.prepare(F, ghat).reshape(-1)[uniq]
+            last_left = left[0]
+        rconj = left[1] != right[1]
+        val = complex(np.sum(V_at * rho_at(right[0], rconj)))
+        values[sid] = np.conj(val) if left[1] else val
+        covered[sid] = True
+    if timer is not None and t0 is not None:
+        timer.append(_time.perf_counter() - t0)
+    return values, covered
+
+
+def plan_lefts(specs, n_inputs):
+    """Oriented left products of the plan, in execution order (Planner.hpp:83-104)."""
+    plan = compute_plan(specs, n_inputs * (n_inputs + 1) // 2)
+    seen = []
+    for (_, left, _) in plan:
+        if not seen or seen[-1] != left[0]:
+            if left[0] not in seen:
+                seen.append(left[0])
+    return seen
+
+
 def format_outputs(specs, values, n_holes, n_electrons):
     """coulombo.cpp:213-262 -> {core: text}.  Hole numbering is reversed."""
     table = {tuple(s): v for s, v in zip(specs, values)}

@@ -11,8 +11,8 @@ from oracle import host as H
 
 pytestmark = pytest.mark.gpu
 
-MODES = [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER]
-TOL = {cl.MODE_FP64_PLAIN: 1e-10, cl.MODE_FP32_FOURIER: 1e-6}
+MODES = [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS]
+TOL = {cl.MODE_FP64_PLAIN: 1e-10, cl.MODE_FP32_ROUNDS: 1e-6}
 # every axis has a non-square split, so the swapped variant differs from the balanced one
 SHAPES = [(96, 128, 40), (160, 72, 48), (48, 80, 96)]
 
@@ -100,7 +100,7 @@ def test_tune_file_persists_choices(tmp_path):
         "from coulombo_lattice_b200 import synth\n"
         "d = synth.build('c1', cells=(10, 12, 8))\n"
         "specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals('****', 4, 2)]\n"
-        "with cl.CoulombCalculator(d['dims'], (synth.A_ZB / 4,) * 3, cl.MODE_FP32_FOURIER) as cc:\n"
+        "with cl.CoulombCalculator(d['dims'], (synth.A_ZB / 4,) * 3, cl.MODE_FP32_ROUNDS) as cc:\n"
         "    cc.initialize(dielectric=10.89)\n"
         "    cc.set_states(d['states'], d['cells_idx'], 2)\n"
         "    v = cc.compute(specs)\n"

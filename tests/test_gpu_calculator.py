@@ -7,9 +7,9 @@ from oracle import coulomb as C
 
 pytestmark = pytest.mark.gpu
 
-MODES = [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER]
+MODES = [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS]
 # plain FP64 path: 1e-10 relative; FP32 transforms with FP64 sums: 1e-6 relative
-TOL = {cl.MODE_FP64_PLAIN: 1e-10, cl.MODE_FP32_FOURIER: 1e-6}
+TOL = {cl.MODE_FP64_PLAIN: 1e-10, cl.MODE_FP32_ROUNDS: 1e-6}
 
 
 def _exp_kernel(dims):

@@ -18,7 +18,7 @@ def _run(d, specs, holes, env=None, monkeypatch=None, profile=False):
         for k, v in env.items():
             monkeypatch.setenv(k, v)
     try:
-        with cl.CoulombCalculator(d["dims"], STEP, cl.MODE_FP32_FOURIER) as cc:
+        with cl.CoulombCalculator(d["dims"], STEP, cl.MODE_FP32_ROUNDS) as cc:
             cc.initialize(dielectric=10.89)
             cc.set_states(d["states"], d["cells_idx"], holes)
             if profile:
@@ -84,7 +84,7 @@ def test_grid_calculate_uses_tensor_core_gram():
     g = C.kernel_octant(dims, (1.0, 1.0, 1.0), 1.0, 0.0)
     V = C.prepare(F, C.kernel_spectrum(g, dims))
     want = C.calculate(V, F2)
-    with cl.CoulombCalculator(dims, (1.0, 1.0, 1.0), cl.MODE_FP32_FOURIER) as cc:
+    with cl.CoulombCalculator(dims, (1.0, 1.0, 1.0), cl.MODE_FP32_ROUNDS) as cc:
         cc.initialize(dielectric=1.0)
         cc.prepare(F)
         got = cc.calculate(F2)
@@ -96,7 +96,7 @@ def test_profile_recorded_inside_graph():
     the graph; each replay adds one request's launches, the same classes as an eager request."""
     d = synth.build("c1", cells=(4, 4, 4))
     specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
-    with cl.CoulombCalculator(d["dims"], STEP, cl.MODE_FP32_FOURIER) as cc:
+    with cl.CoulombCalculator(d["dims"], STEP, cl.MODE_FP32_ROUNDS) as cc:
         cc.initialize(dielectric=10.89)
         cc.set_states(d["states"], d["cells_idx"], 2)
         req = cc.request(specs)

@@ -23,7 +23,7 @@ def gate(got, want, mode):
     return err, lim
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_example_golden(mode):
     import make_example_fixture as fx
     d = fx.load()
@@ -44,7 +44,7 @@ def _oracle_values(d, specs, dielectric=10.89, onsite=0.0, tf=None):
                                         dielectric=dielectric, onsite=onsite, tf_lattice=tf))
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 @pytest.mark.parametrize("pattern", ["****", "eeee,hhhh,ehhe,eheh", "ijji,1*2*"])
 def test_c1_all_patterns(mode, pattern):
     d = synth.build("c1")
@@ -60,7 +60,7 @@ def test_c1_all_patterns(mode, pattern):
     assert np.all(err <= lim), (err / lim).max()
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_medium_structure_eight_states(mode):
     """64^3 grid, 8 states (36 densities), the default four classes."""
     d = synth.build("c3", cells=(16, 16, 16))
@@ -76,7 +76,7 @@ def test_medium_structure_eight_states(mode):
     assert np.all(err <= lim), (err / lim).max()
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_unsorted_atoms_duplicates_onsite_tf(mode):
     """Atom order does not matter; a later atom in the same cell replaces an earlier one
     (F[cell] = value in atom order, Product.cpp:16-30); onsite and Thomas-Fermi kernel."""
@@ -102,7 +102,7 @@ def test_unsorted_atoms_duplicates_onsite_tf(mode):
     assert np.all(err <= lim), (err / lim).max()
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_potentials_match_oracle(mode):
     d = synth.build("c1", cells=(3, 3, 2))
     step = (synth.A_ZB / 4,) * 3
@@ -134,7 +134,7 @@ def test_compute_requires_states_and_kernel():
             cc.set_states(np.ones((1, 2, 1), complex), np.array([0, 512]), 0)
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 @pytest.mark.parametrize("env", [{"CL_XY_PLANE": "0"}, {"CL_NO_REGISTER_FFT": "1"}, {"CL_L2_CHUNK_MB": "4"}])
 def test_pass_variants_agree(mode, env, monkeypatch):
     """The register row/column passes (with the fused plane passes off), the generic passes and
@@ -158,7 +158,7 @@ def test_pass_variants_agree(mode, env, monkeypatch):
     assert np.abs(other - base).max() <= tol * np.abs(base).max()
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_round_split_adds_up(mode):
     """cl_compute_rounds over disjoint round masks (the multi-GPU split) sums to cl_compute,
     and matches the oracle's partial sums over the same rounds."""
@@ -179,7 +179,7 @@ def test_round_split_adds_up(mode):
     assert np.all(err <= np.maximum(lim, 1e-9 * np.abs(full).max()))
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_prepared_requests_and_graph_batch(mode):
     """cl_request runs equal cl_compute; a batch of uneven structures captured as one CUDA
     graph gives every structure's values, on the first (capturing) run and on replays."""
@@ -212,7 +212,7 @@ def test_prepared_requests_and_graph_batch(mode):
         cc.close()
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_round_split_over_more_ranks_than_rounds(mode):
     """With 10 shares of the 8 rounds, the two shares without a round give exact zeros and all
     shares still add up to the full request."""
@@ -231,7 +231,7 @@ def test_round_split_over_more_ranks_than_rounds(mode):
     assert np.abs(sum(parts) - full).max() <= tol * np.abs(full).max()
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_prepared_request_follows_new_coefficients(mode):
     """New coefficients on the same atoms (cl_set_states) are picked up by an existing prepared
     request and by its graph batch."""
@@ -255,7 +255,7 @@ def test_prepared_request_follows_new_coefficients(mode):
         req.close()
 
 
-@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_FOURIER])
+@pytest.mark.parametrize("mode", [cl.MODE_FP64_PLAIN, cl.MODE_FP32_ROUNDS])
 def test_compute_states_overlapped_matches(mode):
     """cl_compute_states (upload overlapped with the transforms, densities grouped by state)
     gives the values of cl_set_states + cl_compute, on a first call and on a repeat with the same
@@ -288,7 +288,7 @@ def test_graph_batch_of_requests_with_different_state_counts():
         d["states"] = d["states"][:n_states, :, :5]
         holes = n_states // 2
         specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", n_states, holes)]
-        cc = cl.CoulombCalculator(d["dims"], step, cl.MODE_FP32_FOURIER)
+        cc = cl.CoulombCalculator(d["dims"], step, cl.MODE_FP32_ROUNDS)
         cc.initialize(dielectric=10.89)
         cc.set_states(d["states"], d["cells_idx"], holes)
         wants.append(cc.compute(specs))

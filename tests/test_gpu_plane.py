@@ -13,7 +13,7 @@ from oracle import host as H
 pytestmark = pytest.mark.gpu
 
 STEP = (synth.A_ZB / 4,) * 3
-FP32, FP64 = cl.MODE_FP32_FOURIER, cl.MODE_FP64_PLAIN
+FP32, FP64 = cl.MODE_FP32_ROUNDS, cl.MODE_FP64_PLAIN
 
 
 def _gate(mode, want):
