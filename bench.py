@@ -41,12 +41,20 @@ WORKLOADS = {
           "orbitals, 4e+4h each, eeee,hhhh,ehhe,eheh (16 x 1024 integrals), one CUDA-graph launch per batch",
 }
 DIELECTRIC = 10.89
-HEADLINE_MODE = 1  # coulombo_lattice_b200.MODE_FP32_ROUNDS
+HEADLINE_MODE = 3  # coulombo_lattice_b200.MODE_FP32_SUBLATTICE
 FORM_TEXT = {
     0: "all-FP64: 8 rounds of N-point FFTs (the reference's method), FP64 Gram",
     1: "FP32 transforms in 8 rounds; FP64 kernel, twiddles, V accumulation and round sum; split-precision "
        "(3xTF32) tensor-core reductions accumulated in FP64",
+    2: "all-FP64 sub-lattice decomposition (exact): per residue class of the atoms' grid points, zero-padded "
+       "(2n/m)^3 transforms and one class-mixing step per frequency; FP64 Gram",
+    3: "sub-lattice decomposition with FP32 transforms; FP64 kernel spectrum, class kernels and phases built in "
+       "FP64 and rounded once; split-precision (3xTF32) tensor-core reductions accumulated in FP64",
 }
+FORM_KEYS = {0: "fp64_rounds", 1: "fp32_rounds", 2: "fp64_sublattice", 3: "fp32_sublattice"}
+# kernel classes bound by HBM (the tensor-core Gram is reported against the tensor rate)
+HBM_CLASSES = ("pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram_split", "round_sum")
+TRANSFORM_CLASSES = ("x_forward", "y_pass", "z_pass", "x_inverse")
 
 
 def parse_args():
@@ -447,29 +455,49 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    # all-FP64 plain path: accuracy reference and the 1x point of the FP32/FP64 ratio
-    plain = cl.CoulombCalculator(d["dims"], d["step"], cl.MODE_FP64_PLAIN)
-    plain.initialize(dielectric=DIELECTRIC)
-    plain.set_states(d["states"], d["cells_idx"], d["holes"])
-    v64 = plain.compute(specs)
-    # timed like the FP32 form: graph replays of the prepared request (best of 3)
-    preq = plain.request(specs)
-    pgraph64 = cl.Batch([preq])
-    pgraph64.run()
-    plain_ms = []
-    for _ in range(3):
-        pgraph64.run()
-        plain_ms.append(pgraph64.last_ms())
-    pgraph64.close()
-    preq.close()
-    plain.close()
-    plain_ms = max_over_ranks(min(plain_ms))
+    def time_form(mode):
+        """Values and device ms per request (graph replay of the prepared request, best of 3)."""
+        cc = cl.CoulombCalculator(d["dims"], d["step"], mode)
+        cc.initialize(dielectric=DIELECTRIC)
+        cc.set_states(d["states"], d["cells_idx"], d["holes"])
+        vals = cc.compute(specs)
+        r = cc.request(specs)
+        g = cl.Batch([r])
+        g.run()
+        ms = []
+        for _ in range(3):
+            g.run()
+            ms.append(g.last_ms())
+        info = cc.form_info()
+        g.close()
+        r.close()
+        cc.close()
+        return vals, max_over_ranks(min(ms)), info
+
+    # the all-FP64 8-round path: accuracy reference and the 1x point of the FP32/FP64 ratio; the
+    # other forms timed alike, to separate what the decomposition and the precision each give
+    v64, plain_ms, _ = time_form(cl.MODE_FP64_PLAIN)
+    other_forms = {}
+    for mode in cl.ALL_MODES:
+        if mode in (cl.MODE_FP64_PLAIN, HEADLINE_MODE):
+            continue
+        vals, ms, info = time_form(mode)
+        err = np.abs(vals - v64)
+        if cl.mode_is_fp64(mode):
+            lim = 1e-10 * np.abs(v64) + 1e-16
+        else:
+            lim = np.maximum(1e-6 * np.abs(v64), 1e-9)
+        other_forms[FORM_KEYS[mode]] = {"ms_per_step": ms, "value": world * n_int / (ms / 1e3),
+                                        "speedup_vs_fp64_rounds": plain_ms / ms,
+                                        "worst_err_over_gate_vs_fp64_rounds": float((err / lim).max()),
+                                        "sublattice": info["sublattice"], "form": FORM_TEXT[mode]}
 
     calc = cl.CoulombCalculator(d["dims"], d["step"], HEADLINE_MODE)
     t0 = time.perf_counter()
     calc.initialize(dielectric=DIELECTRIC)
     init_ms = 1e3 * (time.perf_counter() - t0)
     calc.set_states(d["states"], d["cells_idx"], d["holes"])
+    form_info = calc.form_info()
     for _ in range(max(3, args.warmup)):
         v32 = calc.compute(specs)
 
@@ -564,12 +592,14 @@ def run_ours(args):
 
     # ---- roofline of the dominant kernel --------------------------------------------------
     peak, peak_kind = measured_peaks()
-    fft_classes = {k: v for k, v in prof.items() if k in ("x_forward", "y_pass", "z_pass", "x_inverse")}
-    dom = max(fft_classes, key=lambda k: fft_classes[k][0])
-    ms_k, launches_k, bytes_k = fft_classes[dom]
+    fft_classes = {k: v for k, v in prof.items() if k in TRANSFORM_CLASSES}
+    hbm_classes = {k: v for k, v in prof.items() if k in HBM_CLASSES}
+    dom = max(hbm_classes, key=lambda k: hbm_classes[k][0])
+    ms_k, launches_k, bytes_k = hbm_classes[dom]
     achieved = bytes_k / (ms_k / 1e3) / 1e9
     traffic = profiled_traffic(args.config, dom)
     fft_ms = sum(v[0] for v in fft_classes.values())
+    fft_alg_bytes = sum(v[2] for v in fft_classes.values())
     # FFT HBM-roofline %: sum of 2*M*s bytes over every 3D transform (8 forward + 8 inverse
     # per prepared density) / time of all transform passes / peak.
     M = int(np.prod(d["dims"]))
@@ -588,8 +618,12 @@ def run_ours(args):
                    "peak": tf32_peak, "unit": "TFLOP/s", "frac": flops / (g_ms / 1e3) / 1e12 / tf32_peak,
                    "peak_source": "measured BF16 burst / 2 (TF32 rate)",
                    "flops_per_launch": flops / g_launches, "avg_launch_ms": g_ms / g_launches}
-    fft_bytes = args.steps * 16 * n_prepared * 2.0 * M * 8
-    buf_mb = n_prepared * M * 8 / 1e6
+    if form_info["sublattice"]:
+        pts = form_info["classes"] * form_info["lengths"][0] * form_info["lengths"][1] * (
+            form_info["lengths"][2] // 2)
+        buf_mb = n_prepared * pts * 8 / 1e6
+    else:
+        buf_mb = n_prepared * M * 8 / 1e6
     total_launches = sum(v[1] for v in prof.values())
 
     line = {
@@ -597,7 +631,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_of(args, n_int),
-        "details": {"form": FORM_TEXT[HEADLINE_MODE],
+        "details": {"form": FORM_TEXT[HEADLINE_MODE], "form_info": form_info,
                     "l2": "inputs larger than L2 (126 MB): %.0f MB of transformed grids per request, "
                           "streamed in chunks" % buf_mb, "prepared_densities": n_prepared,
                     "init_ms_kernel_build": init_ms, "wall_ms_per_step": wall_ms / args.steps,
@@ -609,6 +643,7 @@ def run_ours(args):
                        "form": FORM_TEXT[cl.MODE_FP64_PLAIN],
                        "timing": "device time of a CUDA-graph replay of the prepared request, best of 3",
                        "speedup_of_fp32_form": plain_ms / ms_per_step},
+        "other_forms": other_forms,
         "e2e": {"value": world * n_int / (e2e_ms / 1e3), "unit": "integrals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms,
                 "call": "cl_compute_states from pinned host buffers (coefficient upload overlapped with the "
@@ -626,11 +661,13 @@ def run_ours(args):
         "kernels": {k: {"ms": v[0] / args.steps, "launches": v[1] // args.steps,
                         "GBps": (v[2] / (v[0] / 1e3) / 1e9) if v[0] > 0 else None} for k, v in prof.items()},
         "fft_share_of_step": fft_ms / (dev_ms if world == 1 else fft_ms + 1e-30),
-        "fft_hbm_roofline": {"frac": fft_bytes / (fft_ms / 1e3) / 1e9 / peak,
-                             "transforms_per_density": 16, "bytes_per_transform": "2*M*8 (FP32 complex)"},
+        "fft_hbm_roofline": {"frac": fft_alg_bytes / (fft_ms / 1e3) / 1e9 / peak,
+                             "achieved_GBps": fft_alg_bytes / (fft_ms / 1e3) / 1e9,
+                             "definition": "algorithmic bytes of every transform-pass launch (x, y, z passes) / "
+                                           "their summed device time / measured HBM peak"},
         "gram_tensor_roofline": gram_tc,
         "autotune": [ln for ln in cl.autotune_report().splitlines()
-                     if "fp32 %dx%dx%d:" % tuple(d["dims"]) in ln],
+                     if ln.split(":")[0].split(" ", 1)[1].startswith("fp32")],
         "gpu_launches": int(total_launches),
         "clocks": clock_info,
     }

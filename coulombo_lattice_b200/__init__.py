@@ -25,12 +25,16 @@ BIN_DIR = os.path.join(_HERE, "bin")
 MODE_FP64_PLAIN = 0   # all-FP64, 8 rounds of N-point transforms (the reference's method)
 MODE_FP32_ROUNDS = 1  # FP32 transforms, FP64 kernel/twiddles/round sum/reductions, 8 rounds
 MODE_FP32_FOURIER = MODE_FP32_ROUNDS  # former name of MODE_FP32_ROUNDS
-ALL_MODES = [MODE_FP64_PLAIN, MODE_FP32_ROUNDS]
+MODE_FP64_SUBLATTICE = 2  # all-FP64, per residue class of the atoms' grid points (exact decomposition)
+MODE_FP32_SUBLATTICE = 3  # the same with FP32 transforms, FP64-built class kernels and reductions
+ALL_MODES = [MODE_FP64_PLAIN, MODE_FP32_ROUNDS, MODE_FP64_SUBLATTICE, MODE_FP32_SUBLATTICE]
+MODE_NAMES = {MODE_FP64_PLAIN: "fp64 rounds", MODE_FP32_ROUNDS: "fp32 rounds",
+              MODE_FP64_SUBLATTICE: "fp64 sub-lattice", MODE_FP32_SUBLATTICE: "fp32 sub-lattice"}
 
 
 def mode_is_fp64(mode):
     """True for the all-FP64 forms (parity gate 1e-10 relative)."""
-    return mode in (MODE_FP64_PLAIN,)
+    return mode in (MODE_FP64_PLAIN, MODE_FP64_SUBLATTICE)
 
 # kernel classes of cl_kernel_profile (include/coulombo_lattice.h CL_KCLASS_*)
 KERNEL_CLASSES = ["pair_density", "x_forward", "y_pass", "z_pass", "x_inverse", "gram", "kernel_build", "gram_split",
@@ -68,6 +72,7 @@ SIGNATURES = [
     ("cl_compute_states", _i, [_vp, _i, _i, _i64, _i, _P(_d), _P(_i64), _i64, _P(ctypes.c_int16), _P(_d)]),
     ("cl_potentials", _i, [_vp, _P(_d)]),
     ("cl_last_timings", _i, [_vp, _P(_d)]),
+    ("cl_form_info", _i, [_vp, _P(_i)]),
     ("cl_autotune_report", _i, [ctypes.c_char_p, _i64, _P(_i64)]),
     ("cl_compute_rounds", _i, [_vp, _i64, _P(ctypes.c_int16), _i, _P(_d)]),
     ("cl_set_profiling", _i, [_vp, _i]),
@@ -332,6 +337,13 @@ class CoulombCalculator:
         out = np.zeros((self.n_states, self.n_atoms))
         _check(lib().cl_potentials(self._h, _ptr(out)))
         return out
+
+    def form_info(self):
+        """cl_form_info: which decomposition the loaded states run (sub-lattice or 8 rounds)."""
+        info = (ctypes.c_int * 8)()
+        _check(lib().cl_form_info(self._h, info))
+        return dict(sublattice=bool(info[0]), m=info[1], classes=info[2], zincblende=bool(info[3]),
+                    lengths=(info[4], info[5], info[6]), class_kernels=info[7])
 
     def timings(self):
         t = np.zeros(4)

@@ -24,6 +24,7 @@
 #include "kernels.cuh"
 #include "passes.hpp"
 #include "gram_tc.cuh"
+#include "sublattice.cuh"
 
 using clk::cx;
 using clk::FftPlan;
@@ -236,9 +237,32 @@ void ensure_smem(K kernel, size_t bytes) {
 // ---------------------------------------------------------------------------------------
 // The context
 // ---------------------------------------------------------------------------------------
+// State of the sub-lattice decomposition (sublattice.cuh) for the loaded structure.
+struct Sublattice {
+    bool active = false;  // the request paths use the decomposition (a sub-lattice mode whose structure qualifies)
+    bool zb = false;      // the classes are the zinc-blende set: compiled mixing table, canonical class order
+    int m = 0, S = 0;
+    int off[clk::kSlMaxClasses][3] = {};  // offset (x, y, z) of each class, in the order used on the GPU
+    int sub[3] = {0, 0, 0};               // sub-grid points per axis, n/m
+    int pad[3] = {0, 0, 0};               // transform length per axis, 2n/m
+    int vn[3] = {0, 0, 0};                // virtual grid of the x and y passes: (pad x, pad y, S * sub z)
+    long long vM = 0;
+    clk::SlTable table;
+    Axis ax[3];                           // plans and twiddles of the transform lengths
+    DevBuf<cx<double>> H64, phxy64, phz64;
+    DevBuf<cx<float>> H32, phxy32, phz32;
+    long long tables_version = -1;        // kernel version the tables were built from
+};
+
 struct cl_ctx {
     int device = 0;
     int mode = CL_MODE_FP64_PLAIN;
+    Sublattice sl;
+    long long kernel_version = 0;  // bumped at every kernel build
+    // grid the register passes run on (the real grid, or the sub-lattice virtual grid), the key
+    // of the autotuner's choices
+    int tune_dims[3] = {0, 0, 0};
+    int tune_form = 0;  // 2 on the virtual grid
     int n[3] = {0, 0, 0};
     long long M = 0;
     double step[3] = {1, 1, 1};
@@ -312,6 +336,12 @@ struct cl_ctx {
 
 namespace {
 
+// Precision of a form: the all-FP64 forms against the FP32-transform forms.
+bool fp64_form(const cl_ctx* c) { return c->mode == CL_MODE_FP64_PLAIN || c->mode == CL_MODE_FP64_SUBLATTICE; }
+bool sublattice_mode(const cl_ctx* c) {
+    return c->mode == CL_MODE_FP64_SUBLATTICE || c->mode == CL_MODE_FP32_SUBLATTICE;
+}
+
 size_t free_device_bytes() {
     size_t fr = 0, tot = 0;
     CL_CUDA(cudaMemGetInfo(&fr, &tot));
@@ -375,7 +405,7 @@ void build_khat(cl_ctx* c) {
     const double denom = (double)((unsigned long long)c->M * 8ull);
     for (int r = 0; r < 8; ++r) {
         const int kx = r & 1, ky = (r >> 1) & 1, kz = (r >> 2) & 1;
-        if (c->mode == CL_MODE_FP64_PLAIN) {
+        if (fp64_form(c)) {
             c->khat64[r].alloc(c->M);
             clk::k_khat<double><<<grid_for(c->M), 256, 0, c->stream>>>(c->ghat.p, nx, ny, nz, kx, ky, kz, denom,
                                                                        c->khat64[r].p);
@@ -422,6 +452,7 @@ void transform_kernel(cl_ctx* c) {
     build_khat(c);
     CL_CUDA(cudaStreamSynchronize(c->stream));
     c->kernel_ready = true;
+    ++c->kernel_version;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -444,6 +475,12 @@ struct TuneEntry {
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;
+
+// Key of a pass on the grid the context's passes currently run on; fp32 carries the form: bit 0
+// FP32 transforms, bit 1 the sub-lattice virtual grid.
+TuneKey tune_key(const cl_ctx* c, int pass, bool fp32) {
+    return TuneKey{pass, (fp32 ? 1 : 0) | c->tune_form, c->tune_dims[0], c->tune_dims[1], c->tune_dims[2]};
+}
 bool g_tune_loaded = false;
 
 // CL_TUNE_FILE: choices persist across processes.  Lines "pass fp32 nx ny nz split half pad";
@@ -495,7 +532,7 @@ clp::Variant tuned_variant(const cl_ctx* c, int pass, bool fp32) {
     }
     std::lock_guard<std::mutex> g(g_tune_mu);
     tune_load_locked();
-    auto it = g_tune.find(TuneKey{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]});
+    auto it = g_tune.find(tune_key(c, pass, fp32));
     return it == g_tune.end() ? clp::Variant{} : it->second.v;
 }
 
@@ -510,7 +547,7 @@ bool stream_capturing(cudaStream_t s) {
 // each with the default and (FP32) the half lines per block; the default is tried first.
 template <typename F>
 void tune_pass(cl_ctx* c, int pass, bool fp32, int len, F&& launch) {
-    const TuneKey key{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]};
+    const TuneKey key = tune_key(c, pass, fp32);
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         tune_load_locked();
@@ -559,7 +596,7 @@ void tune_pass(cl_ctx* c, int pass, bool fp32, int len, F&& launch) {
 // tuned separate passes' times on the same sample.
 template <typename F>
 void tune_plane(cl_ctx* c, int pass, bool fp32, double sep_ms, F&& launch) {
-    const TuneKey key{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]};
+    const TuneKey key = tune_key(c, pass, fp32);
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         tune_load_locked();
@@ -591,7 +628,7 @@ void tune_plane(cl_ctx* c, int pass, bool fp32, double sep_ms, F&& launch) {
 
 double tuned_ms(const cl_ctx* c, int pass, bool fp32) {
     std::lock_guard<std::mutex> g(g_tune_mu);
-    auto it = g_tune.find(TuneKey{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]});
+    auto it = g_tune.find(tune_key(c, pass, fp32));
     return it == g_tune.end() ? 0.0 : it->second.ms;
 }
 
@@ -604,7 +641,7 @@ bool use_plane(const cl_ctx* c, int pass, bool fp32, bool supported) {
     if (std::getenv("CL_TUNE_FORCE")) return false;
     std::lock_guard<std::mutex> g(g_tune_mu);
     tune_load_locked();
-    auto it = g_tune.find(TuneKey{pass, fp32 ? 1 : 0, c->n[0], c->n[1], c->n[2]});
+    auto it = g_tune.find(tune_key(c, pass, fp32));
     return it == g_tune.end() ? true : it->second.v.split != 0;
 }
 
@@ -624,6 +661,8 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
     const int nrows = ny * nz;
     const long long nxy = (long long)nx * ny;
     const size_t grid_bytes = sizeof(cx<T>) * (size_t)c->M;
+    for (int d = 0; d < 3; ++d) c->tune_dims[d] = c->n[d];
+    c->tune_form = 0;
     // Densities per chunk.  When a few grids fit in L2, chunks are sized so that the passes of
     // one round hand their output to the next pass through L2; otherwise chunks are as large
     // as 60% of the free memory allows (fewer, larger launches and Khat reuse in the z pass).
@@ -796,14 +835,14 @@ void run_rounds(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, const
 
 // Pair densities are complex128 in the plain form and complex64 in the FP32 form (rounded
 // once from their FP64 sums); buffers are addressed in elements of the form's type.
-size_t rho_bytes(const cl_ctx* c) { return c->mode == CL_MODE_FP64_PLAIN ? sizeof(cx<double>) : sizeof(cx<float>); }
+size_t rho_bytes(const cl_ctx* c) { return fp64_form(c) ? sizeof(cx<double>) : sizeof(cx<float>); }
 void* rho_at(const cl_ctx* c, void* base, long long elems) {
     return static_cast<unsigned char*>(base) + elems * (long long)rho_bytes(c);
 }
 
 void run_rounds_mode(cl_ctx* c, const void* rho, long long rho_stride, int np, const int* row_ptr, const int* cell,
                      cx<double>* V, long long v_stride, int round_mask = 0xFF) {
-    if (c->mode == CL_MODE_FP64_PLAIN)
+    if (fp64_form(c))
         run_rounds<double>(c, static_cast<const cx<double>*>(rho), rho_stride, np, row_ptr, cell, V, v_stride,
                            round_mask);
     else
@@ -811,10 +850,259 @@ void run_rounds_mode(cl_ctx* c, const void* rho, long long rho_stride, int np, c
                           round_mask);
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Sub-lattice decomposition (sublattice.cuh)
+// ---------------------------------------------------------------------------------------
+
+// Plans and twiddles of the transform lengths, the class kernels H (from the kernel spectrum in
+// c->ghat) and the class phases, built once per kernel and class set.  Not during a capture.
+void ensure_sl_tables(cl_ctx* c) {
+    Sublattice& sl = c->sl;
+    if (sl.tables_version == c->kernel_version) return;
+    if (stream_capturing(c->stream))
+        cl::fail(CL_ERR_STATE, "the sub-lattice tables must be built by an eager call before a capture");
+    const bool fp32 = !fp64_form(c);
+    for (int d = 0; d < 3; ++d) {
+        Axis& A = sl.ax[d];
+        A.plan = make_plan(sl.pad[d]);
+        auto t64 = twiddles64(sl.pad[d]);
+        std::vector<cx<float>> t32(t64.size());
+        for (size_t i = 0; i < t64.size(); ++i) t32[i] = cx<float>{(float)t64[i].re, (float)t64[i].im};
+        A.tw64.upload(t64.data(), t64.size(), c->stream);
+        A.tw32.upload(t32.data(), t32.size(), c->stream);
+    }
+    const int px = sl.pad[0], py = sl.pad[1], pz = sl.pad[2];
+    const long long nxy = (long long)px * py, nq = nxy * pz;
+    // class kernels H_r(q): the residue representatives and the m-th roots of unity
+    clk::SlRes res{};
+    res.nh = sl.table.nh;
+    res.m = sl.m;
+    for (int h = 0; h < res.nh; ++h)
+        for (int d = 0; d < 3; ++d) res.rep[h][d] = sl.table.rep[h][d];
+    for (int e = 0; e < 4; ++e) {  // exact: m is 2 or 4
+        const int q = (sl.m == 4) ? e : 2 * e;  // quarter turns
+        static const double cq[4] = {1.0, 0.0, -1.0, 0.0}, sq[4] = {0.0, 1.0, 0.0, -1.0};
+        res.wc[e] = cq[q & 3];
+        res.ws[e] = sq[q & 3];
+    }
+    const double denom = (double)((unsigned long long)c->M * 8ull);
+    const int blocks = grid_for(nq);
+    if (fp32) {
+        sl.H32.alloc((size_t)res.nh * nq);
+        clk::k_sl_build_h<float><<<blocks, 256, 0, c->stream>>>(c->ghat.p, c->n[0], c->n[1], c->n[2], px, py, pz, res,
+                                                                denom, sl.H32.p);
+    } else {
+        sl.H64.alloc((size_t)res.nh * nq);
+        clk::k_sl_build_h<double><<<blocks, 256, 0, c->stream>>>(c->ghat.p, c->n[0], c->n[1], c->n[2], px, py, pz,
+                                                                 res, denom, sl.H64.p);
+    }
+    CL_LAUNCHED();
+    // phases: phxy[s][ky][kx] = exp(-i pi (kx bx/nx + ky by/ny)), phz[b][kz] = exp(-i pi kz b/nz) (b < m;
+    // rows up to 4), in extended precision and rounded once
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<cx<double>> phxy((size_t)sl.S * nxy), phz((size_t)4 * pz, cx<double>{0.0, 0.0});
+    for (int s2 = 0; s2 < sl.S; ++s2)
+        for (int ky = 0; ky < py; ++ky)
+            for (int kx = 0; kx < px; ++kx) {
+                const long double a = -pi * ((long double)kx * sl.off[s2][0] / c->n[0] +
+                                             (long double)ky * sl.off[s2][1] / c->n[1]);
+                phxy[(size_t)s2 * nxy + (size_t)ky * px + kx] = cx<double>{(double)std::cos(a), (double)std::sin(a)};
+            }
+    for (int b = 0; b < sl.m; ++b)
+        for (int kz = 0; kz < pz; ++kz) {
+            const long double a = -pi * (long double)kz * b / c->n[2];
+            phz[(size_t)b * pz + kz] = cx<double>{(double)std::cos(a), (double)std::sin(a)};
+        }
+    if (fp32) {
+        std::vector<cx<float>> f1(phxy.size()), f2(phz.size());
+        for (size_t i = 0; i < phxy.size(); ++i) f1[i] = cx<float>{(float)phxy[i].re, (float)phxy[i].im};
+        for (size_t i = 0; i < phz.size(); ++i) f2[i] = cx<float>{(float)phz[i].re, (float)phz[i].im};
+        sl.phxy32.upload(f1.data(), f1.size(), c->stream);
+        sl.phz32.upload(f2.data(), f2.size(), c->stream);
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+    } else {
+        sl.phxy64.upload(phxy.data(), phxy.size(), c->stream);
+        sl.phz64.upload(phz.data(), phz.size(), c->stream);
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    sl.tables_version = c->kernel_version;
+}
+
+// One request's transforms in the sub-lattice form: for every density p in [0, np), V[p] at the
+// atoms (virtual-grid order).  Per chunk of densities: x and y forward passes on the virtual
+// grid (fused plane pass where compiled and faster), the z pass with class mixing, the y and x
+// inverse passes writing the values at the atoms; in the FP32 form they are widened to V.
+template <typename T>
+void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, cx<double>* V, long long v_stride) {
+    ensure_sl_tables(c);
+    const Sublattice& sl = c->sl;
+    const int nx = sl.vn[0], ny = sl.vn[1], nz = sl.vn[2];
+    const int nrows = ny * nz;
+    const long long nxy = (long long)nx * ny;
+    const long long vM = sl.vM;
+    const size_t grid_bytes = sizeof(cx<T>) * (size_t)vM;
+    const bool fp32 = sizeof(T) == 4;
+    for (int d = 0; d < 3; ++d) c->tune_dims[d] = sl.vn[d];
+    c->tune_form = 2;
+    const int* row_ptr = c->row_ptr.p;
+    const int* cell = c->cell_sorted.p;
+    const long long n_at = c->n_sorted;
+    // values at the atoms: straight into V in FP64; through the rounds buffer in FP32
+    const size_t at_bytes = fp32 ? sizeof(cx<T>) * (size_t)n_at : 0;
+    size_t budget = (size_t)(0.6 * (double)(free_device_bytes() + c->work.n + c->rounds.n));
+    int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(np, 1), budget / (grid_bytes + at_bytes)));
+    c->work.alloc(std::max(c->work.n, (size_t)chunk * grid_bytes));
+    if (fp32) c->rounds.alloc(std::max(c->rounds.n, (size_t)chunk * at_bytes));
+    cx<T>* buf = reinterpret_cast<cx<T>*>(c->work.p);
+    cx<T>* tr = reinterpret_cast<cx<T>*>(c->rounds.p);
+    const cx<T>* twx = fp32 ? (const cx<T>*)sl.ax[0].tw32.p : (const cx<T>*)sl.ax[0].tw64.p;
+    const cx<T>* twy = fp32 ? (const cx<T>*)sl.ax[1].tw32.p : (const cx<T>*)sl.ax[1].tw64.p;
+    const cx<T>* twz = fp32 ? (const cx<T>*)sl.ax[2].tw32.p : (const cx<T>*)sl.ax[2].tw64.p;
+    const cx<T>* H = fp32 ? (const cx<T>*)sl.H32.p : (const cx<T>*)sl.H64.p;
+    const cx<T>* phxy = fp32 ? (const cx<T>*)sl.phxy32.p : (const cx<T>*)sl.phxy64.p;
+    const cx<T>* phz = fp32 ? (const cx<T>*)sl.phz32.p : (const cx<T>*)sl.phz64.p;
+    clk::SlMix mix{};
+    mix.S = sl.S;
+    for (int s2 = 0; s2 < clk::kSlMaxClasses; ++s2) mix.offz[s2] = s2 < sl.S ? sl.off[s2][2] : 0;
+    for (int i = 0; i < clk::kSlMaxClasses * clk::kSlMaxClasses; ++i) {
+        mix.h[i] = sl.table.h[i];
+        mix.cj[i] = sl.table.cj[i];
+    }
+    const XTile xt = x_tile<T>(nx, nrows);
+    const LTile yt = l_tile<T>(ny, false);
+    ensure_smem(clk::k_xfwd<T>, xt.smem);
+    ensure_smem(clk::k_xinv<T>, xt.smem);
+    ensure_smem(clk::k_ypass<-1, T>, yt.smem);
+    ensure_smem(clk::k_ypass<+1, T>, yt.smem);
+    const int xblocks = (nrows + xt.rows - 1) / xt.rows;
+    const int ychunks = (nx + yt.W - 1) / yt.W;
+    const bool reg_x = register_passes_enabled() && clp::split_variants(nx) > 0;
+    const bool reg_y = register_passes_enabled() && clp::split_variants(ny) > 0;
+    const int skip_empty = (reg_x && reg_y && !std::getenv("CL_NO_ROW_SKIP")) ? 1 : 0;
+    const bool plane_ok = reg_x && reg_y && clp::plane_supported(fp32, nx, ny);
+    // no phase in any pass: the rounds' phase tables are never read with kappa = 0
+    const clk::RoundPhase rp0{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
+    cx<T>* out0 = fp32 ? tr : reinterpret_cast<cx<T>*>(V);
+    const long long out_stride = fp32 ? n_at : v_stride;
+    if (autotune_enabled() && !std::getenv("CL_TUNE_FORCE") && np > 0 && !stream_capturing(c->stream)) {
+        const int cnt_t = (int)std::max<size_t>(1, std::min<size_t>((size_t)chunk, (512ull << 20) / grid_bytes));
+        const int* rp_skip = skip_empty ? row_ptr : nullptr;
+        if (reg_x)
+            tune_pass(c, clp::kXFwd, fp32, nx, [&](clp::Variant v) {
+                clp::xfwd<T>(c->stream, v, rho, rho_stride, row_ptr, cell, buf, vM, twx, rp0, nx, ny, nrows, cnt_t,
+                             skip_empty);
+            });
+        if (reg_y) {
+            tune_pass(c, clp::kYFwd, fp32, ny, [&](clp::Variant v) {
+                clp::ycol<-1, T>(c->stream, v, buf, vM, twy, nx, ny, nz, cnt_t, rp_skip);
+            });
+            tune_pass(c, clp::kYInv, fp32, ny, [&](clp::Variant v) {
+                clp::ycol<+1, T>(c->stream, v, buf, vM, twy, nx, ny, nz, cnt_t, rp_skip);
+            });
+        }
+        if (reg_x)
+            tune_pass(c, clp::kXInv, fp32, nx, [&](clp::Variant v) {
+                clp::xinv<T>(c->stream, v, buf, vM, twx, row_ptr, cell, out0, out_stride, nx, nrows, cnt_t);
+            });
+        if (plane_ok && !std::getenv("CL_XY_PLANE")) {
+            tune_plane(c, clp::kXYFwd, fp32, tuned_ms(c, clp::kXFwd, fp32) + tuned_ms(c, clp::kYFwd, fp32), [&] {
+                clp::xyfwd<T>(c->stream, rho, rho_stride, row_ptr, cell, buf, vM, twx, rp0, nx, ny, nz, cnt_t);
+            });
+            tune_plane(c, clp::kXYInv, fp32, tuned_ms(c, clp::kYInv, fp32) + tuned_ms(c, clp::kXInv, fp32), [&] {
+                clp::xyinv<T>(c->stream, buf, vM, twx, row_ptr, cell, out0, out_stride, nx, ny, nz, cnt_t);
+            });
+        }
+    }
+    const bool xy_fwd = use_plane(c, clp::kXYFwd, fp32, plane_ok);
+    const bool xy_inv = use_plane(c, clp::kXYInv, fp32, plane_ok);
+    const clp::Variant v_xf = tuned_variant(c, clp::kXFwd, fp32), v_yf = tuned_variant(c, clp::kYFwd, fp32),
+                       v_yi = tuned_variant(c, clp::kYInv, fp32), v_xi = tuned_variant(c, clp::kXInv, fp32);
+    const double gbytes = (double)grid_bytes;
+    const double atoms = (double)n_at;
+    const double live = skip_empty ? (double)c->live_rows / nrows : 1.0;
+    const double row_side = (double)c->live_rows / nrows;
+    const double h_bytes = (double)sl.table.nh * sl.pad[2] * nxy * sizeof(cx<T>);
+    for (int p0 = 0; p0 < np; p0 += chunk) {
+        const int cnt = std::min(chunk, np - p0);
+        const cx<T>* rho_c = rho + (long long)p0 * rho_stride;
+        cx<T>* out_c = fp32 ? tr : reinterpret_cast<cx<T>*>(V + (long long)p0 * v_stride);
+        cudaEvent_t e = prof_begin(c);
+        if (xy_fwd) {
+            clp::xyfwd<T>(c->stream, rho_c, rho_stride, row_ptr, cell, buf, vM, twx, rp0, nx, ny, nz, cnt);
+        } else if (!(reg_x && clp::xfwd<T>(c->stream, v_xf, rho_c, rho_stride, row_ptr, cell, buf, vM, twx, rp0, nx,
+                                            ny, nrows, cnt, skip_empty))) {
+            clk::k_xfwd<T><<<xblocks, 256, xt.smem, c->stream>>>(rho_c, rho_stride, row_ptr, cell, buf, vM,
+                                                                 sl.ax[0].plan, twx, rp0, nx, ny, nrows, xt.rows,
+                                                                 xt.ld, cnt);
+        }
+        CL_LAUNCHED();
+        prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * (double)sizeof(cx<T>) + (xy_fwd ? 1.0 : live) * gbytes) +
+                                           atoms * 4.0);
+        if (!xy_fwd) {
+            e = prof_begin(c);
+            if (!(reg_y && clp::ycol<-1, T>(c->stream, v_yf, buf, vM, twy, nx, ny, nz, cnt,
+                                             skip_empty ? row_ptr : nullptr)))
+                clk::k_ypass<-1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, vM, sl.ax[1].plan, twy,
+                                                                                          nx, ny, yt.W, ychunks);
+            CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_YPASS, cnt * (1.0 + live) * gbytes);
+        }
+        e = prof_begin(c);
+        if (!clp::zmix<T>(c->stream, buf, vM, twz, H, phxy, phz, mix, sl.zb, nxy, sl.pad[2], cnt))
+            cl::fail(CL_ERR_UNSUPPORTED, "no sub-lattice z pass for %d points", sl.pad[2]);
+        CL_LAUNCHED();
+        prof_end(c, e, CL_KCLASS_ZPASS, cnt * 2.0 * gbytes + h_bytes);
+        if (!xy_inv) {
+            e = prof_begin(c);
+            if (!(reg_y && clp::ycol<+1, T>(c->stream, v_yi, buf, vM, twy, nx, ny, nz, cnt,
+                                             skip_empty ? row_ptr : nullptr)))
+                clk::k_ypass<+1, T><<<dim3(ychunks * nz, cnt), 256, yt.smem, c->stream>>>(buf, vM, sl.ax[1].plan, twy,
+                                                                                          nx, ny, yt.W, ychunks);
+            CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_YPASS, cnt * (1.0 + live) * gbytes);
+        }
+        e = prof_begin(c);
+        if (xy_inv) {
+            clp::xyinv<T>(c->stream, buf, vM, twx, row_ptr, cell, out_c, out_stride, nx, ny, nz, cnt);
+        } else if (!(reg_x && clp::xinv<T>(c->stream, v_xi, buf, vM, twx, row_ptr, cell, out_c, out_stride, nx, nrows,
+                                            cnt))) {
+            clk::k_xinv<T><<<xblocks, 256, xt.smem, c->stream>>>(buf, vM, sl.ax[0].plan, twx, row_ptr, cell, out_c,
+                                                                 out_stride, nx, nrows, xt.rows, xt.ld, cnt);
+        }
+        CL_LAUNCHED();
+        prof_end(c, e, CL_KCLASS_XINV,
+                 cnt * ((xy_inv ? 1.0 : row_side) * gbytes + atoms * (double)sizeof(cx<T>)) + atoms * 4.0);
+        if (fp32) {
+            e = prof_begin(c);
+            clk::k_sl_widen<T><<<dim3((unsigned)std::min<long long>((n_at + 255) / 256, 148LL * 8), cnt), 256, 0,
+                                 c->stream>>>(tr, n_at, V + (long long)p0 * v_stride, v_stride, n_at);
+            CL_LAUNCHED();
+            prof_end(c, e, CL_KCLASS_ROUND_SUM, cnt * atoms * ((double)sizeof(cx<T>) + 16.0));
+        }
+    }
+}
+
+// The transforms of a request on the context's loaded atoms: the sub-lattice decomposition when
+// it is in use, else the 8 rounds (of the rounds in round_mask).
+void run_transforms(cl_ctx* c, const void* rho, long long rho_stride, int np, cx<double>* V, long long v_stride,
+                    int round_mask = 0xFF) {
+    if (c->sl.active) {
+        if ((round_mask & 0xFF) != 0xFF)
+            cl::fail(CL_ERR_UNSUPPORTED, "the sub-lattice form has no rounds to split (use an 8-round form)");
+        if (fp64_form(c))
+            run_sublattice<double>(c, static_cast<const cx<double>*>(rho), rho_stride, np, V, v_stride);
+        else
+            run_sublattice<float>(c, static_cast<const cx<float>*>(rho), rho_stride, np, V, v_stride);
+        return;
+    }
+    run_rounds_mode(c, rho, rho_stride, np, c->row_ptr.p, c->cell_sorted.p, V, v_stride, round_mask);
+}
+
 // ---------------------------------------------------------------------------------------
 // Tensor-core Gram (FP32 form): TF32 split pass + tcgen05 GEMM, see gram_tc.cuh.
 // ---------------------------------------------------------------------------------------
-bool use_tc_gram(const cl_ctx* c) { return c->mode == CL_MODE_FP32_ROUNDS && !std::getenv("CL_NO_TC_GRAM"); }
+bool use_tc_gram(const cl_ctx* c) { return !fp64_form(c) && !std::getenv("CL_NO_TC_GRAM"); }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -1002,10 +1290,12 @@ void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const void
 // device lists and launch shape are set up once (setup synchronises), the launch itself only
 // enqueues (it can be captured in a CUDA graph).
 struct PairSetup {
-    DevBuf<clk::PairSeg> segs;  // products grouped by left state, indices into `states`
+    DevBuf<clk::PairSeg> segs;  // products grouped by left state, indices into `states` (FP64 kernel)
+    DevBuf<clk::PairBlock> pblocks;  // products in 4 x 4 state blocks (FP32 kernel)
     DevBuf<int> states;
     int np = 0, n_segs = 0, n_used = 0, chunk = 1, blocks = 1;
-    size_t smem = 0;
+    int n_pblocks = 0, chunk32 = 1, grid32 = 1;
+    size_t smem = 0, smem32 = 0;
 };
 
 void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
@@ -1033,6 +1323,53 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
         }
     ps.n_segs = (int)segs.size();
     ps.segs.upload(segs.data(), segs.size(), c->stream);
+    // FP32 kernel: the used states in ascending order, in groups of four; every product
+    // (higher state x, lower state y) falls in the block (group of x, group of y)
+    {
+        std::vector<int> order(used.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::sort(order.begin(), order.end(), [&](int a, int b) { return used[a] < used[b]; });
+        std::vector<int> group(used.size()), pos(used.size());
+        for (size_t k = 0; k < order.size(); ++k) {
+            group[order[k]] = (int)(k / 4);
+            pos[order[k]] = (int)(k % 4);
+        }
+        const int ng = ((int)used.size() + 3) / 4;
+        std::vector<int> bidx((size_t)ng * ng, -1);
+        std::vector<clk::PairBlock> pb;
+        for (int p = 0; p < ps.np; ++p) {
+            const int ux = where[fl[p].x], uy = where[fl[p].y];  // rows are conj(c_x) c_y with x >= y
+            if (group[ux] < group[uy]) cl::fail(CL_ERR_STATE, "pair density with its lower state first");
+            const int gx = group[ux], gy = group[uy];
+            int& bi = bidx[(size_t)gx * ng + gy];
+            if (bi < 0) {
+                bi = (int)pb.size();
+                clk::PairBlock b{};
+                for (int k = 0; k < 4; ++k) {
+                    const int kx = std::min<int>(4 * gx + k, (int)used.size() - 1);
+                    const int ky = std::min<int>(4 * gy + k, (int)used.size() - 1);
+                    b.I[k] = order[kx];
+                    b.J[k] = order[ky];
+                }
+                for (int k = 0; k < 16; ++k) b.prod[k] = -1;
+                pb.push_back(b);
+            }
+            pb[bi].prod[pos[ux] * 4 + pos[uy]] = p;
+        }
+        ps.n_pblocks = (int)pb.size();
+        ps.pblocks.upload(pb.data(), pb.size(), c->stream);
+        // chunk: enough (atom, block) items for the block's threads, at most ~56 KB staged
+        const size_t per_atom32 = sizeof(cx<float>) * (size_t)used.size() * c->n_orb;
+        int ch = std::max(8, (clk::PD32_THREADS + ps.n_pblocks - 1) / std::max(1, ps.n_pblocks));
+        while (ch > 8 && per_atom32 * (ch + 1) > 56 * 1024) --ch;
+        while (ch > 1 && per_atom32 * (ch + 1) > 200 * 1024) --ch;
+        ps.chunk32 = ch;
+        ps.smem32 = per_atom32 * (ch + 1);
+        ensure_smem(clk::k_pair_density32, ps.smem32);
+        const long long chunks32 = (c->n_sorted + ch - 1) / ch;
+        const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(16, (200 * 1024) / ps.smem32));
+        ps.grid32 = (int)std::min<long long>(chunks32, 148LL * per_sm);
+    }
     ps.states.upload(used.data(), used.size(), c->stream);
     ps.n_used = (int)used.size();
     // two stages of `chunk` atoms, each up to 48 KB (about two blocks per SM)
@@ -1062,16 +1399,21 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
     // the shared-memory attribute is per kernel, so another setup (of another group or
     // request) may have lowered it since this one was prepared
     cudaEvent_t e = prof_begin(c);
-    if (c->mode == CL_MODE_FP64_PLAIN) {
+    if (fp64_form(c)) {
         ensure_smem(clk::k_pair_density<double>, ps.smem);
         clk::k_pair_density<double><<<ps.blocks, 256, ps.smem, c->stream>>>(
             c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<double>*>(rho));
-    } else {
+    } else if (std::getenv("CL_PAIR_FP64_SUMS")) {  // the FP32 forms with FP64 sums, rounded once
         ensure_smem(clk::k_pair_density<float>, ps.smem);
         clk::k_pair_density<float><<<ps.blocks, 256, ps.smem, c->stream>>>(
             c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<float>*>(rho));
+    } else {
+        ensure_smem(clk::k_pair_density32, ps.smem32);
+        clk::k_pair_density32<<<ps.grid32, clk::PD32_THREADS, ps.smem32, c->stream>>>(
+            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.pblocks.p, ps.n_pblocks,
+            ps.states.p, ps.n_used, ps.chunk32, static_cast<cx<float>*>(rho));
     }
     CL_LAUNCHED();
     prof_end(c, e, CL_KCLASS_DENSITY,
@@ -1125,7 +1467,7 @@ int cl_create(cl_ctx** out, int nx, int ny, int nz, double sx, double sy, double
     int st = cl::guarded([&] {
         if (!out) cl::fail(CL_ERR_ARGUMENT, "null output pointer");
         if (nx <= 0 || ny <= 0 || nz <= 0) cl::fail(CL_ERR_ARGUMENT, "dimensions must be positive");
-        if (mode != CL_MODE_FP64_PLAIN && mode != CL_MODE_FP32_ROUNDS) cl::fail(CL_ERR_ARGUMENT, "unknown mode %d", mode);
+        if (mode < CL_MODE_FP64_PLAIN || mode > CL_MODE_FP32_SUBLATTICE) cl::fail(CL_ERR_ARGUMENT, "unknown mode %d", mode);
         const int dims[3] = {nx, ny, nz};
         for (int d = 0; d < 3; ++d) {
             if (!smooth235(dims[d]))
@@ -1193,7 +1535,7 @@ int cl_set_kernel_coulomb(cl_ctx* c, double dielectric, double onsite, double tf
                                                                      c->step[2], km);
         CL_LAUNCHED();
         transform_kernel(c);
-        prof_end(c, pe, CL_KCLASS_KERNEL, (double)total * 8.0 * 7.0 + (double)c->M * 8.0 * (c->mode ? 4.0 : 8.0));
+        prof_end(c, pe, CL_KCLASS_KERNEL, (double)total * 8.0 * 7.0 + (double)c->M * 8.0 * (fp64_form(c) ? 8.0 : 4.0));
         CL_CUDA(cudaStreamSynchronize(c->stream));
         prof_collect(c);
     });
@@ -1219,7 +1561,7 @@ int cl_prepare_grid(cl_ctx* c, const double* rho) {
         c->grid_rho.upload(reinterpret_cast<const cx<double>*>(rho), c->M, c->stream);
         c->grid_V.alloc(c->M);
         const void* rho_in = c->grid_rho.p;
-        if (c->mode != CL_MODE_FP64_PLAIN) {  // the FP32 form's densities are complex64
+        if (!fp64_form(c)) {  // the FP32 forms' densities are complex64
             c->grid_rho32.alloc(c->M);
             clk::k_narrow<float><<<grid_for(c->M), 256, 0, c->stream>>>(c->grid_rho.p, c->grid_rho32.p, c->M);
             CL_LAUNCHED();
@@ -1274,10 +1616,89 @@ void check_states_args(int n_states, int n_holes, int64_t n_atoms, int n_orb, co
     if (n_atoms >= (1LL << 31)) cl::fail(CL_ERR_UNSUPPORTED, "too many atoms");
 }
 
+// Sub-lattice decomposition for the (deduplicated) atom cells, in the sub-lattice modes: the
+// modulus m in {4, 2} dividing every grid size whose classes need the least transform work,
+// S / m^3 of the 8 rounds' (S occupied classes, each transformed at (2n/m)^3 points), kept when
+// at most half of it, with at most 8 classes and a compiled z-mix length.  Classes go in
+// class-id order, or in the canonical zinc-blende order when they are that set (shifted).
+// CL_NO_SUBLATTICE=1 keeps the 8 rounds.
+void plan_sublattice(cl_ctx* c, const std::vector<int>& cell_s) {
+    Sublattice& sl = c->sl;
+    const int old_m = sl.m, old_S = sl.S;
+    int old_off[clk::kSlMaxClasses][3];
+    std::memcpy(old_off, sl.off, sizeof old_off);
+    sl.active = false;
+    sl.zb = false;
+    if (!sublattice_mode(c) || std::getenv("CL_NO_SUBLATTICE")) return;
+    const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+    double best = 0.5;
+    int best_m = 0;
+    std::vector<int> best_ids;
+    for (int m : {4, 2}) {
+        if (nx % m || ny % m || nz % m) continue;
+        if (!clp::zmix_supported(2 * nz / m)) continue;
+        std::vector<char> seen((size_t)m * m * m, 0);
+        for (int cs : cell_s) {
+            const int x = cs % nx, y = (cs / nx) % ny, z = cs / (nx * ny);
+            seen[((z % m) * m + y % m) * m + x % m] = 1;
+        }
+        std::vector<int> ids;
+        for (int id = 0; id < m * m * m; ++id)
+            if (seen[id]) ids.push_back(id);
+        if (ids.empty() || (int)ids.size() > clk::kSlMaxClasses) continue;
+        const double cost = (double)ids.size() / (double)(m * m * m);
+        if (cost <= best) {
+            best = cost;
+            best_m = m;
+            best_ids = ids;
+        }
+    }
+    if (!best_m) return;
+    const int m = best_m, S = (int)best_ids.size();
+    sl.m = m;
+    sl.S = S;
+    for (int s = 0; s < S; ++s) {
+        sl.off[s][0] = best_ids[s] % m;
+        sl.off[s][1] = (best_ids[s] / m) % m;
+        sl.off[s][2] = best_ids[s] / (m * m);
+    }
+    if (m == 4 && S == 8) {  // the zinc-blende set, shifted by t?
+        for (int t = 0; t < 64 && !sl.zb; ++t) {
+            const int tx = t % 4, ty = (t / 4) % 4, tz = t / 16;
+            int cand[8][3];
+            bool all = true;
+            for (int s = 0; s < 8 && all; ++s) {
+                cand[s][0] = (clk::ZincBlende::off[s][0] + tx) % 4;
+                cand[s][1] = (clk::ZincBlende::off[s][1] + ty) % 4;
+                cand[s][2] = (clk::ZincBlende::off[s][2] + tz) % 4;
+                all = std::binary_search(best_ids.begin(), best_ids.end(),
+                                         (cand[s][2] * 4 + cand[s][1]) * 4 + cand[s][0]);
+            }
+            if (all) {
+                sl.zb = true;
+                std::memcpy(sl.off, cand, sizeof cand);
+            }
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        sl.sub[d] = c->n[d] / m;
+        sl.pad[d] = 2 * c->n[d] / m;
+    }
+    sl.vn[0] = sl.pad[0];
+    sl.vn[1] = sl.pad[1];
+    sl.vn[2] = S * sl.sub[2];
+    sl.vM = (long long)sl.vn[0] * sl.vn[1] * sl.vn[2];
+    sl.table = clk::sl_table(sl.off, S, m);
+    if (m != old_m || S != old_S || std::memcmp(old_off, sl.off, sizeof old_off) != 0) sl.tables_version = -1;
+    sl.active = true;
+}
+
 // Atoms sorted by cell; where several atoms share a cell the one listed last wins, as with
 // F[cell] = value in atom order (Product.cpp:16-30).  Builds the sorted cell list, the input
-// atom of each slot, the row CSR and the live-row count, and uploads them (synchronously).  A
-// list identical to the previous load's is not processed again.
+// atom of each slot, the row CSR and the live-row count, and uploads them (synchronously).  With
+// the sub-lattice decomposition the atoms are then ordered by their cell of the virtual grid
+// (class-stacked sub-grids), which is the order every later pass and reduction uses.  A list
+// identical to the previous load's is not processed again.
 void load_cells(cl_ctx* c, int64_t n_atoms, const int64_t* cells) {
     if ((int64_t)c->cells_seen.size() == n_atoms && c->n_sorted > 0 &&
         std::memcmp(c->cells_seen.data(), cells, sizeof(int64_t) * (size_t)n_atoms) == 0)
@@ -1304,8 +1725,36 @@ void load_cells(cl_ctx* c, int64_t n_atoms, const int64_t* cells) {
         }
         c->atom_slot[a] = (long long)cell_s.size() - 1;
     }
-    const int nx = c->n[0];
-    const int nrows = c->n[1] * c->n[2];
+    plan_sublattice(c, cell_s);
+    int nx = c->n[0];
+    int nrows = c->n[1] * c->n[2];
+    if (c->sl.active) {
+        const Sublattice& sl = c->sl;
+        const int m = sl.m, gx = c->n[0], gy = c->n[1];
+        int cls_of[64];
+        for (int s = 0; s < sl.S; ++s) cls_of[(sl.off[s][2] * m + sl.off[s][1]) * m + sl.off[s][0]] = s;
+        std::vector<int> vcell(cell_s.size()), perm(cell_s.size());
+        for (size_t i = 0; i < cell_s.size(); ++i) {
+            const int cs = cell_s[i];
+            const int x = cs % gx, y = (cs / gx) % gy, z = cs / (gx * gy);
+            const int s = cls_of[((z % m) * m + y % m) * m + x % m];
+            vcell[i] = ((s * sl.sub[2] + z / m) * sl.pad[1] + y / m) * sl.pad[0] + x / m;
+        }
+        std::iota(perm.begin(), perm.end(), 0);
+        std::sort(perm.begin(), perm.end(), [&](int a, int b) { return vcell[a] < vcell[b]; });
+        std::vector<int> new_pos(cell_s.size());
+        std::vector<int> vc(cell_s.size()), vo(cell_s.size());
+        for (size_t k = 0; k < perm.size(); ++k) {
+            new_pos[perm[k]] = (int)k;
+            vc[k] = vcell[perm[k]];
+            vo[k] = orig_s[perm[k]];
+        }
+        for (auto& slot : c->atom_slot) slot = new_pos[slot];
+        cell_s.swap(vc);
+        orig_s.swap(vo);
+        nx = sl.vn[0];
+        nrows = sl.vn[1] * sl.vn[2];
+    }
     std::vector<int> rp((size_t)nrows + 1, 0);
     for (int cs : cell_s) rp[cs / nx + 1]++;
     for (int r = 0; r < nrows; ++r) rp[r + 1] += rp[r];
@@ -1422,7 +1871,7 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
-        run_rounds_mode(c, rho.p, As, nl, c->row_ptr.p, c->cell_sorted.p, V.p, As, round_mask);
+        run_transforms(c, rho.p, As, nl, V.p, As, round_mask);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
         gram(c, V.p, As, nl, rho.p, rho_bytes(c) == sizeof(cx<float>), As, dr.p, nr, As, o4.p);
         CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
@@ -1585,9 +2034,8 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
         upload_through(g->last_state);
         CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[g->last_state], 0));
         pair_launch(c, g->ps, rho_at(c, rho.p, (long long)g->begin * As));
-        run_rounds_mode(c, rho_at(c, rho.p, (long long)g->begin * As), As, g->end - g->begin, c->row_ptr.p,
-                        c->cell_sorted.p,
-                        V.p + (long long)g->begin * As, As);
+        run_transforms(c, rho_at(c, rho.p, (long long)g->begin * As), As, g->end - g->begin,
+                       V.p + (long long)g->begin * As, As);
     }
     upload_through(n_states - 1);
     CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[n_states - 1], 0));
@@ -1676,7 +2124,7 @@ int cl_potentials(cl_ctx* c, double* out) {
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
-        run_rounds_mode(c, rho.p, As, n, c->row_ptr.p, c->cell_sorted.p, V.p, As);
+        run_transforms(c, rho.p, As, n, V.p, As);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
         std::vector<cx<double>> h((size_t)n * As);
         CL_CUDA(cudaMemcpyAsync(h.data(), V.p, h.size() * sizeof(cx<double>), cudaMemcpyDeviceToHost, c->stream));
@@ -1747,7 +2195,7 @@ void request_enqueue(cl_request* r) {
     cl_ctx* c = r->ctx;
     const long long As = c->n_sorted;
     pair_launch(c, r->ps, r->rho.p);
-    run_rounds_mode(c, r->rho.p, As, r->nl, c->row_ptr.p, c->cell_sorted.p, r->V.p, As);
+    run_transforms(c, r->rho.p, As, r->nl, r->V.p, As);
     gram(c, r->V.p, As, r->nl, r->rho.p, rho_bytes(c) == sizeof(cx<float>), As, r->ridx.p, r->nr, As, r->o4.p);
     CL_CUDA(cudaMemcpyAsync(r->o4_host, r->o4.p, sizeof(double) * (4 * (size_t)r->nl * r->nr + 1),
                             cudaMemcpyDeviceToHost, c->stream));
@@ -1937,6 +2385,12 @@ int cl_batch_last_ms(cl_batch* b, double* ms) {
 }
 
 int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
+    // precision and grid of a tuning key: "fp32" / "fp64" on the real grid, "fp32 sub-lattice" /
+    // "fp64 sub-lattice" on the virtual grid of the sub-lattice forms
+    const auto form_name = [](int f) {
+        static const char* n[4] = {"fp64", "fp32", "fp64 sub-lattice", "fp32 sub-lattice"};
+        return n[f & 3];
+    };
     return cl::guarded([&] {
         static const char* names[clp::kNumPasses] = {"x_forward", "y_forward", "z_pass",   "y_inverse",
                                                      "x_inverse", "xy_forward", "xy_inverse"};
@@ -1950,16 +2404,16 @@ int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
                     const char* ch = kv.second.v.split ? "fused plane pass" : "separate passes";
                     if (kv.second.candidates == 0)
                         std::snprintf(line, sizeof line, "%s %s %dx%dx%d: %s, from CL_TUNE_FILE\n", pn,
-                                      kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny, kv.first.nz, ch);
+                                      form_name(kv.first.fp32), kv.first.nx, kv.first.ny, kv.first.nz, ch);
                     else
                         std::snprintf(line, sizeof line,
                                       "%s %s %dx%dx%d: %s, 2 candidates, fused %.4f ms, separate %.4f ms\n", pn,
-                                      kv.first.fp32 ? "fp32" : "fp64", kv.first.nx, kv.first.ny, kv.first.nz, ch,
+                                      form_name(kv.first.fp32), kv.first.nx, kv.first.ny, kv.first.nz, ch,
                                       kv.second.ms, kv.second.ms_default);
                     out += line;
                     continue;
                 }
-                const char* pr = kv.first.fp32 ? "fp32" : "fp64";
+                const char* pr = form_name(kv.first.fp32);
                 const char* sp = kv.second.v.split ? "swapped" : "balanced";
                 const char* ln = kv.second.v.half ? "half" : "default";
                 const char* pd = kv.second.v.pad ? ", padded tile" : "";
@@ -1980,6 +2434,20 @@ int cl_autotune_report(char* buf, int64_t len, int64_t* needed) {
             std::memcpy(buf, out.data(), n);
             buf[n] = 0;
         }
+    });
+}
+
+int cl_form_info(cl_ctx* c, int info[8]) {
+    return cl::guarded([&] {
+        check_ctx(c);
+        if (!info) cl::fail(CL_ERR_ARGUMENT, "null output");
+        const Sublattice& sl = c->sl;
+        info[0] = sl.active ? 1 : 0;
+        info[1] = sl.active ? sl.m : 0;
+        info[2] = sl.active ? sl.S : 0;
+        info[3] = sl.active && sl.zb ? 1 : 0;
+        for (int d = 0; d < 3; ++d) info[4 + d] = sl.active ? sl.pad[d] : 0;
+        info[7] = sl.active ? sl.table.nh : 0;
     });
 }
 

@@ -378,7 +378,8 @@ __device__ __forceinline__ void dft_2f(cx<T>* v) {
 
 template <int R, int S, typename T>
 __device__ __forceinline__ void dft(cx<T>* v) {
-    if constexpr (R == 2) dft2<S>(v);
+    if constexpr (R == 1) return;  // a one-point DFT is the identity
+    else if constexpr (R == 2) dft2<S>(v);
     else if constexpr (R == 3) dft3<S>(v);
     else if constexpr (R == 4) dft4<S>(v);
     else if constexpr (R == 5) dft5<S>(v);

@@ -241,6 +241,96 @@ __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restri
 }
 
 // ---------------------------------------------------------------------------------------
+// Pair densities of the FP32 forms, computed in FP32 (the coefficients rounded once).  The
+// products of a request are grouped into blocks of up to 4 x 4: left states I (the higher
+// state of each product) by right states J; block entry prod[i*4 + j] is the density row of
+// (I[i], J[j]) or -1.  A block of PD32_THREADS threads stages `chunk` consecutive sorted atoms:
+// every used state's coefficients are read from HBM once, coalesced along each (state, atom)
+// row of orbitals, rounded to FP32 and stored [state][orbital][atom] (pitch chunk + 1); a thread
+// then takes one (atom, product block) item at a time, 8 shared-memory loads per orbital for 16
+// complex multiply-adds, and writes the block's densities (consecutive threads: consecutive
+// atoms, so the stores are coalesced).
+// ---------------------------------------------------------------------------------------
+constexpr int PD32_THREADS = 128;
+struct PairBlock {
+    int I[4], J[4];  // used-state indices (a missing one repeats a valid state; its outputs are unused)
+    int prod[16];    // density row of (I[i], J[j]), -1: not requested
+};
+
+static __global__ void __launch_bounds__(PD32_THREADS) k_pair_density32(
+    const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb, const int* __restrict__ orig,
+    long long n_sorted, const PairBlock* __restrict__ blocks, int n_blocks, const int* __restrict__ states,
+    int n_used, int chunk, cx<float>* __restrict__ rho) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<float>* sc = reinterpret_cast<cx<float>*>(smem_raw);
+    const int pitch = chunk + 1;
+    const long long n_chunks = (n_sorted + chunk - 1) / chunk;
+    for (long long ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        const long long i0 = ci * chunk;
+        const int ca = (int)min((long long)chunk, n_sorted - i0);
+        // stage: orbital fastest over the threads (each (state, atom) row is contiguous in HBM)
+        // (eight loads in flight per thread before their stores)
+        const int total = n_used * ca * n_orb;
+        for (int e0 = threadIdx.x; e0 < total; e0 += 8 * PD32_THREADS) {
+            cx<double> v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int e = e0 + k * PD32_THREADS;
+                if (e < total) {
+                    const int o = e % n_orb, r = e / n_orb;
+                    const int a = r % ca, su = r / ca;
+                    v[k] = coeff[((long long)states[su] * n_atoms + orig[i0 + a]) * n_orb + o];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int e = e0 + k * PD32_THREADS;
+                if (e < total) {
+                    const int o = e % n_orb, r = e / n_orb;
+                    const int a = r % ca, su = r / ca;
+                    sc[(su * n_orb + o) * pitch + a] = mk((float)v[k].re, (float)v[k].im);
+                }
+            }
+        }
+        __syncthreads();
+        for (int it = threadIdx.x; it < n_blocks * ca; it += PD32_THREADS) {
+            const int b = it / ca, a = it - b * ca;
+            const PairBlock& pb = blocks[b];
+            int ib[4], jb[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                ib[k] = pb.I[k] * n_orb * pitch + a;
+                jb[k] = pb.J[k] * n_orb * pitch + a;
+            }
+            float ar[16], ai[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) ar[k] = ai[k] = 0.f;
+            for (int o = 0; o < n_orb; ++o) {
+                cx<float> l[4], r[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    l[k] = sc[ib[k] + o * pitch];
+                    r[k] = sc[jb[k] + o * pitch];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {  // conj(l) r
+                        ar[i * 4 + j] += l[i].re * r[j].re + l[i].im * r[j].im;
+                        ai[i * 4 + j] += l[i].re * r[j].im - l[i].im * r[j].re;
+                    }
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int p = pb.prod[k];
+                if (p >= 0) rho[(long long)p * n_sorted + i0 + a] = mk(ar[k], ai[k]);
+            }
+        }
+        __syncthreads();  // the stage is refilled for the next chunk
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Pass 1: scatter + conj(phase) + forward FFT along x.  A block owns `rows` consecutive
 // rows (row = z*ny + y); atoms of those rows are [row_ptr[r0], row_ptr[r0+rows]) in the
 // cell-sorted atom list.  Densities are processed one after another by the same block.

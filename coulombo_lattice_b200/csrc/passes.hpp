@@ -19,6 +19,10 @@
 #include "fft.cuh"
 #include "kernels.cuh"
 
+namespace clk {
+struct SlMix;
+}
+
 namespace clp {
 
 using clk::cx;
@@ -75,5 +79,14 @@ bool xyfwd(cudaStream_t s, const cx<T>* rho, long long rho_stride, const int* ro
 template <typename T>
 bool xyinv(cudaStream_t s, cx<T>* buf, long long M, const cx<T>* tw, const int* row_ptr, const int* cell,
            cx<T>* out, long long o_stride, int nx, int ny, int nz, int cnt);
+
+// z pass of the sub-lattice forms (sublattice.cuh): for every (kx, ky) column of the virtual
+// grid and every class, forward FFT along z of nz = 2s points (the s stored planes, the rest zero
+// padding), class mixing with the residue kernels H and the phases, inverse FFT, the s stored
+// planes written back.  zb selects the compiled zinc-blende mixing table.
+bool zmix_supported(int nz);
+template <typename T>
+bool zmix(cudaStream_t s, cx<T>* buf, long long stride, const cx<T>* tw, const cx<T>* H, const cx<T>* phxy,
+          const cx<T>* phz, const clk::SlMix& mix, bool zb, long long nxy, int nz, int cnt);
 
 }  // namespace clp

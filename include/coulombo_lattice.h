@@ -39,6 +39,18 @@ extern "C" {
 #define CL_MODE_FP32_ROUNDS  1  /* the same 8 rounds with FP32 FFT stages; FP64 kernel, twiddles,
                                    round sum and reductions (split-precision tensor-core Gram) */
 #define CL_MODE_FP32_FOURIER CL_MODE_FP32_ROUNDS /* former name of CL_MODE_FP32_ROUNDS */
+/* The sub-lattice forms compute the same aperiodic convolution exactly, but per residue class of
+ * the atoms' grid points modulo m (m = 4 or 2 per axis): each occupied class is a dense sub-grid
+ * transformed with zero padding to 2n/m points per axis, and the classes are coupled once per
+ * frequency by kernels built from the same Ghat.  For zinc-blende or diamond on the a/4 grid (8
+ * of 64 classes) that is one eighth of the 8-round method's transform work.  The choice is made
+ * when the states are loaded: a structure that occupies too many classes (or a grid size not
+ * divisible by m) runs the 8-round method of the same precision.  The grid-level calls
+ * (cl_prepare_grid ...) always run the 8 rounds.  cl_form_info reports what was chosen. */
+#define CL_MODE_FP64_SUBLATTICE 2  /* all-FP64 sub-lattice form */
+#define CL_MODE_FP32_SUBLATTICE 3  /* sub-lattice form with FP32 transforms; FP64 kernel and class
+                                      kernels built in FP64 and rounded once; split-precision
+                                      tensor-core reductions with FP64 accumulation */
 
 typedef struct cl_ctx cl_ctx;
 
@@ -130,6 +142,13 @@ int cl_potentials(cl_ctx* ctx, double* out);
  * rank before one all-reduce.  No reference counterpart (single-process decomposition of
  * the reference's prepare()). */
 int cl_compute_rounds(cl_ctx* ctx, int64_t n_int, const int16_t* spec, int round_mask, double* out);
+
+/* What the context runs for the loaded states: info[0] = 1 when the sub-lattice
+ * decomposition is used (0: the 8 rounds), info[1] = m, info[2] = occupied classes S,
+ * info[3] = 1 when the classes are the zinc-blende set (compiled mixing table), info[4..6] =
+ * transform lengths per axis (2n/m), info[7] = class kernels stored per frequency.  No reference
+ * counterpart (the reference always runs the 8 rounds, CoulombCalculator.cpp:105-163). */
+int cl_form_info(cl_ctx* ctx, int info[8]);
 
 /* Device time in milliseconds of the phases of the last cl_compute / cl_potentials:
  * t[0] pair densities, t[1] transforms (all rounds), t[2] reductions, t[3] total. */
