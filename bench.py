@@ -65,6 +65,12 @@ def parse_args():
     ap.add_argument("--config", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--split", default="densities", choices=["densities", "structures"],
+                    help="N > 1: one request split by left densities over the ranks with one all-reduce of the "
+                         "integrals (strong scaling), or one independent structure per rank (weak scaling)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiler runs: only the headline form's timed replays (inside an NVTX range 'timed'); "
+                         "no other forms, no e2e, no CPU baseline -- the line is not a bench result")
     ap.add_argument("--cells", default=None,
                     help="Lx,Ly,Lz conventional cells instead of the workload's own box (a smaller case of the "
                          "same states and integral list, for profiler captures); the JSON line then names it")
@@ -427,6 +433,111 @@ def run_batch(args):
         torch.distributed.destroy_process_group()
 
 
+def run_sharded(args):
+    """N > 1 GPUs on one request: rank r runs shard r of the plan's left densities (a prepared
+    request of cl_request_create_shard, replayed as a CUDA graph), then one NCCL all-reduce (sum,
+    FP64) of the integral vector.  A step is both; its time is the max over ranks of the device
+    time of the replay plus the all-reduce (CUDA events).  The total work is fixed: strong scaling.
+    e2e: every rank uploads the coefficients from pinned host memory (cl_set_states) and computes
+    its shard (cl_compute_shard); the all-reduced integrals come back to the host."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import coulombo_lattice_b200 as cl
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    d = build_workload(args.config, cells=cells_arg(args))  # the same structure on every rank
+    n = d["states"].shape[0]
+    specs = d["specs"]
+    n_int = specs.shape[0]
+    calc = cl.CoulombCalculator(d["dims"], d["step"], HEADLINE_MODE)
+    calc.initialize(dielectric=DIELECTRIC)
+    calc.set_states(d["states"], d["cells_idx"], d["holes"])
+    full = calc.compute(specs)
+    req = calc.request(specs, rank, world)
+    calc.set_profiling(True)
+    req.run()
+    launches_per_step = sum(v[1] for v in calc.kernel_profile().values())
+    calc.set_profiling(False)
+    graph = cl.Batch([req])
+    vec = torch.zeros(2 * n_int, dtype=torch.float64, device="cuda")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def step():
+        part = graph.run()[0]
+        dev = graph.last_ms()
+        vec.copy_(torch.from_numpy(np.ascontiguousarray(part).view(np.float64)), non_blocking=False)
+        ev0.record()
+        dist.all_reduce(vec, op=dist.ReduceOp.SUM)
+        ev1.record()
+        ev1.synchronize()
+        return dev + ev0.elapsed_time(ev1)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    got = vec.cpu().numpy().view(np.complex128)
+    if not np.allclose(got, full, rtol=1e-9, atol=1e-15):
+        raise RuntimeError("sharded integrals differ from the single-GPU request")
+    torch.cuda.synchronize()
+    dist.barrier()
+    dev_ms = sum(step() for _ in range(args.steps))
+    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t.item()) / args.steps
+    graph.close()
+    req.close()
+    # e2e through the C ABI from pinned host buffers
+    coeff_h = torch.from_numpy(np.ascontiguousarray(d["states"]).view(np.float64).reshape(-1)).pin_memory()
+    cells_h = torch.from_numpy(np.ascontiguousarray(d["cells_idx"], dtype=np.int64)).pin_memory()
+    spec_h = torch.from_numpy(np.ascontiguousarray(specs, dtype=np.int16).reshape(-1)).pin_memory()
+    out_h = torch.zeros(2 * n_int, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        calc.set_states_raw(n, d["holes"], d["states"].shape[1], d["states"].shape[2], coeff_h.data_ptr(),
+                            cells_h.data_ptr())
+        calc.compute_raw_shard(n_int, spec_h.data_ptr(), rank, world, out_h.data_ptr())
+        vec.copy_(out_h, non_blocking=False)
+        dist.all_reduce(vec, op=dist.ReduceOp.SUM)
+        out_h.copy_(vec, non_blocking=False)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    e2e_ms = 1e3 * (time.perf_counter() - e0) / args.steps
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    line = {
+        "metric": "integrals/s", "value": n_int / (ms_per_step / 1e3), "unit": "integrals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_of(args, n_int),
+        "details": {"form": FORM_TEXT[HEADLINE_MODE], "split": "left densities dealt round-robin over the ranks "
+                    "(cl_request_create_shard), one NCCL all-reduce (sum, FP64) of the integral vector per step",
+                    "timing": "max over ranks of the device time of the shard's graph replay plus the all-reduce "
+                              "(CUDA events)"},
+        "e2e": {"value": n_int / (e2e_ms / 1e3), "unit": "integrals/s",
+                "h2d_bytes_per_step": int(coeff_h.numel() * 8 + cells_h.numel() * 8 + spec_h.numel() * 2),
+                "d2h_bytes_per_step": int(out_h.numel() * 8), "ms_per_step": e2e_ms,
+                "call": "per rank: cl_set_states + cl_compute_shard from pinned host buffers, all-reduce, "
+                        "integrals back to the host; wall clock, max over ranks"},
+        "gpu_launches": int(launches_per_step * args.steps),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    calc.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+
 def run_ours(args):
     import torch
     import coulombo_lattice_b200 as cl
@@ -476,9 +587,9 @@ def run_ours(args):
 
     # the all-FP64 8-round path: accuracy reference and the 1x point of the FP32/FP64 ratio; the
     # other forms timed alike, to separate what the decomposition and the precision each give
-    v64, plain_ms, _ = time_form(cl.MODE_FP64_PLAIN)
+    v64, plain_ms, _ = time_form(cl.MODE_FP64_PLAIN) if not args.profile else (None, float("nan"), None)
     other_forms = {}
-    for mode in cl.ALL_MODES:
+    for mode in ([] if args.profile else cl.ALL_MODES):
         if mode in (cl.MODE_FP64_PLAIN, HEADLINE_MODE):
             continue
         vals, ms, info = time_form(mode)
@@ -501,6 +612,8 @@ def run_ours(args):
     for _ in range(max(3, args.warmup)):
         v32 = calc.compute(specs)
 
+    if v64 is None:
+        v64 = v32
     err = np.abs(v32 - v64)
     lim = np.maximum(1e-6 * np.abs(v64), 1e-9)
     accuracy = {"vs_plain_fp64": {
@@ -525,12 +638,14 @@ def run_ours(args):
         pass
     clocks = ClockSampler(uuid)
     barrier()
+    torch.cuda.nvtx.range_push("timed")
     wall0 = time.perf_counter()
     dev_ms = 0.0
     for _ in range(args.steps):
         graph.run()
         dev_ms += graph.last_ms()
     barrier()
+    torch.cuda.nvtx.range_pop()
     wall_ms = 1e3 * (time.perf_counter() - wall0)
     # per-kernel device times: the same request captured with a CUDA-event pair around every
     # launch, replayed for the same number of steps
@@ -556,39 +671,44 @@ def run_ours(args):
     # ---- e2e: pinned host inputs through the C ABI ---------------------------------------
     # The host buffers are allocated and the calls made from the GPU's own NUMA node, so the
     # uploads do not cross the inter-socket link; the affinity is restored afterwards.
-    saved_affinity = os.sched_getaffinity(0)
-    local_cpus = gpu_local_cpus(local)
-    if local_cpus:
-        os.sched_setaffinity(0, local_cpus)
-    coeff_h = torch.from_numpy(np.ascontiguousarray(d["states"]).view(np.float64).reshape(-1)).pin_memory()
-    cells_h = torch.from_numpy(np.ascontiguousarray(d["cells_idx"], dtype=np.int64)).pin_memory()
-    spec_h = torch.from_numpy(np.ascontiguousarray(specs, dtype=np.int16).reshape(-1)).pin_memory()
-    out_h = torch.zeros(2 * n_int, dtype=torch.float64).pin_memory()
-    h2d = coeff_h.numel() * 8 + cells_h.numel() * 8 + spec_h.numel() * 2
-    d2h = out_h.numel() * 8
-    def e2e_step():
-        # one C-ABI call: coefficients and cells in (pinned host memory), integrals out; the
-        # coefficient upload overlaps the transforms (cl_compute_states)
-        calc.compute_states_raw(n, d["holes"], d["states"].shape[1], d["states"].shape[2], coeff_h.data_ptr(),
-                                cells_h.data_ptr(), n_int, spec_h.data_ptr(), out_h.data_ptr())
+    if not args.profile:
+        saved_affinity = os.sched_getaffinity(0)
+        local_cpus = gpu_local_cpus(local)
+        if local_cpus:
+            os.sched_setaffinity(0, local_cpus)
+        coeff_h = torch.from_numpy(np.ascontiguousarray(d["states"]).view(np.float64).reshape(-1)).pin_memory()
+        cells_h = torch.from_numpy(np.ascontiguousarray(d["cells_idx"], dtype=np.int64)).pin_memory()
+        spec_h = torch.from_numpy(np.ascontiguousarray(specs, dtype=np.int16).reshape(-1)).pin_memory()
+        out_h = torch.zeros(2 * n_int, dtype=torch.float64).pin_memory()
+        h2d = coeff_h.numel() * 8 + cells_h.numel() * 8 + spec_h.numel() * 2
+        d2h = out_h.numel() * 8
+        def e2e_step():
+            # one C-ABI call: coefficients and cells in (pinned host memory), integrals out; the
+            # coefficient upload overlaps the transforms (cl_compute_states)
+            calc.compute_states_raw(n, d["holes"], d["states"].shape[1], d["states"].shape[2], coeff_h.data_ptr(),
+                                    cells_h.data_ptr(), n_int, spec_h.data_ptr(), out_h.data_ptr())
 
-    for _ in range(2):
-        e2e_step()
-    barrier()
-    e0 = time.perf_counter()
-    call_ms, call_dev_ms = [], []
-    for _ in range(args.steps):
-        c0 = time.perf_counter()
-        e2e_step()
-        call_ms.append(1e3 * (time.perf_counter() - c0))
-        call_dev_ms.append(calc.timings()["total_ms"])  # first upload to last result, on the device
-    barrier()
-    e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - e0) / args.steps)
-    e2e_device_ms = call_dev_ms[-1]
-    os.sched_setaffinity(0, saved_affinity)
-    e2e_vals = out_h.numpy()[0::2] + 1j * out_h.numpy()[1::2]
-    if not np.allclose(e2e_vals, v32, rtol=1e-9, atol=1e-15):
-        raise RuntimeError("e2e results differ from the resident-input results")
+        for _ in range(2):
+            e2e_step()
+        barrier()
+        e0 = time.perf_counter()
+        call_ms, call_dev_ms = [], []
+        for _ in range(args.steps):
+            c0 = time.perf_counter()
+            e2e_step()
+            call_ms.append(1e3 * (time.perf_counter() - c0))
+            call_dev_ms.append(calc.timings()["total_ms"])  # first upload to last result, on the device
+        barrier()
+        e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - e0) / args.steps)
+        e2e_device_ms = call_dev_ms[-1]
+        os.sched_setaffinity(0, saved_affinity)
+        e2e_vals = out_h.numpy()[0::2] + 1j * out_h.numpy()[1::2]
+        if not np.allclose(e2e_vals, v32, rtol=1e-9, atol=1e-15):
+            raise RuntimeError("e2e results differ from the resident-input results")
+    else:
+        local_cpus, h2d, d2h = None, 0, 0
+        e2e_ms = e2e_device_ms = float("nan")
+        call_ms = call_dev_ms = [float("nan")]
 
     # ---- roofline of the dominant kernel --------------------------------------------------
     peak, peak_kind = measured_peaks()
@@ -671,7 +791,7 @@ def run_ours(args):
         "gpu_launches": int(total_launches),
         "clocks": clock_info,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
         # the oracle's reference-structured FP64 loop on a bounded sample (about 20 s) of this
         # workload's left densities: the CPU baseline, and the per-integral check of both forms
         loop = OracleLoop(d)
@@ -704,6 +824,8 @@ def main():
         run_reference(args)
     elif args.config == "c5":
         run_batch(args)
+    elif dist_env()[1] > 1 and args.split == "densities":
+        run_sharded(args)
     else:
         run_ours(args)
 

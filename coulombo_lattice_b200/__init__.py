@@ -78,6 +78,8 @@ SIGNATURES = [
     ("cl_set_profiling", _i, [_vp, _i]),
     ("cl_kernel_profile", _i, [_vp, _P(_d), _P(_i64), _P(_d)]),
     ("cl_request_create", _i, [_vp, _i64, _P(ctypes.c_int16), _P(_vp)]),
+    ("cl_request_create_shard", _i, [_vp, _i64, _P(ctypes.c_int16), _i, _i, _P(_vp)]),
+    ("cl_compute_shard", _i, [_vp, _i64, _P(ctypes.c_int16), _i, _i, _P(_d)]),
     ("cl_request_run", _i, [_vp, _P(_d)]),
     ("cl_request_destroy", None, [_vp]),
     ("cl_batch_create", _i, [_P(_vp), _i, _P(_vp)]),
@@ -306,6 +308,15 @@ class CoulombCalculator:
         _check(lib().cl_compute_rounds(self._h, s.shape[0], _ptr(s, ctypes.c_int16), int(round_mask), _ptr(out)))
         return out[0::2] + 1j * out[1::2]
 
+    def compute_shard(self, specs, shard, n_shards):
+        """cl_compute_shard: the integrals whose left density is dealt to `shard` of `n_shards`
+        (zeros elsewhere); the shards' results add up to compute()'s."""
+        s = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
+        out = np.zeros(2 * s.shape[0])
+        _check(lib().cl_compute_shard(self._h, s.shape[0], _ptr(s, ctypes.c_int16), int(shard), int(n_shards),
+                                      _ptr(out)))
+        return out[0::2] + 1j * out[1::2]
+
     def set_profiling(self, on=True):
         _check(lib().cl_set_profiling(self._h, int(bool(on))))
 
@@ -325,13 +336,19 @@ class CoulombCalculator:
                                    ctypes.cast(cells_ptr, ctypes.POINTER(ctypes.c_int64))))
         self.n_states, self.n_atoms = n_states, n_atoms
 
+    def compute_raw_shard(self, n_int, spec_ptr, shard, n_shards, out_ptr):
+        """cl_compute_shard on raw host addresses (e.g. pinned buffers)."""
+        _check(lib().cl_compute_shard(self._h, int(n_int), ctypes.cast(spec_ptr, ctypes.POINTER(ctypes.c_int16)),
+                                      int(shard), int(n_shards), ctypes.cast(out_ptr, ctypes.POINTER(ctypes.c_double))))
+
     def compute_raw(self, n_int, spec_ptr, out_ptr):
         _check(lib().cl_compute(self._h, int(n_int), ctypes.cast(spec_ptr, ctypes.POINTER(ctypes.c_int16)),
                                 ctypes.cast(out_ptr, ctypes.POINTER(ctypes.c_double))))
 
-    def request(self, specs):
-        """A prepared request (Request) for repeated runs of the same integral list."""
-        return Request(self, specs)
+    def request(self, specs, shard=0, n_shards=1):
+        """A prepared request (Request) for repeated runs of the same integral list (of one shard
+        of it, see compute_shard)."""
+        return Request(self, specs, shard, n_shards)
 
     def potentials(self):
         out = np.zeros((self.n_states, self.n_atoms))
@@ -354,12 +371,12 @@ class CoulombCalculator:
 class Request:
     """cl_request: plan, device buffers and pinned results prepared once; run() enqueues only."""
 
-    def __init__(self, calc, specs):
+    def __init__(self, calc, specs, shard=0, n_shards=1):
         self.calc = calc
         self.specs = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
         h = ctypes.c_void_p()
-        _check(lib().cl_request_create(calc._h, self.specs.shape[0], _ptr(self.specs, ctypes.c_int16),
-                                       ctypes.byref(h)))
+        _check(lib().cl_request_create_shard(calc._h, self.specs.shape[0], _ptr(self.specs, ctypes.c_int16),
+                                             int(shard), int(n_shards), ctypes.byref(h)))
         self._h = h
         self.out = np.zeros(2 * self.specs.shape[0])
 

@@ -29,7 +29,8 @@ struct Inputs {
 };
 
 // --threads-per-node (coulombo.cpp:36-54): accepted as in the reference, used as the number
-// of text-parser threads.  --precision selects the device form (default fp64 = plain path).
+// of text-parser threads.  --precision and --method select the device form (default fp64 and
+// rounds: the plain path, the reference's method).
 inline void parse_common_options(const clio::ParseResults& pr, Inputs& in) {
     std::string value;
     if (pr.has_value("threads-per-node", value)) {
@@ -38,14 +39,25 @@ inline void parse_common_options(const clio::ParseResults& pr, Inputs& in) {
     } else {
         in.threads = std::max(1u, std::thread::hardware_concurrency());
     }
+    bool fp32 = false, sublattice = false;
     if (pr.has_value("precision", value)) {
         if (value == "fp64")
-            in.mode = CL_MODE_FP64_PLAIN;
+            fp32 = false;
         else if (value == "fp32")
-            in.mode = CL_MODE_FP32_ROUNDS;
+            fp32 = true;
         else
             clio::throwfr("invalid value for precision: %s", value.c_str());
     }
+    if (pr.has_value("method", value)) {
+        if (value == "rounds")
+            sublattice = false;
+        else if (value == "sublattice")
+            sublattice = true;
+        else
+            clio::throwfr("invalid value for method: %s", value.c_str());
+    }
+    in.mode = sublattice ? (fp32 ? CL_MODE_FP32_SUBLATTICE : CL_MODE_FP64_SUBLATTICE)
+                         : (fp32 ? CL_MODE_FP32_ROUNDS : CL_MODE_FP64_PLAIN);
 }
 
 // "Reading atom positions" (coulombo.cpp:56-74, FunctionCollection.cpp:14-20)

@@ -28,6 +28,8 @@ const char* kUsage =
     "  --orbitals=N           number of (spin-)orbitals per atom, default: 20\n"
     "  --output-dir=DIR       directory for output files, default: current\n"
     "  --precision=fp64|fp32  fp64: all-FP64 path (default); fp32: FP32 transforms, FP64 sums\n"
+    "  --method=rounds|sublattice  rounds: the 8-round convolution (default); sublattice: the\n"
+    "                           exact per-residue-class decomposition where the structure allows\n"
     "  --skip-lines=N         number of lines to be skipped on top of each LCAO file, default: 0\n"
     "  --threads-per-node=N   number of host threads for reading inputs, default: all cores\n"
     "  --tf-lattice=VALUE     lattice constant (A) for Thomas-Fermi-Resta model,\n"
@@ -87,7 +89,7 @@ void run(const clio::ParseResults& pr) {
 int main(int argc, char** argv) {
     try {
         clio::Parser cmd;
-        for (const char* v : {"atoms", "dielectric", "integrals", "onsite", "orbitals", "output-dir", "precision",
+        for (const char* v : {"atoms", "dielectric", "integrals", "onsite", "orbitals", "method", "output-dir", "precision",
                               "skip-lines", "threads-per-node", "tf-lattice"})
             cmd.allow_value(v);
         clio::ParseResults pr = cmd.process(argc, argv);

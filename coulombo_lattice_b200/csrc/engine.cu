@@ -888,7 +888,28 @@ void ensure_sl_tables(cl_ctx* c) {
     }
     const double denom = (double)((unsigned long long)c->M * 8ull);
     const int blocks = grid_for(nq);
-    if (fp32) {
+    if (sl.zb) {
+        // raw class kernels in FP64, then their Walsh-Hadamard form (sublattice.cuh) rounded once
+        DevBuf<cx<double>> raw;
+        raw.alloc((size_t)res.nh * nq);
+        clk::k_sl_build_h<double><<<blocks, 256, 0, c->stream>>>(c->ghat.p, c->n[0], c->n[1], c->n[2], px, py, pz,
+                                                                 res, denom, raw.p);
+        CL_LAUNCHED();
+        clk::SlWht w{};
+        for (int k = 0; k < 8; ++k) {
+            w.src[k] = sl.table.h[k * clk::kSlMaxClasses];  // (class k, class 0): alpha_k, then beta_k
+            w.cj[k] = sl.table.cj[k * clk::kSlMaxClasses];
+        }
+        if (fp32) {
+            sl.H32.alloc((size_t)8 * nq);
+            clk::k_sl_zb_wht<float><<<blocks, 256, 0, c->stream>>>(raw.p, nq, w, sl.H32.p);
+        } else {
+            sl.H64.alloc((size_t)8 * nq);
+            clk::k_sl_zb_wht<double><<<blocks, 256, 0, c->stream>>>(raw.p, nq, w, sl.H64.p);
+        }
+        CL_LAUNCHED();
+        CL_CUDA(cudaStreamSynchronize(c->stream));  // raw goes out of scope
+    } else if (fp32) {
         sl.H32.alloc((size_t)res.nh * nq);
         clk::k_sl_build_h<float><<<blocks, 256, 0, c->stream>>>(c->ghat.p, c->n[0], c->n[1], c->n[2], px, py, pz, res,
                                                                 denom, sl.H32.p);
@@ -934,7 +955,9 @@ void ensure_sl_tables(cl_ctx* c) {
 // grid (fused plane pass where compiled and faster), the z pass with class mixing, the y and x
 // inverse passes writing the values at the atoms; in the FP32 form they are widened to V.
 template <typename T>
-void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, cx<double>* V, long long v_stride) {
+void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, void* V_any, long long v_stride,
+                    bool v32) {
+    cx<double>* V = static_cast<cx<double>*>(V_any);
     ensure_sl_tables(c);
     const Sublattice& sl = c->sl;
     const int nx = sl.vn[0], ny = sl.vn[1], nz = sl.vn[2];
@@ -948,12 +971,14 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, c
     const int* row_ptr = c->row_ptr.p;
     const int* cell = c->cell_sorted.p;
     const long long n_at = c->n_sorted;
-    // values at the atoms: straight into V in FP64; through the rounds buffer in FP32
-    const size_t at_bytes = fp32 ? sizeof(cx<T>) * (size_t)n_at : 0;
+    // values at the atoms: straight into V in FP64, and in FP32 when the reductions read FP32
+    // potentials (v32); otherwise through the rounds buffer, widened to V
+    const bool via_tr = fp32 && !v32;
+    const size_t at_bytes = via_tr ? sizeof(cx<T>) * (size_t)n_at : 0;
     size_t budget = (size_t)(0.6 * (double)(free_device_bytes() + c->work.n + c->rounds.n));
     int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(np, 1), budget / (grid_bytes + at_bytes)));
     c->work.alloc(std::max(c->work.n, (size_t)chunk * grid_bytes));
-    if (fp32) c->rounds.alloc(std::max(c->rounds.n, (size_t)chunk * at_bytes));
+    if (via_tr) c->rounds.alloc(std::max(c->rounds.n, (size_t)chunk * at_bytes));
     cx<T>* buf = reinterpret_cast<cx<T>*>(c->work.p);
     cx<T>* tr = reinterpret_cast<cx<T>*>(c->rounds.p);
     const cx<T>* twx = fp32 ? (const cx<T>*)sl.ax[0].tw32.p : (const cx<T>*)sl.ax[0].tw64.p;
@@ -983,8 +1008,8 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, c
     const bool plane_ok = reg_x && reg_y && clp::plane_supported(fp32, nx, ny);
     // no phase in any pass: the rounds' phase tables are never read with kappa = 0
     const clk::RoundPhase rp0{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
-    cx<T>* out0 = fp32 ? tr : reinterpret_cast<cx<T>*>(V);
-    const long long out_stride = fp32 ? n_at : v_stride;
+    cx<T>* out0 = via_tr ? tr : static_cast<cx<T>*>(V_any);
+    const long long out_stride = via_tr ? n_at : v_stride;
     if (autotune_enabled() && !std::getenv("CL_TUNE_FORCE") && np > 0 && !stream_capturing(c->stream)) {
         const int cnt_t = (int)std::max<size_t>(1, std::min<size_t>((size_t)chunk, (512ull << 20) / grid_bytes));
         const int* rp_skip = skip_empty ? row_ptr : nullptr;
@@ -1026,7 +1051,7 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, c
     for (int p0 = 0; p0 < np; p0 += chunk) {
         const int cnt = std::min(chunk, np - p0);
         const cx<T>* rho_c = rho + (long long)p0 * rho_stride;
-        cx<T>* out_c = fp32 ? tr : reinterpret_cast<cx<T>*>(V + (long long)p0 * v_stride);
+        cx<T>* out_c = via_tr ? tr : static_cast<cx<T>*>(V_any) + (long long)p0 * v_stride;
         cudaEvent_t e = prof_begin(c);
         if (xy_fwd) {
             clp::xyfwd<T>(c->stream, rho_c, rho_stride, row_ptr, cell, buf, vM, twx, rp0, nx, ny, nz, cnt);
@@ -1073,7 +1098,7 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, c
         CL_LAUNCHED();
         prof_end(c, e, CL_KCLASS_XINV,
                  cnt * ((xy_inv ? 1.0 : row_side) * gbytes + atoms * (double)sizeof(cx<T>)) + atoms * 4.0);
-        if (fp32) {
+        if (via_tr) {
             e = prof_begin(c);
             clk::k_sl_widen<T><<<dim3((unsigned)std::min<long long>((n_at + 255) / 256, 148LL * 8), cnt), 256, 0,
                                  c->stream>>>(tr, n_at, V + (long long)p0 * v_stride, v_stride, n_at);
@@ -1085,24 +1110,36 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, c
 
 // The transforms of a request on the context's loaded atoms: the sub-lattice decomposition when
 // it is in use, else the 8 rounds (of the rounds in round_mask).
-void run_transforms(cl_ctx* c, const void* rho, long long rho_stride, int np, cx<double>* V, long long v_stride,
+// V is complex128 [np][v_stride], or complex64 when v32 (the FP32 sub-lattice form whose
+// reductions read FP32 potentials, see v_fp32).
+void run_transforms(cl_ctx* c, const void* rho, long long rho_stride, int np, void* V, long long v_stride, bool v32,
                     int round_mask = 0xFF) {
     if (c->sl.active) {
         if ((round_mask & 0xFF) != 0xFF)
             cl::fail(CL_ERR_UNSUPPORTED, "the sub-lattice form has no rounds to split (use an 8-round form)");
         if (fp64_form(c))
-            run_sublattice<double>(c, static_cast<const cx<double>*>(rho), rho_stride, np, V, v_stride);
+            run_sublattice<double>(c, static_cast<const cx<double>*>(rho), rho_stride, np, V, v_stride, false);
         else
-            run_sublattice<float>(c, static_cast<const cx<float>*>(rho), rho_stride, np, V, v_stride);
+            run_sublattice<float>(c, static_cast<const cx<float>*>(rho), rho_stride, np, V, v_stride, v32);
         return;
     }
-    run_rounds_mode(c, rho, rho_stride, np, c->row_ptr.p, c->cell_sorted.p, V, v_stride, round_mask);
+    if (v32) cl::fail(CL_ERR_STATE, "the 8-round forms write FP64 potentials");
+    run_rounds_mode(c, rho, rho_stride, np, c->row_ptr.p, c->cell_sorted.p, static_cast<cx<double>*>(V), v_stride,
+                    round_mask);
 }
 
 // ---------------------------------------------------------------------------------------
 // Tensor-core Gram (FP32 form): TF32 split pass + tcgen05 GEMM, see gram_tc.cuh.
 // ---------------------------------------------------------------------------------------
 bool use_tc_gram(const cl_ctx* c) { return !fp64_form(c) && !std::getenv("CL_NO_TC_GRAM"); }
+
+// The FP32 sub-lattice form keeps the potentials at the atoms in FP32 (as the inverse passes
+// produce them) when the tensor-core Gram reads them: its split rounds them to TF32 parts
+// directly, with no FP64 copy in between.
+bool v_fp32(const cl_ctx* c) { return c->sl.active && !fp64_form(c) && use_tc_gram(c); }
+void* v_at(void* base, long long elems, bool v32) {
+    return static_cast<unsigned char*>(base) + elems * (long long)(v32 ? sizeof(cx<float>) : sizeof(cx<double>));
+}
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -1118,14 +1155,15 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// 2D FP32 tensor [outer][k_pad] viewed in boxes of 32 x box_rows, 128-byte swizzle.
-CUtensorMap tc_tensor_map(float* base, long long k_pad, long long outer, int box_rows) {
+// 3D FP32 tensor [2 parts][rows][k_pad] viewed in boxes of 32 atoms x box_rows rows x 1 part,
+// 128-byte swizzle; rows of a box beyond `rows` are zero-filled by the copy (not read).
+CUtensorMap tc_tensor_map(float* base, long long k_pad, long long rows, int box_rows) {
     CUtensorMap m;
-    const cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)outer};
-    const cuuint64_t strides[1] = {(cuuint64_t)k_pad * sizeof(float)};
-    const cuuint32_t box[2] = {(cuuint32_t)clk::tc::BK, (cuuint32_t)box_rows};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+    const cuuint64_t dims[3] = {(cuuint64_t)k_pad, (cuuint64_t)rows, 2};
+    const cuuint64_t strides[2] = {(cuuint64_t)k_pad * sizeof(float), (cuuint64_t)(rows * k_pad) * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)clk::tc::BK, (cuuint32_t)box_rows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
                                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) cl::fail(CL_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -1133,7 +1171,7 @@ CUtensorMap tc_tensor_map(float* base, long long k_pad, long long outer, int box
 }
 
 struct TcShape {
-    int rowsA = 0, rowsB = 0;
+    int rowsA = 0, rowsB = 0;        // real operand rows: re and im of each density
     long long chunk = 0, k_pad = 0;  // atoms per operand chunk, chunk rounded up to a k-tile
 };
 
@@ -1141,8 +1179,8 @@ long long tc_bytes_per_atom(int rowsA, int rowsB) { return 2LL * (rowsA + rowsB)
 
 TcShape tc_shape(const cl_ctx* c, int nl, int nr, long long n_atoms) {
     TcShape s;
-    s.rowsA = (2 * nl + clk::tc::BM - 1) / clk::tc::BM * clk::tc::BM;
-    s.rowsB = (2 * nr + clk::tc::BN - 1) / clk::tc::BN * clk::tc::BN;
+    s.rowsA = 2 * nl;
+    s.rowsB = 2 * nr;
     const long long per_atom = tc_bytes_per_atom(s.rowsA, s.rowsB);
     const long long fit = (long long)(c->tc_buf.n * sizeof(float)) / per_atom / clk::tc::BK * clk::tc::BK;
     const long long full = (n_atoms + clk::tc::BK - 1) / clk::tc::BK * clk::tc::BK;
@@ -1155,8 +1193,7 @@ TcShape tc_shape(const cl_ctx* c, int nl, int nr, long long n_atoms) {
 // device memory (at most 8 GiB), else chunks of the atom range.  Called outside any capture.
 void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms) {
     if (!use_tc_gram(c) || nl <= 0 || nr <= 0 || n_atoms <= 0) return;
-    const int rowsA = (2 * nl + clk::tc::BM - 1) / clk::tc::BM * clk::tc::BM;
-    const int rowsB = (2 * nr + clk::tc::BN - 1) / clk::tc::BN * clk::tc::BN;
+    const int rowsA = 2 * nl, rowsB = 2 * nr;
     const long long per_atom = tc_bytes_per_atom(rowsA, rowsB);
     const long long full = (n_atoms + clk::tc::BK - 1) / clk::tc::BK * clk::tc::BK;
     const long long have = (long long)(c->tc_buf.n * sizeof(float)) / per_atom;
@@ -1171,7 +1208,7 @@ void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms) {
 }
 
 // out4[l][r] += {sum ac, bd, ad, bc} (out4 zeroed by the caller, error slot included).
-void gram_tc(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const void* rho, bool rho_f32,
+void gram_tc(cl_ctx* c, const void* V, bool v_f32, long long v_stride, int nl, const void* rho, bool rho_f32,
              long long r_stride, const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
     using namespace clk::tc;
     const TcShape sh = tc_shape(c, nl, nr, n_atoms);
@@ -1183,27 +1220,32 @@ void gram_tc(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const v
     }
     float* A = c->tc_buf.p;
     float* B = A + 2LL * sh.rowsA * sh.k_pad;
-    const CUtensorMap mapA = tc_tensor_map(A, sh.k_pad, 2LL * sh.rowsA, BM);
-    const CUtensorMap mapB = tc_tensor_map(B, sh.k_pad, 2LL * sh.rowsB, BN);
-    const int tiles = (sh.rowsA / BM) * (sh.rowsB / BN);
+    const CUtensorMap mapA = tc_tensor_map(A, sh.k_pad, sh.rowsA, BM);
+    const CUtensorMap mapB = tc_tensor_map(B, sh.k_pad, sh.rowsB, BN);
+    const int tilesA = (sh.rowsA + BM - 1) / BM, tilesB = (sh.rowsB + BN - 1) / BN;
+    const int tiles = tilesA * tilesB;
     for (long long a0 = 0; a0 < n_atoms; a0 += sh.chunk) {
         const long long na = std::min(sh.chunk, n_atoms - a0);
         const long long kp = (na + BK - 1) / BK * BK;  // k-tiles that hold atoms of this chunk
         const int kt_total = (int)(kp / BK);
         cudaEvent_t e0 = prof_begin(c);
         const int xblocks = (int)std::min<long long>((kp + 255) / 256, 64);
-        clk::tc::k_tf32_split<double><<<dim3(xblocks, sh.rowsA / 2), 256, 0, c->stream>>>(
-            V, v_stride, nullptr, nl, sh.rowsA, a0, na, sh.k_pad, A);
+        if (v_f32)
+            clk::tc::k_tf32_split<float><<<dim3(xblocks, nl), 256, 0, c->stream>>>(
+                static_cast<const cx<float>*>(V), v_stride, nullptr, nl, a0, na, sh.k_pad, A);
+        else
+            clk::tc::k_tf32_split<double><<<dim3(xblocks, nl), 256, 0, c->stream>>>(
+                static_cast<const cx<double>*>(V), v_stride, nullptr, nl, a0, na, sh.k_pad, A);
         CL_LAUNCHED();
         if (rho_f32)
-            clk::tc::k_tf32_split<float><<<dim3(xblocks, sh.rowsB / 2), 256, 0, c->stream>>>(
-                static_cast<const cx<float>*>(rho), r_stride, ridx_dev, nr, sh.rowsB, a0, na, sh.k_pad, B);
+            clk::tc::k_tf32_split<float><<<dim3(xblocks, nr), 256, 0, c->stream>>>(
+                static_cast<const cx<float>*>(rho), r_stride, ridx_dev, nr, a0, na, sh.k_pad, B);
         else
-            clk::tc::k_tf32_split<double><<<dim3(xblocks, sh.rowsB / 2), 256, 0, c->stream>>>(
-                static_cast<const cx<double>*>(rho), r_stride, ridx_dev, nr, sh.rowsB, a0, na, sh.k_pad, B);
+            clk::tc::k_tf32_split<double><<<dim3(xblocks, nr), 256, 0, c->stream>>>(
+                static_cast<const cx<double>*>(rho), r_stride, ridx_dev, nr, a0, na, sh.k_pad, B);
         CL_LAUNCHED();
         prof_end(c, e0, CL_KCLASS_GRAM_SPLIT,
-                 (double)na * (nl * 16.0 + nr * (rho_f32 ? 8.0 : 16.0)) +
+                 (double)na * (nl * (v_f32 ? 8.0 : 16.0) + nr * (rho_f32 ? 8.0 : 16.0)) +
                      (double)tc_bytes_per_atom(sh.rowsA, sh.rowsB) * kp);
         // atom splits: whole waves of 148 blocks, each split at least 2 chunks long
         int best_s = 1;
@@ -1223,8 +1265,8 @@ void gram_tc(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const v
         const int kt_per = (kt_total + best_s - 1) / best_s;
         const int splits = (kt_total + kt_per - 1) / kt_per;
         cudaEvent_t e1 = prof_begin(c);
-        clk::tc::k_gram_tc<<<dim3(sh.rowsA / BM, sh.rowsB / BN, splits), THREADS, SMEM_BYTES, c->stream>>>(
-            mapA, mapB, sh.rowsA, sh.rowsB, kt_total, kt_per, nl, nr, out4_dev);
+        clk::tc::k_gram_tc<<<dim3(tilesA, tilesB, splits), THREADS, SMEM_BYTES, c->stream>>>(
+            mapA, mapB, kt_total, kt_per, nl, nr, out4_dev);
         CL_LAUNCHED();
         prof_end(c, e1, CL_KCLASS_GRAM, (double)tc_bytes_per_atom(sh.rowsA, sh.rowsB) * kp);
     }
@@ -1241,13 +1283,15 @@ void check_gram_slot(double slot) {
 // max(nl, nr) least, preferring larger blocks.
 // rho: the right densities, complex64 when rho_f32 (the FP32 form's pair densities), else
 // complex128 (the plain form's, and the grid API's caller-given density).
-void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const void* rho_any, bool rho_f32,
+void gram(cl_ctx* c, const void* V_any, bool v_f32, long long v_stride, int nl, const void* rho_any, bool rho_f32,
           long long r_stride, const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
     CL_CUDA(cudaMemsetAsync(out4_dev, 0, sizeof(double) * (4 * (size_t)nl * nr + 1), c->stream));
     if (use_tc_gram(c)) {
-        gram_tc(c, V, v_stride, nl, rho_any, rho_f32, r_stride, ridx_dev, nr, n_atoms, out4_dev);
+        gram_tc(c, V_any, v_f32, v_stride, nl, rho_any, rho_f32, r_stride, ridx_dev, nr, n_atoms, out4_dev);
         return;
     }
+    if (v_f32) cl::fail(CL_ERR_STATE, "the FP64 Gram needs FP64 potentials");
+    const cx<double>* V = static_cast<const cx<double>*>(V_any);
     const int pmax = std::max(nl, nr);
     int ib = 4;
     long long best = -1;
@@ -1291,11 +1335,12 @@ void gram(cl_ctx* c, const cx<double>* V, long long v_stride, int nl, const void
 // enqueues (it can be captured in a CUDA graph).
 struct PairSetup {
     DevBuf<clk::PairSeg> segs;  // products grouped by left state, indices into `states` (FP64 kernel)
-    DevBuf<clk::PairBlock> pblocks;  // products in 4 x 4 state blocks (FP32 kernel)
+    clk::PairTri tri{};  // products over at most 8 states (FP32 register kernel)
+    bool reg_ok = false;
+    int grid_reg = 1;
     DevBuf<int> states;
     int np = 0, n_segs = 0, n_used = 0, chunk = 1, blocks = 1;
-    int n_pblocks = 0, chunk32 = 1, grid32 = 1;
-    size_t smem = 0, smem32 = 0;
+    size_t smem = 0;
 };
 
 void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
@@ -1323,52 +1368,27 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
         }
     ps.n_segs = (int)segs.size();
     ps.segs.upload(segs.data(), segs.size(), c->stream);
-    // FP32 kernel: the used states in ascending order, in groups of four; every product
-    // (higher state x, lower state y) falls in the block (group of x, group of y)
-    {
+    // register kernel (at most 8 used states): the used states in ascending order, and the
+    // density row of each product (i, j), i >= j in that order (rows are conj(c_x) c_y, x >= y)
+    ps.reg_ok = !used.empty() && used.size() <= 8;
+    if (ps.reg_ok) {
         std::vector<int> order(used.size());
         std::iota(order.begin(), order.end(), 0);
         std::sort(order.begin(), order.end(), [&](int a, int b) { return used[a] < used[b]; });
-        std::vector<int> group(used.size()), pos(used.size());
+        std::vector<int> pos(used.size());
         for (size_t k = 0; k < order.size(); ++k) {
-            group[order[k]] = (int)(k / 4);
-            pos[order[k]] = (int)(k % 4);
+            pos[order[k]] = (int)k;
+            ps.tri.states[k] = used[order[k]];
         }
-        const int ng = ((int)used.size() + 3) / 4;
-        std::vector<int> bidx((size_t)ng * ng, -1);
-        std::vector<clk::PairBlock> pb;
+        for (size_t k = order.size(); k < 8; ++k) ps.tri.states[k] = used[order[0]];
+        for (int& v : ps.tri.prod) v = -1;
         for (int p = 0; p < ps.np; ++p) {
-            const int ux = where[fl[p].x], uy = where[fl[p].y];  // rows are conj(c_x) c_y with x >= y
-            if (group[ux] < group[uy]) cl::fail(CL_ERR_STATE, "pair density with its lower state first");
-            const int gx = group[ux], gy = group[uy];
-            int& bi = bidx[(size_t)gx * ng + gy];
-            if (bi < 0) {
-                bi = (int)pb.size();
-                clk::PairBlock b{};
-                for (int k = 0; k < 4; ++k) {
-                    const int kx = std::min<int>(4 * gx + k, (int)used.size() - 1);
-                    const int ky = std::min<int>(4 * gy + k, (int)used.size() - 1);
-                    b.I[k] = order[kx];
-                    b.J[k] = order[ky];
-                }
-                for (int k = 0; k < 16; ++k) b.prod[k] = -1;
-                pb.push_back(b);
-            }
-            pb[bi].prod[pos[ux] * 4 + pos[uy]] = p;
+            const int i = pos[where[fl[p].x]], j = pos[where[fl[p].y]];
+            if (i < j) cl::fail(CL_ERR_STATE, "pair density with its lower state first");
+            ps.tri.prod[i * (i + 1) / 2 + j] = p;
         }
-        ps.n_pblocks = (int)pb.size();
-        ps.pblocks.upload(pb.data(), pb.size(), c->stream);
-        // chunk: enough (atom, block) items for the block's threads, at most ~56 KB staged
-        const size_t per_atom32 = sizeof(cx<float>) * (size_t)used.size() * c->n_orb;
-        int ch = std::max(8, (clk::PD32_THREADS + ps.n_pblocks - 1) / std::max(1, ps.n_pblocks));
-        while (ch > 8 && per_atom32 * (ch + 1) > 56 * 1024) --ch;
-        while (ch > 1 && per_atom32 * (ch + 1) > 200 * 1024) --ch;
-        ps.chunk32 = ch;
-        ps.smem32 = per_atom32 * (ch + 1);
-        ensure_smem(clk::k_pair_density32, ps.smem32);
-        const long long chunks32 = (c->n_sorted + ch - 1) / ch;
-        const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(16, (200 * 1024) / ps.smem32));
-        ps.grid32 = (int)std::min<long long>(chunks32, 148LL * per_sm);
+        const int apb = clk::pair_atoms_per_block((int)used.size());
+        ps.grid_reg = (int)std::max<long long>(1, std::min<long long>((c->n_sorted + apb - 1) / apb, 148LL * 2 * 8));
     }
     ps.states.upload(used.data(), used.size(), c->stream);
     ps.n_used = (int)used.size();
@@ -1395,25 +1415,51 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
     CL_CUDA(cudaStreamSynchronize(c->stream));
 }
 
+// f(std::integral_constant<int, n>) for 1 <= n <= 8 used states
+template <typename F>
+void with_states(int n, F&& f) {
+    switch (n) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 3: f(std::integral_constant<int, 3>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        case 5: f(std::integral_constant<int, 5>{}); break;
+        case 6: f(std::integral_constant<int, 6>{}); break;
+        case 7: f(std::integral_constant<int, 7>{}); break;
+        default: f(std::integral_constant<int, 8>{}); break;
+    }
+}
+
 void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
     // the shared-memory attribute is per kernel, so another setup (of another group or
     // request) may have lowered it since this one was prepared
     cudaEvent_t e = prof_begin(c);
-    if (fp64_form(c)) {
+    if (fp64_form(c) && ps.reg_ok) {
+        cx<double>* out = static_cast<cx<double>*>(rho);
+        const auto go = [&](auto ns) {
+            constexpr int NS = decltype(ns)::value;
+            clk::k_pair_density_reg<NS, double><<<ps.grid_reg, 256, 0, c->stream>>>(
+                c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
+        };
+        with_states(ps.n_used, go);
+    } else if (fp64_form(c)) {
         ensure_smem(clk::k_pair_density<double>, ps.smem);
         clk::k_pair_density<double><<<ps.blocks, 256, ps.smem, c->stream>>>(
             c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<double>*>(rho));
-    } else if (std::getenv("CL_PAIR_FP64_SUMS")) {  // the FP32 forms with FP64 sums, rounded once
+    } else if (ps.reg_ok) {
+        cx<float>* out = static_cast<cx<float>*>(rho);
+        const auto go = [&](auto ns) {
+            constexpr int NS = decltype(ns)::value;
+            clk::k_pair_density_reg<NS, float><<<ps.grid_reg, 256, 0, c->stream>>>(
+                c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
+        };
+        with_states(ps.n_used, go);
+    } else {  // more than 8 states: the staged kernel (FP64 sums, rounded once)
         ensure_smem(clk::k_pair_density<float>, ps.smem);
         clk::k_pair_density<float><<<ps.blocks, 256, ps.smem, c->stream>>>(
             c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<float>*>(rho));
-    } else {
-        ensure_smem(clk::k_pair_density32, ps.smem32);
-        clk::k_pair_density32<<<ps.grid32, clk::PD32_THREADS, ps.smem32, c->stream>>>(
-            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.pblocks.p, ps.n_pblocks,
-            ps.states.p, ps.n_used, ps.chunk32, static_cast<cx<float>*>(rho));
     }
     CL_LAUNCHED();
     prof_end(c, e, CL_KCLASS_DENSITY,
@@ -1585,7 +1631,7 @@ int cl_calculate_grid(cl_ctx* c, const double* rho2, double out[2]) {
         int zero = 0;
         ridx.upload(&zero, 1, c->stream);
         tc_reserve(c, 1, 1, c->M);
-        gram(c, c->grid_V.p, c->M, 1, c->grid_rho2.p, false, c->M, ridx.p, 1, c->M, o4.p);
+        gram(c, c->grid_V.p, false, c->M, 1, c->grid_rho2.p, false, c->M, ridx.p, 1, c->M, o4.p);
         double h[5];
         CL_CUDA(cudaMemcpyAsync(h, o4.p, sizeof h, cudaMemcpyDeviceToHost, c->stream));
         CL_CUDA(cudaStreamSynchronize(c->stream));
@@ -1822,7 +1868,27 @@ void map_step_values(const std::vector<cl::PlanStep>& plan, const std::vector<in
     for (auto& th : pool) th.join();
 }
 
-void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, int round_mask) {
+// The steps of shard `shard` of `n_shards`: the plan's prepared (left) densities, in ascending
+// product order, are dealt round-robin, and a step belongs to the shard of its left density.
+// Every step is in exactly one shard, so the shards' integrals add up to the whole request's.
+std::vector<cl::PlanStep> shard_steps(std::vector<cl::PlanStep> plan, int n_states, int shard, int n_shards) {
+    if (n_shards < 1 || shard < 0 || shard >= n_shards) cl::fail(CL_ERR_ARGUMENT, "invalid shard %d of %d", shard, n_shards);
+    if (n_shards == 1) return plan;
+    const int P = n_states * (n_states + 1) / 2;
+    std::vector<int> owner(P, -1);
+    for (const auto& st : plan) owner[st.left.product] = 0;
+    int k = 0;
+    for (int p = 0; p < P; ++p)
+        if (owner[p] == 0) owner[p] = k++ % n_shards;
+        else owner[p] = -1;
+    std::vector<cl::PlanStep> mine;
+    for (const auto& st : plan)
+        if (owner[st.left.product] == shard) mine.push_back(st);
+    return mine;
+}
+
+void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, int round_mask, int shard = 0,
+                  int n_shards = 1) {
     {
         check_ctx(c);
         check_kernel(c);
@@ -1833,7 +1899,9 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
         for (int64_t i = 0; i < n_int; ++i)
             for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
-        const auto plan = cl::orient_steps(c->n_states, specs);
+        const auto plan = shard_steps(cl::orient_steps(c->n_states, specs), c->n_states, shard, n_shards);
+        if (n_shards > 1) std::memset(out, 0, sizeof(double) * 2 * (size_t)n_int);
+        if (plan.empty()) return;
         // densities: prepared (left) products first, then right-only products
         const int P = c->n_states * (c->n_states + 1) / 2;
         std::vector<int> slot(P, -1), is_left(P, 0), is_right(P, 0);
@@ -1871,9 +1939,10 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
-        run_transforms(c, rho.p, As, nl, V.p, As, round_mask);
+        const bool v32 = v_fp32(c);
+        run_transforms(c, rho.p, As, nl, V.p, As, v32, round_mask);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
-        gram(c, V.p, As, nl, rho.p, rho_bytes(c) == sizeof(cx<float>), As, dr.p, nr, As, o4.p);
+        gram(c, V.p, v32, As, nl, rho.p, rho_bytes(c) == sizeof(cx<float>), As, dr.p, nr, As, o4.p);
         CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
         std::vector<double> h((size_t)4 * nl * nr + 1);
         CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -2019,6 +2088,7 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     PairSetup ps_right;
     if (nu > nl) pair_setup(c, pairs_of(nl, nu), ps_right);
     const long long As = c->n_sorted;
+    const bool v32 = v_fp32(c);
     DevBuf<int>& dr = c->req_ridx;
     grow(dr, rights.size());
     CL_CUDA(cudaMemcpyAsync(dr.p, rights.data(), rights.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -2035,13 +2105,13 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
         CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[g->last_state], 0));
         pair_launch(c, g->ps, rho_at(c, rho.p, (long long)g->begin * As));
         run_transforms(c, rho_at(c, rho.p, (long long)g->begin * As), As, g->end - g->begin,
-                       V.p + (long long)g->begin * As, As);
+                       v_at(V.p, (long long)g->begin * As, v32), As, v32);
     }
     upload_through(n_states - 1);
     CL_CUDA(cudaStreamWaitEvent(c->stream, c->state_ev[n_states - 1], 0));
     if (nu > nl) pair_launch(c, ps_right, rho_at(c, rho.p, (long long)nl * As));
     CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
-    gram(c, V.p, As, nl, rho.p, rho_bytes(c) == sizeof(cx<float>), As, dr.p, nr, As, o4.p);
+    gram(c, V.p, v32, As, nl, rho.p, rho_bytes(c) == sizeof(cx<float>), As, dr.p, nr, As, o4.p);
     CL_CUDA(cudaEventRecord(c->ev[3], c->stream));
     std::vector<double> h((size_t)4 * nl * nr + 1);
     CL_CUDA(cudaMemcpyAsync(h.data(), o4.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -2078,6 +2148,10 @@ int cl_compute_rounds(cl_ctx* c, int64_t n_int, const int16_t* spec, int round_m
         if (round_mask < 0 || round_mask > 0xFF) cl::fail(CL_ERR_ARGUMENT, "round mask must be within 0..255");
         compute_impl(c, n_int, spec, out, round_mask);
     });
+}
+
+int cl_compute_shard(cl_ctx* c, int64_t n_int, const int16_t* spec, int shard, int n_shards, double* out) {
+    return cl::guarded([&] { compute_impl(c, n_int, spec, out, 0xFF, shard, n_shards); });
 }
 
 int cl_set_profiling(cl_ctx* c, int enable) {
@@ -2124,7 +2198,7 @@ int cl_potentials(cl_ctx* c, double* out) {
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
-        run_transforms(c, rho.p, As, n, V.p, As);
+        run_transforms(c, rho.p, As, n, V.p, As, false);
         CL_CUDA(cudaEventRecord(c->ev[2], c->stream));
         std::vector<cx<double>> h((size_t)n * As);
         CL_CUDA(cudaMemcpyAsync(h.data(), V.p, h.size() * sizeof(cx<double>), cudaMemcpyDeviceToHost, c->stream));
@@ -2159,6 +2233,7 @@ struct cl_request {
     DevBuf<double> o4;
     double* o4_host = nullptr;  // pinned
     bool warm = false;
+    int n_shards = 1;  // out entries of other shards' steps are zero
     ~cl_request() {
         if (o4_host) cudaFreeHost(o4_host);
     }
@@ -2193,15 +2268,19 @@ namespace {
 // pageable copies -- it can be captured.
 void request_enqueue(cl_request* r) {
     cl_ctx* c = r->ctx;
+    if (r->nl == 0) return;  // a shard without densities
     const long long As = c->n_sorted;
     pair_launch(c, r->ps, r->rho.p);
-    run_transforms(c, r->rho.p, As, r->nl, r->V.p, As);
-    gram(c, r->V.p, As, r->nl, r->rho.p, rho_bytes(c) == sizeof(cx<float>), As, r->ridx.p, r->nr, As, r->o4.p);
+    const bool v32 = v_fp32(c);
+    run_transforms(c, r->rho.p, As, r->nl, r->V.p, As, v32);
+    gram(c, r->V.p, v32, As, r->nl, r->rho.p, rho_bytes(c) == sizeof(cx<float>), As, r->ridx.p, r->nr, As, r->o4.p);
     CL_CUDA(cudaMemcpyAsync(r->o4_host, r->o4.p, sizeof(double) * (4 * (size_t)r->nl * r->nr + 1),
                             cudaMemcpyDeviceToHost, c->stream));
 }
 
 void request_finish(cl_request* r, double* out) {
+    if (r->n_shards > 1) std::memset(out, 0, sizeof(double) * 2 * (size_t)r->n_int);
+    if (r->nl == 0) return;
     check_gram_slot(r->o4_host[4 * (size_t)r->nl * r->nr]);
     map_step_values(r->plan, r->slot, r->rcol, r->nr, r->o4_host, out);
 }
@@ -2211,6 +2290,11 @@ void request_finish(cl_request* r, double* out) {
 extern "C" {
 
 int cl_request_create(cl_ctx* c, int64_t n_int, const int16_t* spec, cl_request** out) {
+    return cl_request_create_shard(c, n_int, spec, 0, 1, out);
+}
+
+int cl_request_create_shard(cl_ctx* c, int64_t n_int, const int16_t* spec, int shard, int n_shards,
+                            cl_request** out) {
     if (out) *out = nullptr;
     cl_request* r = nullptr;
     int st = cl::guarded([&] {
@@ -2225,7 +2309,12 @@ int cl_request_create(cl_ctx* c, int64_t n_int, const int16_t* spec, cl_request*
         std::vector<std::array<int16_t, 4>> specs((size_t)n_int);
         for (int64_t i = 0; i < n_int; ++i)
             for (int k = 0; k < 4; ++k) specs[i][k] = spec[4 * i + k];
-        r->plan = cl::orient_steps(c->n_states, specs);
+        r->plan = shard_steps(cl::orient_steps(c->n_states, specs), c->n_states, shard, n_shards);
+        r->n_shards = n_shards;
+        if (r->plan.empty()) {  // a shard without densities: runs produce zeros
+            *out = r;
+            return;
+        }
         const int P = c->n_states * (c->n_states + 1) / 2;
         std::vector<int> is_left(P, 0), is_right(P, 0);
         r->slot.assign(P, -1);

@@ -96,11 +96,14 @@ __device__ __forceinline__ void mbar_drain(uint32_t a, uint32_t parity) {
         if (clock64() - t0 > TIMEOUT_CYCLES) return;
 }
 
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+// Tile (x = atom, y = row, z = part) of a [part][row][atom] operand; rows beyond the operand's
+// real rows are filled with zeros by the copy itself (nothing is read for them).
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint32_t mbar) {
     asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(mbar)
         : "memory");
 }
 
@@ -152,23 +155,22 @@ __device__ __forceinline__ float tf32_rn(float x) {
 
 // ---------------------------------------------------------------------------------------
 // Split pass: density d of `src` (row idx[d], or d; complex of S) over atoms [a0, a0 + na) ->
-//   dst[part][2d + {0: re, 1: im}][k], part 0 = hi, 1 = lo; rows >= 2n and k >= na are zero.
-// grid.y = rows_pad / 2 densities, grid.x strides over k.
+//   dst[part][2d + {0: re, 1: im}][k], part 0 = hi, 1 = lo, 2n rows a part; k >= na are zero.
+// grid.y = n densities, grid.x strides over k.  (The Gram's tiles are 128 rows; its copies fill
+// the rows beyond 2n with zeros, so no padding is stored.)
 // ---------------------------------------------------------------------------------------
 template <typename S>
 __global__ void __launch_bounds__(256) k_tf32_split(const cx<S>* __restrict__ src, long long stride,
-                                                    const int* __restrict__ idx, int n, int rows_pad,
-                                                    long long a0, long long na, long long k_pad,
-                                                    float* __restrict__ dst) {
+                                                    const int* __restrict__ idx, int n, long long a0,
+                                                    long long na, long long k_pad, float* __restrict__ dst) {
     const int d = blockIdx.y;
-    const long long plane = (long long)rows_pad * k_pad;
+    const long long plane = (long long)(2 * n) * k_pad;
     float* hre = dst + (long long)(2 * d) * k_pad;
     float* him = hre + k_pad;
-    const cx<S>* s = nullptr;
-    if (d < n) s = src + (long long)(idx ? idx[d] : d) * stride + a0;
+    const cx<S>* s = src + (long long)(idx ? idx[d] : d) * stride + a0;
     for (long long k = blockIdx.x * 256LL + threadIdx.x; k < k_pad; k += (long long)gridDim.x * 256) {
         double re = 0.0, im = 0.0;
-        if (s && k < na) {
+        if (k < na) {
             const cx<S> z = s[k];
             re = (double)z.re;
             im = (double)z.im;
@@ -182,13 +184,13 @@ __global__ void __launch_bounds__(256) k_tf32_split(const cx<S>* __restrict__ sr
 }
 
 // ---------------------------------------------------------------------------------------
-// The Gram.  grid = (rowsA / BM, rowsB / BN, splits); block z covers k-tiles
+// The Gram.  grid = (ceil(2 nl / BM), ceil(2 nr / BN), splits); block z covers k-tiles
 // [z * kt_per, min(kt_total, (z + 1) * kt_per)), never empty.  out4[l][r] += {ac, bd, ad, bc};
 // out4[4 * nl * nr] (as int) is set to 1 if any wait expired.
 // ---------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(THREADS, 1)
-    k_gram_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int rowsA,
-              int rowsB, int kt_total, int kt_per, int nl, int nr, double* __restrict__ out4) {
+    k_gram_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int kt_total,
+              int kt_per, int nl, int nr, double* __restrict__ out4) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -241,10 +243,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const uint32_t st = base + (uint32_t)(s * STAGE_BYTES);
                 mbar_expect_tx(bar(FULL + s), STAGE_BYTES);
                 const int x = kt * BK;
-                tma_load_2d(st, &mapA, x, m0, bar(FULL + s));
-                tma_load_2d(st + A_BYTES, &mapA, x, rowsA + m0, bar(FULL + s));
-                tma_load_2d(st + 2 * A_BYTES, &mapB, x, n0, bar(FULL + s));
-                tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mapB, x, rowsB + n0, bar(FULL + s));
+                tma_load_3d(st, &mapA, x, m0, 0, bar(FULL + s));
+                tma_load_3d(st + A_BYTES, &mapA, x, m0, 1, bar(FULL + s));
+                tma_load_3d(st + 2 * A_BYTES, &mapB, x, n0, 0, bar(FULL + s));
+                tma_load_3d(st + 2 * A_BYTES + B_BYTES, &mapB, x, n0, 1, bar(FULL + s));
                 ++issued;
                 if (++s == STAGES) {
                     s = 0;

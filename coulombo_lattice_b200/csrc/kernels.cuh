@@ -241,92 +241,76 @@ __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restri
 }
 
 // ---------------------------------------------------------------------------------------
-// Pair densities of the FP32 forms, computed in FP32 (the coefficients rounded once).  The
-// products of a request are grouped into blocks of up to 4 x 4: left states I (the higher
-// state of each product) by right states J; block entry prod[i*4 + j] is the density row of
-// (I[i], J[j]) or -1.  A block of PD32_THREADS threads stages `chunk` consecutive sorted atoms:
-// every used state's coefficients are read from HBM once, coalesced along each (state, atom)
-// row of orbitals, rounded to FP32 and stored [state][orbital][atom] (pitch chunk + 1); a thread
-// then takes one (atom, product block) item at a time, 8 shared-memory loads per orbital for 16
-// complex multiply-adds, and writes the block's densities (consecutive threads: consecutive
-// atoms, so the stores are coalesced).
+// Pair densities for requests over at most 8 states, summed in FP64 and rounded once to the
+// form's precision RT.  Two threads take one atom, each half of the products (t even / odd,
+// t = i (i + 1) / 2 + j for states i >= j in ascending order), over every orbital: per orbital
+// both load the NS used states' coefficients straight from HBM (the same addresses, one
+// request) and add conj(c_i) c_j to their products in FP64 registers; consecutive orbitals
+// share 32-byte sectors, so the second half of each sector is an L1 hit.  Rows prod[t] of rho.
+// No shared memory and no barrier: the loads of many warps stay in flight.
 // ---------------------------------------------------------------------------------------
-constexpr int PD32_THREADS = 128;
-struct PairBlock {
-    int I[4], J[4];  // used-state indices (a missing one repeats a valid state; its outputs are unused)
-    int prod[16];    // density row of (I[i], J[j]), -1: not requested
+struct PairTri {
+    int states[8];  // used states in ascending order (coefficient rows)
+    int prod[36];   // density row of product (i, j), i >= j, at i (i + 1) / 2 + j; -1: not requested
 };
 
-static __global__ void __launch_bounds__(PD32_THREADS) k_pair_density32(
-    const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb, const int* __restrict__ orig,
-    long long n_sorted, const PairBlock* __restrict__ blocks, int n_blocks, const int* __restrict__ states,
-    int n_used, int chunk, cx<float>* __restrict__ rho) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<float>* sc = reinterpret_cast<cx<float>*>(smem_raw);
-    const int pitch = chunk + 1;
-    const long long n_chunks = (n_sorted + chunk - 1) / chunk;
-    for (long long ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
-        const long long i0 = ci * chunk;
-        const int ca = (int)min((long long)chunk, n_sorted - i0);
-        // stage: orbital fastest over the threads (each (state, atom) row is contiguous in HBM)
-        // (eight loads in flight per thread before their stores)
-        const int total = n_used * ca * n_orb;
-        for (int e0 = threadIdx.x; e0 < total; e0 += 8 * PD32_THREADS) {
-            cx<double> v[8];
+template <int NS, int NP, int H, typename RT>
+__device__ __forceinline__ void pair_part(const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb,
+                                          long long atom, long long slot, long long n_sorted, const PairTri& tri,
+                                          cx<RT>* __restrict__ rho) {
+    constexpr int NT = NS * (NS + 1) / 2;
+    constexpr int NH = (NT - H + NP - 1) / NP;  // products t = NP k + H of this part
+    const cx<double>* rows[NS];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int e = e0 + k * PD32_THREADS;
-                if (e < total) {
-                    const int o = e % n_orb, r = e / n_orb;
-                    const int a = r % ca, su = r / ca;
-                    v[k] = coeff[((long long)states[su] * n_atoms + orig[i0 + a]) * n_orb + o];
+    for (int i = 0; i < NS; ++i) rows[i] = coeff + ((long long)tri.states[i] * n_atoms + atom) * n_orb;
+    double ar[NH > 0 ? NH : 1], ai[NH > 0 ? NH : 1];
+#pragma unroll
+    for (int k = 0; k < NH; ++k) ar[k] = ai[k] = 0.0;
+#pragma unroll 2
+    for (int o = 0; o < n_orb; ++o) {
+        cx<double> c[NS];
+#pragma unroll
+        for (int i = 0; i < NS; ++i) c[i] = rows[i][o];
+#pragma unroll
+        for (int i = 0; i < NS; ++i)
+#pragma unroll
+            for (int j = 0; j <= i; ++j) {
+                const int t = i * (i + 1) / 2 + j;
+                if (t % NP == H) {  // compile-time after unrolling
+                    ar[t / NP] += c[i].re * c[j].re + c[i].im * c[j].im;  // conj(c_i) c_j
+                    ai[t / NP] += c[i].re * c[j].im - c[i].im * c[j].re;
                 }
             }
+    }
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int e = e0 + k * PD32_THREADS;
-                if (e < total) {
-                    const int o = e % n_orb, r = e / n_orb;
-                    const int a = r % ca, su = r / ca;
-                    sc[(su * n_orb + o) * pitch + a] = mk((float)v[k].re, (float)v[k].im);
-                }
-            }
+    for (int k = 0; k < NH; ++k) {
+        const int p = tri.prod[NP * k + H];
+        if (p >= 0) rho[(long long)p * n_sorted + slot] = narrow<RT>(mk(ar[k], ai[k]));
+    }
+}
+
+// Block = 256 threads over pair_atoms_per_block(NS) atoms: the products are split into NP parts
+// (2, or 4 from 7 states on, to fit the FP64 sums in registers), each taken by its own warps (the
+// part is uniform over a warp: no predicated work).
+__host__ __device__ constexpr int pair_parts(int ns) { return ns >= 7 ? 4 : 2; }
+__host__ __device__ constexpr int pair_atoms_per_block(int ns) { return 256 / pair_parts(ns); }
+
+template <int NS, typename RT>
+__global__ void __launch_bounds__(256, 2) k_pair_density_reg(const cx<double>* __restrict__ coeff, long long n_atoms,
+                                                            int n_orb, const int* __restrict__ orig,
+                                                            long long n_sorted, const PairTri tri,
+                                                            cx<RT>* __restrict__ rho) {
+    constexpr int NP = pair_parts(NS), APB = pair_atoms_per_block(NS);
+    const int part = threadIdx.x / APB;
+    for (long long slot = (long long)blockIdx.x * APB + (threadIdx.x % APB); slot < n_sorted;
+         slot += (long long)gridDim.x * APB) {
+        const long long atom = orig[slot];
+        if (part == 0) pair_part<NS, NP, 0, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
+        else if (part == 1) pair_part<NS, NP, 1, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
+        else if constexpr (NP == 4) {
+            if (part == 2) pair_part<NS, NP, 2, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
+            else pair_part<NS, NP, 3, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
         }
-        __syncthreads();
-        for (int it = threadIdx.x; it < n_blocks * ca; it += PD32_THREADS) {
-            const int b = it / ca, a = it - b * ca;
-            const PairBlock& pb = blocks[b];
-            int ib[4], jb[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                ib[k] = pb.I[k] * n_orb * pitch + a;
-                jb[k] = pb.J[k] * n_orb * pitch + a;
-            }
-            float ar[16], ai[16];
-#pragma unroll
-            for (int k = 0; k < 16; ++k) ar[k] = ai[k] = 0.f;
-            for (int o = 0; o < n_orb; ++o) {
-                cx<float> l[4], r[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    l[k] = sc[ib[k] + o * pitch];
-                    r[k] = sc[jb[k] + o * pitch];
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {  // conj(l) r
-                        ar[i * 4 + j] += l[i].re * r[j].re + l[i].im * r[j].im;
-                        ai[i * 4 + j] += l[i].re * r[j].im - l[i].im * r[j].re;
-                    }
-            }
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const int p = pb.prod[k];
-                if (p >= 0) rho[(long long)p * n_sorted + i0 + a] = mk(ar[k], ai[k]);
-            }
-        }
-        __syncthreads();  // the stage is refilled for the next chunk
     }
 }
 

@@ -138,6 +138,49 @@ __global__ void k_sl_build_h(const double* __restrict__ ghat, int nx, int ny, in
     }
 }
 
+// 4-point Walsh-Hadamard transform y[c] = sum_a (-1)^popcount(c & a) x[a].
+template <typename T>
+__device__ __forceinline__ void wht4(const cx<T>* x, cx<T>* y) {
+    const cx<T> s01 = x[0] + x[1], d01 = x[0] - x[1], s23 = x[2] + x[3], d23 = x[2] - x[3];
+    y[0] = s01 + s23;
+    y[1] = d01 + d23;
+    y[2] = s01 - s23;
+    y[3] = d01 - d23;
+}
+
+// The zinc-blende mixing in Walsh-Hadamard form.  In the canonical class order the fcc offsets
+// f_0..f_3 form a group under addition mod 4 (f_a + f_b = f_{a xor b}, -f = f), so the 8 x 8
+// mixing matrix is [[A, C], [B, A]] with A_ab = alpha_{a^b}, B_ab = beta_{a^b}, C_ab =
+// conj(beta_{a^b}), alpha_k = H_{f_k} (real), beta_k = H_{f_k + (1,1,1)}.  The 4-point
+// Walsh-Hadamard transform W (W W = 4) diagonalises such matrices: with x^ = W x per half,
+//     u^_fcc = alpha^ x^_fcc + conj(beta^) x^_other,   u^_other = beta^ x^_fcc + alpha^ x^_other,
+// u = W u^ / 4, alpha^ = W alpha, beta^ = W beta.  This kernel turns the raw FP64 class kernels
+// (entries h of the table, e.g. alpha_k = Hraw[src[k]] conjugated if cj[k]) into
+// H[c] = alpha^_c / 4 and H[4 + c] = beta^_c / 4, rounded once to T.
+struct SlWht {
+    int src[8], cj[8];  // raw table entry (and conjugation) of alpha_0..3, beta_0..3
+};
+template <typename T>
+__global__ void k_sl_zb_wht(const cx<double>* __restrict__ Hraw, long long nq, SlWht w, cx<T>* __restrict__ H) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+         q += (long long)gridDim.x * blockDim.x) {
+        cx<double> v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            v[k] = Hraw[w.src[k] * nq + q];
+            if (w.cj[k]) v[k].im = -v[k].im;
+        }
+        cx<double> a[4], b[4];
+        wht4(v, a);
+        wht4(v + 4, b);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            H[c * nq + q] = mk(T(0.25 * a[c].re), T(0));  // alpha is real (self-conjugate residues)
+            H[(4 + c) * nq + q] = mk(T(0.25 * b[c].re), T(0.25 * b[c].im));
+        }
+    }
+}
+
 // V[p][i] = widen(src[p][i]) for the densities p = blockIdx.y (FP32 forms: the values at the
 // atoms from the inverse passes, into the FP64 potentials the reductions read).
 template <typename T>
@@ -217,8 +260,7 @@ __global__ void __launch_bounds__(kSlMaxClasses * L * ColShape<R1, R2>::P, 1)
         phxy[i] = (s < S && cc < nxy) ? phxy_g[(long long)s * nxy + cc] : mk(T(0), T(0));
     }
     // the residue kernels of this thread's mixing points, for every density (zinc-blende)
-    constexpr SlTable zt = zb_table();
-    constexpr int NHR = ZB ? zt.nh : 1;
+    constexpr int NHR = ZB ? 8 : 1;
     cx<T> hv[NPT][NHR];
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
@@ -297,25 +339,42 @@ __global__ void __launch_bounds__(kSlMaxClasses * L * ColShape<R1, R2>::P, 1)
                         xt[b] = mk(T(0), T(0));
                     }
                 }
+                if constexpr (ZB) {
+                    // Walsh-Hadamard form (see k_sl_build_h): fcc classes 0-3, fcc + (1,1,1) 4-7;
+                    // hv = alpha^/4 (real, 0-3) and beta^/4 (4-7) per character
+                    cx<T> xf[4], xa[4];
+                    wht4(xt, xf);
+                    wht4(xt + 4, xa);
+                    cx<T> uf[4], ua[4];
 #pragma unroll
-                for (int a = 0; a < kSlMaxClasses; ++a) {
-                    if (a >= S) continue;
-                    cx<T> u = mk(T(0), T(0));
-#pragma unroll
-                    for (int b = 0; b < kSlMaxClasses; ++b) {
-                        if (b >= S) continue;
-                        cx<T> g;
-                        if constexpr (ZB) {
-                            g = hv[j][zt.h[a * kSlMaxClasses + b] < NHR ? zt.h[a * kSlMaxClasses + b] : 0];
-                            if (zt.cj[a * kSlMaxClasses + b]) g.im = -g.im;
-                        } else {
-                            g = H[mix.h[a * kSlMaxClasses + b] * h_stride + (long long)k * nxy + cc];
-                            if (mix.cj[a * kSlMaxClasses + b]) g.im = -g.im;
-                        }
-                        u.re += g.re * xt[b].re - g.im * xt[b].im;
-                        u.im += g.re * xt[b].im + g.im * xt[b].re;
+                    for (int c = 0; c < 4; ++c) {
+                        const T al = hv[j][c].re;
+                        const cx<T> be = hv[j][4 + c];
+                        uf[c] = mk(al * xf[c].re + be.re * xa[c].re + be.im * xa[c].im,
+                                   al * xf[c].im + be.re * xa[c].im - be.im * xa[c].re);  // + conj(be) xa
+                        ua[c] = mk(al * xa[c].re + be.re * xf[c].re - be.im * xf[c].im,
+                                   al * xa[c].im + be.re * xf[c].im + be.im * xf[c].re);  // + be xf
                     }
-                    sm[k * LPM + a * L + l] = cmulc(u, tb[a]);
+                    cx<T> u8[8];
+                    wht4(uf, u8);
+                    wht4(ua, u8 + 4);
+#pragma unroll
+                    for (int a = 0; a < kSlMaxClasses; ++a) sm[k * LPM + a * L + l] = cmulc(u8[a], tb[a]);
+                } else {
+#pragma unroll
+                    for (int a = 0; a < kSlMaxClasses; ++a) {
+                        if (a >= S) continue;
+                        cx<T> u = mk(T(0), T(0));
+#pragma unroll
+                        for (int b = 0; b < kSlMaxClasses; ++b) {
+                            if (b >= S) continue;
+                            cx<T> g = H[mix.h[a * kSlMaxClasses + b] * h_stride + (long long)k * nxy + cc];
+                            if (mix.cj[a * kSlMaxClasses + b]) g.im = -g.im;
+                            u.re += g.re * xt[b].re - g.im * xt[b].im;
+                            u.im += g.re * xt[b].im + g.im * xt[b].re;
+                        }
+                        sm[k * LPM + a * L + l] = cmulc(u, tb[a]);
+                    }
                 }
             }
         }

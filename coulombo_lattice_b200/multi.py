@@ -1,6 +1,12 @@
 """Multi-GPU decomposition of the integral path (one process per GPU, torch.distributed).
 
-Two ways to spread work over ranks:
+Three ways to spread work over ranks:
+
+* One request over several GPUs, by prepared densities (both forms): the plan's left
+  densities are dealt round-robin to the ranks (cl_compute_shard); each rank transforms its
+  own left densities, forms every right density and returns the integrals of its steps, zeros
+  elsewhere.  One all-reduce (sum, FP64) of the integral vector combines them -- the
+  counterpart of the reference's MPI_Reduce of every calculate() (CoulombCalculator.cpp:170).
 
 * One request over several GPUs: the integrals are sums over the 8 rounds kappa
   (CoulombCalculator.cpp:105-163 accumulates V_ += Ftemp round by round), so rank r takes the
@@ -49,6 +55,19 @@ def compute_sharded(compute_rounds, specs, group=None, device="cpu"):
         part = np.asarray(compute_rounds(specs, mask), dtype=np.complex128)
     else:
         part = np.zeros(len(specs), dtype=np.complex128)
+    return allreduce_complex(part, group=group, device=device)
+
+
+def compute_density_sharded(compute_shard, specs, group=None, device="cpu"):
+    """Full integrals of `specs` from this rank's shard of the left densities.
+
+    compute_shard(specs, shard, n_shards) -> complex vector with this shard's integrals and
+    zeros elsewhere (on a GPU rank: CoulombCalculator.compute_shard); every rank calls this with
+    the same specs."""
+    import torch.distributed as dist
+    rank = dist.get_rank(group)
+    world = dist.get_world_size(group)
+    part = np.asarray(compute_shard(specs, rank, world), dtype=np.complex128)
     return allreduce_complex(part, group=group, device=device)
 
 

@@ -150,6 +150,15 @@ int cl_compute_rounds(cl_ctx* ctx, int64_t n_int, const int16_t* spec, int round
  * counterpart (the reference always runs the 8 rounds, CoulombCalculator.cpp:105-163). */
 int cl_form_info(cl_ctx* ctx, int info[8]);
 
+/* Same as cl_compute for one shard of the request: the prepared (left) densities of the plan, in
+ * ascending product order, are dealt round-robin to n_shards shards, and out[i] holds integral i
+ * when its left density belongs to shard `shard`, zero otherwise.  The shards' outputs add up to
+ * cl_compute's, so n_shards GPUs (one process each) run one shard each and combine them with one
+ * all-reduce (sum) of out: the multi-GPU unit of both forms (the sub-lattice forms have no
+ * rounds).  Right densities are formed on every shard.  No reference counterpart: the reference
+ * splits each grid over MPI ranks and reduces every calculate() (CoulombCalculator.cpp:165-172). */
+int cl_compute_shard(cl_ctx* ctx, int64_t n_int, const int16_t* spec, int shard, int n_shards, double* out);
+
 /* Device time in milliseconds of the phases of the last cl_compute / cl_potentials:
  * t[0] pair densities, t[1] transforms (all rounds), t[2] reductions, t[3] total. */
 int cl_last_timings(cl_ctx* ctx, double t[4]);
@@ -194,6 +203,10 @@ typedef struct cl_batch cl_batch;
  * is what lets batches be captured in a CUDA graph.  Replaces, for repeated requests over the
  * same states, the per-call planning of coulombo.cpp:121-151. */
 int cl_request_create(cl_ctx* ctx, int64_t n_int, const int16_t* spec, cl_request** out);
+/* A prepared request of one shard (see cl_compute_shard): runs write zeros for the other shards'
+ * integrals; cl_request_create is shard 0 of 1. */
+int cl_request_create_shard(cl_ctx* ctx, int64_t n_int, const int16_t* spec, int shard, int n_shards,
+                            cl_request** out);
 int cl_request_run(cl_request* req, double* out /* [n_int]{re,im} */);
 void cl_request_destroy(cl_request* req);
 

@@ -43,6 +43,7 @@ def test_usage(tmp_path):
     (["--atoms=X.3d", "--orbitals=0", "e1.dat"], "invalid value for orbitals"),
     (["--atoms=X.3d", "--skip-lines=0", "e1.dat"], "invalid value for skip-lines"),
     (["--atoms=X.3d", "--threads-per-node=0", "e1.dat"], "invalid value for threads-per-node"),
+    (["--atoms=X.3d", "--method=fast", "e1.dat"], "invalid value for method: fast"),
     (["--atoms=X.3d", "--orbitals=10", "--skip-lines=1", "e1.dat", "h1.dat"],
      "hole states must appear before electron states"),
     (["--atoms=X.3d", "--orbitals=10", "--skip-lines=1", "x1.dat"], "invalid state file name: x1.dat"),

@@ -45,14 +45,15 @@ def test_example_potentials(tmp_path):
     assert np.abs(got - V).max() <= 1e-10 * np.abs(V).max()
 
 
+@pytest.mark.parametrize("method", ["rounds", "sublattice"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_synthetic_outputs(tmp_path, precision):
+def test_synthetic_outputs(tmp_path, precision, method):
     d = synth.build("c1", cells=(4, 4, 4))
     names = synth.write_inputs(str(tmp_path), d)
     out = tmp_path / "out"
     out.mkdir()
     run(COULOMBO, ["--atoms=X.3d", "--dielectric=10.89", "--orbitals=10", "--skip-lines=1",
-                   "--integrals=eeee,hhhh,ehhe,eheh", "--output-dir=out", "--precision=" + precision] + names, tmp_path)
+                   "--integrals=eeee,hhhh,ehhe,eheh", "--output-dir=out", "--precision=" + precision, "--method=" + method] + names, tmp_path)
     specs = H.enumerate_integrals(H.Pattern("eeee,hhhh,ehhe,eheh", 2), 4)
     g = H.detect_grid(np.loadtxt(tmp_path / "X.3d"))
     states = [H.load_state(str(tmp_path / n), len(g["cells"]), 10, 1) for n in names]
