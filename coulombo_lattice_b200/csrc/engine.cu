@@ -1387,8 +1387,8 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
             if (i < j) cl::fail(CL_ERR_STATE, "pair density with its lower state first");
             ps.tri.prod[i * (i + 1) / 2 + j] = p;
         }
-        const int apb = clk::pair_atoms_per_block((int)used.size());
-        ps.grid_reg = (int)std::max<long long>(1, std::min<long long>((c->n_sorted + apb - 1) / apb, 148LL * 2 * 8));
+        ps.grid_reg = (int)std::max<long long>(
+            1, std::min<long long>((c->n_sorted + clk::kPairAtoms - 1) / clk::kPairAtoms, 148LL * 2 * 4));
     }
     ps.states.upload(used.data(), used.size(), c->stream);
     ps.n_used = (int)used.size();
@@ -1438,7 +1438,9 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
         cx<double>* out = static_cast<cx<double>*>(rho);
         const auto go = [&](auto ns) {
             constexpr int NS = decltype(ns)::value;
-            clk::k_pair_density_reg<NS, double><<<ps.grid_reg, 256, 0, c->stream>>>(
+            const size_t smem = 2 * sizeof(cx<double>) * clk::pair_stage_elems(NS);
+            ensure_smem(clk::k_pair_density_reg<NS, double>, smem);
+            clk::k_pair_density_reg<NS, double><<<ps.grid_reg, 256, smem, c->stream>>>(
                 c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
         };
         with_states(ps.n_used, go);
@@ -1451,7 +1453,9 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
         cx<float>* out = static_cast<cx<float>*>(rho);
         const auto go = [&](auto ns) {
             constexpr int NS = decltype(ns)::value;
-            clk::k_pair_density_reg<NS, float><<<ps.grid_reg, 256, 0, c->stream>>>(
+            const size_t smem = 2 * sizeof(cx<double>) * clk::pair_stage_elems(NS);
+            ensure_smem(clk::k_pair_density_reg<NS, float>, smem);
+            clk::k_pair_density_reg<NS, float><<<ps.grid_reg, 256, smem, c->stream>>>(
                 c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
         };
         with_states(ps.n_used, go);

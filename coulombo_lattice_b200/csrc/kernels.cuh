@@ -242,74 +242,118 @@ __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restri
 
 // ---------------------------------------------------------------------------------------
 // Pair densities for requests over at most 8 states, summed in FP64 and rounded once to the
-// form's precision RT.  Two threads take one atom, each half of the products (t even / odd,
-// t = i (i + 1) / 2 + j for states i >= j in ascending order), over every orbital: per orbital
-// both load the NS used states' coefficients straight from HBM (the same addresses, one
-// request) and add conj(c_i) c_j to their products in FP64 registers; consecutive orbitals
-// share 32-byte sectors, so the second half of each sector is an L1 hit.  Rows prod[t] of rho.
-// No shared memory and no barrier: the loads of many warps stay in flight.
+// form's precision RT; products t = i (i + 1) / 2 + j of states i >= j (ascending order) go to
+// rows prod[t] of rho.
 // ---------------------------------------------------------------------------------------
 struct PairTri {
     int states[8];  // used states in ascending order (coefficient rows)
     int prod[36];   // density row of product (i, j), i >= j, at i (i + 1) / 2 + j; -1: not requested
 };
 
-template <int NS, int NP, int H, typename RT>
-__device__ __forceinline__ void pair_part(const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb,
-                                          long long atom, long long slot, long long n_sorted, const PairTri& tri,
-                                          cx<RT>* __restrict__ rho) {
+// Block = 256 threads over 64 atoms: the products are split into four parts (t mod 4), each
+// taken by two warps (the part is uniform over a warp: no predicated work; nine FP64 sums at most
+// per thread).  The coefficients are staged through shared memory four orbitals at a time: per
+// (state, atom) the 64 contiguous bytes of those orbitals are copied with 16-byte cp.async
+// (coalesced; the next slice is in flight while this one is used), at an 80-byte pitch per atom
+// so that threads on consecutive atoms read distinct banks.  Every coefficient leaves HBM once and
+// each part reads the slice from shared memory.  The barriers are in the kernel body, reached by
+// every thread; only the arithmetic is specialised per part.
+constexpr int kPairParts = 4;
+constexpr int kPairAtoms = 256 / kPairParts;  // atoms per block and step
+constexpr int kPairOrbSlice = 4;              // orbitals per stage
+__host__ __device__ constexpr int pair_stage_elems(int ns) { return ns * kPairAtoms * (kPairOrbSlice + 1); }
+
+template <int NS, int H>
+__device__ __forceinline__ void pair_accumulate(const cx<double>* __restrict__ st, int a, double* ar, double* ai) {
     constexpr int NT = NS * (NS + 1) / 2;
-    constexpr int NH = (NT - H + NP - 1) / NP;  // products t = NP k + H of this part
-    const cx<double>* rows[NS];
 #pragma unroll
-    for (int i = 0; i < NS; ++i) rows[i] = coeff + ((long long)tri.states[i] * n_atoms + atom) * n_orb;
-    double ar[NH > 0 ? NH : 1], ai[NH > 0 ? NH : 1];
-#pragma unroll
-    for (int k = 0; k < NH; ++k) ar[k] = ai[k] = 0.0;
-#pragma unroll 2
-    for (int o = 0; o < n_orb; ++o) {
+    for (int o = 0; o < kPairOrbSlice; ++o) {
         cx<double> c[NS];
 #pragma unroll
-        for (int i = 0; i < NS; ++i) c[i] = rows[i][o];
+        for (int i = 0; i < NS; ++i) c[i] = st[(i * kPairAtoms + a) * (kPairOrbSlice + 1) + o];
 #pragma unroll
         for (int i = 0; i < NS; ++i)
 #pragma unroll
             for (int j = 0; j <= i; ++j) {
                 const int t = i * (i + 1) / 2 + j;
-                if (t % NP == H) {  // compile-time after unrolling
-                    ar[t / NP] += c[i].re * c[j].re + c[i].im * c[j].im;  // conj(c_i) c_j
-                    ai[t / NP] += c[i].re * c[j].im - c[i].im * c[j].re;
+                if (t % kPairParts == H && t < NT) {  // compile-time after unrolling
+                    ar[t / kPairParts] += c[i].re * c[j].re + c[i].im * c[j].im;  // conj(c_i) c_j
+                    ai[t / kPairParts] += c[i].re * c[j].im - c[i].im * c[j].re;
                 }
             }
     }
+}
+
+template <int NS, int H, typename RT>
+__device__ __forceinline__ void pair_store(const PairTri& tri, const double* ar, const double* ai, long long slot,
+                                           long long n_sorted, cx<RT>* __restrict__ rho) {
+    constexpr int NT = NS * (NS + 1) / 2, NH = (NT - H + kPairParts - 1) / kPairParts;
 #pragma unroll
     for (int k = 0; k < NH; ++k) {
-        const int p = tri.prod[NP * k + H];
+        const int p = tri.prod[kPairParts * k + H];
         if (p >= 0) rho[(long long)p * n_sorted + slot] = narrow<RT>(mk(ar[k], ai[k]));
     }
 }
-
-// Block = 256 threads over pair_atoms_per_block(NS) atoms: the products are split into NP parts
-// (2, or 4 from 7 states on, to fit the FP64 sums in registers), each taken by its own warps (the
-// part is uniform over a warp: no predicated work).
-__host__ __device__ constexpr int pair_parts(int ns) { return ns >= 7 ? 4 : 2; }
-__host__ __device__ constexpr int pair_atoms_per_block(int ns) { return 256 / pair_parts(ns); }
 
 template <int NS, typename RT>
 __global__ void __launch_bounds__(256, 2) k_pair_density_reg(const cx<double>* __restrict__ coeff, long long n_atoms,
                                                             int n_orb, const int* __restrict__ orig,
                                                             long long n_sorted, const PairTri tri,
                                                             cx<RT>* __restrict__ rho) {
-    constexpr int NP = pair_parts(NS), APB = pair_atoms_per_block(NS);
-    const int part = threadIdx.x / APB;
-    for (long long slot = (long long)blockIdx.x * APB + (threadIdx.x % APB); slot < n_sorted;
-         slot += (long long)gridDim.x * APB) {
-        const long long atom = orig[slot];
-        if (part == 0) pair_part<NS, NP, 0, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
-        else if (part == 1) pair_part<NS, NP, 1, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
-        else if constexpr (NP == 4) {
-            if (part == 2) pair_part<NS, NP, 2, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
-            else pair_part<NS, NP, 3, RT>(coeff, n_atoms, n_orb, atom, slot, n_sorted, tri, rho);
+    constexpr int NT = NS * (NS + 1) / 2, NHM = (NT + kPairParts - 1) / kPairParts;
+    constexpr int SE = pair_stage_elems(NS);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<double>* sm = reinterpret_cast<cx<double>*>(smem_raw);
+    const int part = threadIdx.x / kPairAtoms;
+    const int a = threadIdx.x % kPairAtoms;
+    const int n_slices = (n_orb + kPairOrbSlice - 1) / kPairOrbSlice;
+    // the copies of one stage: NS states x 64 atoms x 4 orbitals, 16 bytes each
+    const auto issue = [&](long long a0, int slice, cx<double>* st) {
+        const int na = (int)min((long long)kPairAtoms, n_sorted - a0);
+        for (int e = threadIdx.x; e < NS * kPairAtoms * kPairOrbSlice; e += 256) {
+            const int o = e % kPairOrbSlice, r = e / kPairOrbSlice;
+            const int at = r % kPairAtoms, i = r / kPairAtoms;
+            const int orb = slice * kPairOrbSlice + o;
+            cx<double>* dst = st + (i * kPairAtoms + at) * (kPairOrbSlice + 1) + o;
+            if (at < na && orb < n_orb)
+                pd_cp_async16(dst, coeff + ((long long)tri.states[i] * n_atoms + orig[a0 + at]) * n_orb + orb);
+            else
+                *dst = mk(0.0, 0.0);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    const long long gstep = (long long)gridDim.x * kPairAtoms;
+    long long a0 = (long long)blockIdx.x * kPairAtoms;
+    int stage = 0;
+    if (a0 < n_sorted) issue(a0, 0, sm);
+    for (; a0 < n_sorted; a0 += gstep) {
+        double ar[NHM], ai[NHM];
+#pragma unroll
+        for (int k = 0; k < NHM; ++k) ar[k] = ai[k] = 0.0;
+        for (int sl = 0; sl < n_slices; ++sl) {
+            // next stage: this group's next slice, or the next group's first one
+            const long long na0 = sl + 1 < n_slices ? a0 : a0 + gstep;
+            if (na0 < n_sorted) {
+                issue(na0, sl + 1 < n_slices ? sl + 1 : 0, sm + (stage ^ 1) * SE);
+                asm volatile("cp.async.wait_group 1;\n" ::);
+            } else {
+                asm volatile("cp.async.wait_group 0;\n" ::);
+            }
+            __syncthreads();
+            const cx<double>* st = sm + stage * SE;
+            if (part == 0) pair_accumulate<NS, 0>(st, a, ar, ai);
+            else if (part == 1) pair_accumulate<NS, 1>(st, a, ar, ai);
+            else if (part == 2) pair_accumulate<NS, 2>(st, a, ar, ai);
+            else pair_accumulate<NS, 3>(st, a, ar, ai);
+            __syncthreads();  // the stage is refilled two slices on
+            stage ^= 1;
+        }
+        const long long slot = a0 + a;
+        if (slot < n_sorted) {
+            if (part == 0) pair_store<NS, 0, RT>(tri, ar, ai, slot, n_sorted, rho);
+            else if (part == 1) pair_store<NS, 1, RT>(tri, ar, ai, slot, n_sorted, rho);
+            else if (part == 2) pair_store<NS, 2, RT>(tri, ar, ai, slot, n_sorted, rho);
+            else pair_store<NS, 3, RT>(tri, ar, ai, slot, n_sorted, rho);
         }
     }
 }
