@@ -710,6 +710,13 @@ def run_ours(args):
         e2e_ms = e2e_device_ms = float("nan")
         call_ms = call_dev_ms = [float("nan")]
 
+    # ---- the integral files (coulombo.cpp:213-262), written on the host threads -----------
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        t0 = time.perf_counter()
+        cl.write_integrals(os.path.join(td, ""), d["holes"], n - d["holes"], specs, v32)
+        export_ms = 1e3 * (time.perf_counter() - t0)
+
     # ---- roofline of the dominant kernel --------------------------------------------------
     peak, peak_kind = measured_peaks()
     fft_classes = {k: v for k, v in prof.items() if k in TRANSFORM_CLASSES}
@@ -752,6 +759,9 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_of(args, n_int),
         "details": {"form": FORM_TEXT[HEADLINE_MODE], "form_info": form_info,
+                    "export_ms": export_ms,
+                    "export": "cl_write_integrals of the request's %d integrals (the XXXX.txt files), wall clock, "
+                              "outside value and e2e" % n_int,
                     "l2": "inputs larger than L2 (126 MB): %.0f MB of transformed grids per request, "
                           "streamed in chunks" % buf_mb, "prepared_densities": n_prepared,
                     "init_ms_kernel_build": init_ms, "wall_ms_per_step": wall_ms / args.steps,

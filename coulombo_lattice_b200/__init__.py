@@ -93,6 +93,7 @@ SIGNATURES = [
     ("cl_enumerate_integrals", _i, [ctypes.c_char_p, _i, _i, _P(_i64), _P(ctypes.c_int16), _i64]),
     ("cl_vertex_cover", _i, [_i, _i64, _P(ctypes.c_int32), _P(ctypes.c_uint8)]),
     ("cl_plan", _i, [_i, _i64, _P(ctypes.c_int16), _P(ctypes.c_int32)]),
+    ("cl_write_integrals", _i, [ctypes.c_char_p, _i, _i, _i64, _P(ctypes.c_int16), _P(_d), _i]),
 ]
 
 
@@ -168,6 +169,14 @@ def plan(n_inputs, specs):
     steps = np.empty((s.shape[0], 5), dtype=np.int32)
     _check(lib().cl_plan(n_inputs, s.shape[0], _ptr(s, ctypes.c_int16), _ptr(steps, ctypes.c_int32)))
     return steps
+
+
+def write_integrals(out_prefix, n_holes, n_electrons, specs, values, threads=0):
+    """cl_write_integrals: the XXXX.txt files of coulombo.cpp:213-262 (out_prefix + class + '.txt')."""
+    s = np.ascontiguousarray(np.asarray(specs, dtype=np.int16).reshape(-1, 4))
+    v = np.ascontiguousarray(np.asarray(values, dtype=np.complex128)).view(np.float64)
+    _check(lib().cl_write_integrals(str(out_prefix).encode(), int(n_holes), int(n_electrons), s.shape[0],
+                                    _ptr(s, ctypes.c_int16), _ptr(v), int(threads)))
 
 
 def autotune_report():

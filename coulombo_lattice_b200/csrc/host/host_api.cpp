@@ -2,8 +2,12 @@
 #include <cstring>
 #include <string>
 
+#include <stdexcept>
+#include <vector>
+
 #include "coulombo_lattice.h"
 #include "host_logic.hpp"
+#include "io.hpp"
 #include "status.hpp"
 
 namespace cl {
@@ -97,6 +101,20 @@ int cl_plan(int n_inputs, int64_t n_int, const int16_t* spec, int32_t* steps) {
             steps[5 * i + 2] = plan[i].left.conjugate;
             steps[5 * i + 3] = plan[i].right.product;
             steps[5 * i + 4] = plan[i].right.conjugate;
+        }
+    });
+}
+
+int cl_write_integrals(const char* out_prefix, int n_holes, int n_electrons, int64_t n_int, const int16_t* spec,
+                       const double* values, int threads) {
+    return cl::guarded([&] {
+        if (!out_prefix || n_holes < 0 || n_electrons < 0 || n_int < 0 || (n_int && (!spec || !values)))
+            cl::fail(CL_ERR_ARGUMENT, "invalid arguments");
+        std::vector<int16_t> specs(spec, spec + 4 * n_int);
+        try {
+            clio::write_integrals(out_prefix, specs, values, n_holes, n_electrons, threads);
+        } catch (const std::runtime_error& e) {
+            cl::fail(CL_ERR_ARGUMENT, "%s", e.what());
         }
     });
 }

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <thread>
+#include <unordered_map>
 
 namespace clio {
 
@@ -214,57 +215,89 @@ void Timer::start(const char* msg) {
 }
 
 // ---------------------------------------------------------------------------------------
-// coulombo.cpp:213-262
+// coulombo.cpp:213-262: one file per e/h class with values, rows in (ni, nj, nk, nl) order with
+// the hole numbering reversed, "%2d %2d %2d %2d   %17.14f %17.14f\n".  The lines of a class are
+// formatted in parallel chunks of (ni, nj) on the host threads and written in order; a class
+// file is created only when it has a line, as the reference opens it at its first line.
 // ---------------------------------------------------------------------------------------
 void write_integrals(const std::string& out_prefix, const std::vector<int16_t>& specs, const double* values,
-                     int n_holes, int n_electrons) {
+                     int n_holes, int n_electrons, int threads) {
     const size_t n_int = specs.size() / 4;
-    std::map<std::array<int16_t, 4>, size_t> table;
-    for (size_t i = 0; i < n_int; ++i)
-        table[{specs[4 * i], specs[4 * i + 1], specs[4 * i + 2], specs[4 * i + 3]}] = i;
+    const int n = n_holes + n_electrons;
+    // spec -> integral index: a flat table while n^4 is small, else a hash map
+    const unsigned long long n4 = (unsigned long long)n * n * n * n;
+    const bool flat = n4 <= (1ull << 25);
+    std::vector<int64_t> table(flat ? (size_t)n4 : 0, -1);
+    std::unordered_map<unsigned long long, int64_t> hashed;
+    const auto key_of = [n](int a, int b, int c, int d) {
+        return (((unsigned long long)(a - 1) * n + (b - 1)) * n + (c - 1)) * n + (d - 1);
+    };
+    for (size_t i = 0; i < n_int; ++i) {
+        const int16_t* sp = &specs[4 * i];
+        for (int q = 0; q < 4; ++q)
+            if (sp[q] < 1 || sp[q] > n) throwfr("integral index out of range");
+        const unsigned long long k = key_of(sp[0], sp[1], sp[2], sp[3]);
+        if (flat)
+            table[k] = (int64_t)i;
+        else
+            hashed[k] = (int64_t)i;
+    }
+    const auto find = [&](unsigned long long k) -> int64_t {
+        if (flat) return table[k];
+        auto it = hashed.find(k);
+        return it == hashed.end() ? -1 : it->second;
+    };
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     char core[5];
     core[4] = 0;
     for (int ti = 0; ti < 2; ++ti)
         for (int tj = 0; tj < 2; ++tj)
             for (int tk = 0; tk < 2; ++tk)
                 for (int tl = 0; tl < 2; ++tl) {
-                    FILE* file = nullptr;
                     const int t[4] = {ti, tj, tk, tl};
                     int cnt[4];
                     for (int q = 0; q < 4; ++q) {
                         core[q] = t[q] ? 'e' : 'h';
                         cnt[q] = t[q] ? n_electrons : n_holes;
                     }
-                    std::string buf;
-                    for (int ni = 1; ni <= cnt[0]; ++ni)
-                        for (int nj = 1; nj <= cnt[1]; ++nj)
+                    const long long units = (long long)cnt[0] * cnt[1];  // (ni, nj) pairs
+                    if (units == 0 || cnt[2] == 0 || cnt[3] == 0) continue;
+                    const int nt = (int)std::min<long long>(threads, units);
+                    std::vector<std::string> bufs((size_t)nt);
+                    const auto work = [&](int w) {
+                        std::string& buf = bufs[(size_t)w];
+                        char line[128];
+                        for (long long u = units * w / nt; u < units * (w + 1) / nt; ++u) {
+                            const int ni = (int)(u / cnt[1]) + 1, nj = (int)(u % cnt[1]) + 1;
                             for (int nk = 1; nk <= cnt[2]; ++nk)
                                 for (int nl = 1; nl <= cnt[3]; ++nl) {
                                     const int idx[4] = {ni, nj, nk, nl};
-                                    std::array<int16_t, 4> key;
+                                    int sp[4];
                                     for (int q = 0; q < 4; ++q)
-                                        key[q] = (int16_t)(t[q] ? n_holes + idx[q] : n_holes + 1 - idx[q]);
-                                    auto it = table.find(key);
-                                    if (it == table.end()) continue;
-                                    if (!file) {
-                                        std::string path = out_prefix + core + ".txt";
-                                        file = std::fopen(path.c_str(), "w");
-                                        if (!file) throwfr("cannot open file %s for writing", path.c_str());
-                                    }
-                                    char line[128];
-                                    int len = std::snprintf(line, sizeof line, "%2d %2d %2d %2d   %17.14f %17.14f\n", ni,
-                                                            nj, nk, nl, values[2 * it->second],
-                                                            values[2 * it->second + 1]);
+                                        sp[q] = t[q] ? n_holes + idx[q] : n_holes + 1 - idx[q];
+                                    const int64_t i = find(key_of(sp[0], sp[1], sp[2], sp[3]));
+                                    if (i < 0) continue;
+                                    const int len = std::snprintf(line, sizeof line, "%2d %2d %2d %2d   %17.14f %17.14f\n",
+                                                                  ni, nj, nk, nl, values[2 * i], values[2 * i + 1]);
                                     buf.append(line, (size_t)len);
-                                    if (buf.size() > (1u << 20)) {
-                                        std::fwrite(buf.data(), 1, buf.size(), file);
-                                        buf.clear();
-                                    }
                                 }
-                    if (file) {
-                        std::fwrite(buf.data(), 1, buf.size(), file);
-                        std::fclose(file);
+                        }
+                    };
+                    if (nt == 1) {
+                        work(0);
+                    } else {
+                        std::vector<std::thread> pool;
+                        for (int w = 0; w < nt; ++w) pool.emplace_back(work, w);
+                        for (auto& th : pool) th.join();
                     }
+                    bool any = false;
+                    for (const auto& b2 : bufs) any = any || !b2.empty();
+                    if (!any) continue;
+                    const std::string path = out_prefix + core + ".txt";
+                    FILE* file = std::fopen(path.c_str(), "w");
+                    if (!file) throwfr("cannot open file %s for writing", path.c_str());
+                    for (const auto& b2 : bufs) std::fwrite(b2.data(), 1, b2.size(), file);
+                    std::fclose(file);
                 }
 }
 

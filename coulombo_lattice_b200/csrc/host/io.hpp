@@ -65,8 +65,8 @@ private:
 [[noreturn]] void throwfr(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
 
 // Writes the XXXX.txt files of coulombo.cpp:213-262.  specs are 1-based input indices,
-// values {re, im}; holes are numbered in reverse in the files.
+// values {re, im}; holes are numbered in reverse in the files.  threads <= 0: all host threads.
 void write_integrals(const std::string& out_prefix, const std::vector<int16_t>& specs, const double* values,
-                     int n_holes, int n_electrons);
+                     int n_holes, int n_electrons, int threads = 0);
 
 }  // namespace clio

@@ -92,7 +92,6 @@ bool xfwd(cudaStream_t s, Variant v, const cx<T>* rho, long long rho_stride, con
                 const auto launch = [&](auto pad) {
                     constexpr int LR = decltype(lines)::value;
                     constexpr bool PAD = decltype(pad)::value;
-                    constexpr int N = Tag::r1 * Tag::r2;
                     constexpr int Q = Tag::r1 > Tag::r2 ? Tag::r1 : Tag::r2;
                     auto kern = clk::k_xfwd_rf<T, Tag::r1, Tag::r2, LR, PAD>;
                     const size_t smem =

@@ -272,6 +272,14 @@ int cl_vertex_cover(int n_vertices, int64_t n_edges, const int32_t* edges, uint8
  * right, rconj} in execution order.  Replaces MasterPlanner (src/Planner.hpp:71-117). */
 int cl_plan(int n_inputs, int64_t n_int, const int16_t* spec, int32_t* steps /* [n_int][5] */);
 
+/* Writes the XXXX.txt files of the integrals: one file per electron/hole class that has values,
+ * named out_prefix + class + ".txt", rows "%2d %2d %2d %2d   %17.14f %17.14f\n" in (ni, nj, nk,
+ * nl) order with the hole numbering reversed.  The lines are formatted on `threads` host threads
+ * (<= 0: all) and written in order, byte for byte as the serial loop of the reference.
+ * Replaces coulombo.cpp:213-262. */
+int cl_write_integrals(const char* out_prefix, int n_holes, int n_electrons, int64_t n_int, const int16_t* spec,
+                       const double* values, int threads);
+
 #ifdef __cplusplus
 }
 #endif

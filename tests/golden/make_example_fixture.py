@@ -75,5 +75,5 @@ def write_example(directory):
 
 
 if __name__ == "__main__":
-    build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    build(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CL_REFERENCE_ROOT", os.path.join(os.sep, "root", "reference")))
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
