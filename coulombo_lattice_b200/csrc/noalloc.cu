@@ -12,8 +12,8 @@
 // doubles each, 192 KiB in total.  It is a file-scope __device__ array, so every GPU that
 // loads the library holds it until the process exits.  In host code its name is only a
 // host-side stand-in; the device address is obtained once per device with
-// cudaGetSymbolAddress, on the first call made with that device current (so make that first
-// call before any stream capture).  The address is kept for the life of the process: after a
+// cudaGetSymbolAddress, on the first call made with that device current.  The address is
+// kept for the life of the process: after a
 // cudaDeviceReset the module is loaded again and the array may move, so a process that resets
 // a device must not call this entry point on it afterwards.  Every call rewrites all table
 // entries it reads, so nothing has to start at zero; but all calls share the one array, so
