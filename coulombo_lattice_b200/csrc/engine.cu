@@ -1189,10 +1189,21 @@ TcShape tc_shape(const cl_ctx* c, int nl, int nr, long long n_atoms) {
     return s;
 }
 
+// FP32 potentials and FP32 densities in one tile of each operand (at most 64 left and 64 right
+// densities): the Gram splits its operands itself (k_gram_tc_fused) and needs no operand
+// buffer.  With more tiles a block would convert its operands once per tile of the other
+// side, and the split pass + k_gram_tc is used.  CL_TC_SPLIT=1 keeps the split pass
+// everywhere; CL_TC_FUSED=1 takes the fused Gram at any tile count.
+bool fused_gram(bool v_f32, bool rho_f32, int nl, int nr) {
+    if (!v_f32 || !rho_f32 || std::getenv("CL_TC_SPLIT")) return false;
+    if (std::getenv("CL_TC_FUSED")) return true;
+    return 2 * nl <= clk::tc::BM && 2 * nr <= clk::tc::BN;
+}
+
 // Operand buffer for (nl, nr, n_atoms): whole atom range when it fits in a quarter of the free
 // device memory (at most 8 GiB), else chunks of the atom range.  Called outside any capture.
-void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms) {
-    if (!use_tc_gram(c) || nl <= 0 || nr <= 0 || n_atoms <= 0) return;
+void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms, bool v_f32, bool rho_f32) {
+    if (!use_tc_gram(c) || nl <= 0 || nr <= 0 || n_atoms <= 0 || fused_gram(v_f32, rho_f32, nl, nr)) return;
     const int rowsA = 2 * nl, rowsB = 2 * nr;
     const long long per_atom = tc_bytes_per_atom(rowsA, rowsB);
     const long long full = (n_atoms + clk::tc::BK - 1) / clk::tc::BK * clk::tc::BK;
@@ -1207,10 +1218,75 @@ void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms) {
     c->tc_buf.alloc((size_t)(atoms * per_atom / (long long)sizeof(float)));
 }
 
+// Atom splits of a Gram launch: whole waves of 148 blocks, each split at least 16 k-tiles long.
+int gram_splits(int tiles, int kt_total) {
+    int best_s = 1;
+    double best = -1e30;
+    const int s_max = std::max(1, std::min(256, kt_total / 16));
+    for (int s = 1; s <= s_max; ++s) {
+        const int per = (kt_total + s - 1) / s;
+        const int used = (kt_total + per - 1) / per;
+        const long long items = (long long)tiles * used;
+        const long long waves = (items + 147) / 148;
+        const double score = (double)items / (double)(waves * 148) - 0.01 * (double)waves;
+        if (score > best) {
+            best = score;
+            best_s = used;
+        }
+    }
+    return best_s;
+}
+
+// The fused Gram on FP32 operands over the whole atom range (see k_gram_tc_fused).
+void gram_tc_fused(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, const cx<float>* rho,
+                   long long r_stride, const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
+    using namespace clk::tc;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    });
+    const int tilesA = (2 * nl + BM - 1) / BM, tilesB = (2 * nr + BN - 1) / BN;
+    const int nA = std::min(BM / 2, nl), nB = std::min(BN / 2, nr);
+    const int nb = std::max(16, (2 * nB + 15) / 16 * 16);
+    FusedGram g{};
+    g.V = reinterpret_cast<const float2*>(V);
+    g.v_stride = v_stride;
+    g.rho = reinterpret_cast<const float2*>(rho);
+    g.r_stride = r_stride;
+    g.ridx = ridx_dev;
+    g.nl = nl;
+    g.nr = nr;
+    g.na = n_atoms;
+    g.out4 = out4_dev;
+    g.kt_total = (int)((n_atoms + BK - 1) / BK);
+    g.stage_bytes = (uint32_t)(2 * BM * 128 + 2 * nb * 128);
+    g.raw_slot_bytes = (uint32_t)((nA + nB) * BK * 8);
+    const int splits0 = gram_splits(tilesA * tilesB, g.kt_total);
+    g.kt_per = (g.kt_total + splits0 - 1) / splits0;
+    const int splits = (g.kt_total + g.kt_per - 1) / g.kt_per;
+    const size_t smem3 = fused_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 3);
+    const size_t smem2 = fused_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 2);
+    if (smem2 > 227 * 1024) cl::fail(CL_ERR_UNSUPPORTED, "fused Gram needs %zu bytes of shared memory", smem2);
+    cudaEvent_t e = prof_begin(c);
+    const dim3 grid(tilesA, tilesB, splits);
+    if (smem3 <= 227 * 1024)
+        k_gram_tc_fused<3><<<grid, FUSED_THREADS, smem3, c->stream>>>(g);
+    else
+        k_gram_tc_fused<2><<<grid, FUSED_THREADS, smem2, c->stream>>>(g);
+    CL_LAUNCHED();
+    prof_end(c, e, CL_KCLASS_GRAM, (double)n_atoms * (nl + nr) * (double)sizeof(cx<float>));
+}
+
 // out4[l][r] += {sum ac, bd, ad, bc} (out4 zeroed by the caller, error slot included).
 void gram_tc(cl_ctx* c, const void* V, bool v_f32, long long v_stride, int nl, const void* rho, bool rho_f32,
              long long r_stride, const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
     using namespace clk::tc;
+    if (fused_gram(v_f32, rho_f32, nl, nr)) {
+        gram_tc_fused(c, static_cast<const cx<float>*>(V), v_stride, nl, static_cast<const cx<float>*>(rho), r_stride,
+                      ridx_dev, nr, n_atoms, out4_dev);
+        return;
+    }
     const TcShape sh = tc_shape(c, nl, nr, n_atoms);
     if (sh.k_pad < BK) cl::fail(CL_ERR_STATE, "tensor-core Gram operands not reserved");
     static bool smem_set = false;
@@ -1247,21 +1323,7 @@ void gram_tc(cl_ctx* c, const void* V, bool v_f32, long long v_stride, int nl, c
         prof_end(c, e0, CL_KCLASS_GRAM_SPLIT,
                  (double)na * (nl * (v_f32 ? 8.0 : 16.0) + nr * (rho_f32 ? 8.0 : 16.0)) +
                      (double)tc_bytes_per_atom(sh.rowsA, sh.rowsB) * kp);
-        // atom splits: whole waves of 148 blocks, each split at least 2 chunks long
-        int best_s = 1;
-        double best = -1e30;
-        const int s_max = std::max(1, std::min(256, kt_total / 16));
-        for (int s = 1; s <= s_max; ++s) {
-            const int per = (kt_total + s - 1) / s;
-            const int used = (kt_total + per - 1) / per;
-            const long long items = (long long)tiles * used;
-            const long long waves = (items + 147) / 148;
-            const double score = (double)items / (double)(waves * 148) - 0.01 * (double)waves;
-            if (score > best) {
-                best = score;
-                best_s = used;
-            }
-        }
+        const int best_s = gram_splits(tiles, kt_total);
         const int kt_per = (kt_total + best_s - 1) / best_s;
         const int splits = (kt_total + kt_per - 1) / kt_per;
         cudaEvent_t e1 = prof_begin(c);
@@ -1335,13 +1397,77 @@ void gram(cl_ctx* c, const void* V_any, bool v_f32, long long v_stride, int nl, 
 // enqueues (it can be captured in a CUDA graph).
 struct PairSetup {
     DevBuf<clk::PairSeg> segs;  // products grouped by left state, indices into `states` (FP64 kernel)
-    clk::PairTri tri{};  // products over at most 8 states (FP32 register kernel)
+    clk::PairTri tri{};  // products over at most 12 states (register kernel)
     bool reg_ok = false;
     int grid_reg = 1;
+    // tiles of 4 x 4 states (more than 8 used states, see k_pair_density_tile)
+    bool tile_ok = false;
+    DevBuf<int> tile_states, tiles, tile_prod;
+    int ns_pad = 0, n_tiles = 0, tile_atoms = 0, tile_threads = 0, tile_blocks = 0;
+    size_t tile_smem = 0;
     DevBuf<int> states;
     int np = 0, n_segs = 0, n_used = 0, chunk = 1, blocks = 1;
     size_t smem = 0;
 };
+
+// Tables of the 4 x 4-state tile kernel: used states ascending, padded to a multiple of 4
+// (-1: zero rows); the requested tiles (bi | bj << 16, bi >= bj); and per ordered state pair
+// (i >= j) the density row 2p (rho_p = conj(c_i) c_j) or 2p + 1 (rho_p = conj(c_j) c_i).  The
+// atoms a block stages (A) are the most, of 64, 32, 16, 8, whose coefficients fit 110 KB (two
+// blocks an SM), else 8 atoms in up to 227 KB; beyond that, or when two products name the same
+// pair of states both ways, the segment kernel runs instead (as it does with CL_NO_PAIR_TILE=1).
+void pair_tile_setup(cl_ctx* c, const std::vector<int2>& fl, const std::vector<int>& used,
+                     const std::vector<int>& where, PairSetup& ps) {
+    const int n = (int)used.size();
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return used[a] < used[b]; });
+    std::vector<int> pos(n);
+    const int ns_pad = (n + clk::kPairTile - 1) / clk::kPairTile * clk::kPairTile;
+    std::vector<int> st(ns_pad, -1);
+    for (int k = 0; k < n; ++k) {
+        pos[order[k]] = k;
+        st[k] = used[order[k]];
+    }
+    std::vector<int> prod((size_t)ns_pad * ns_pad, -1);
+    const int nblk = ns_pad / clk::kPairTile;
+    std::vector<char> want((size_t)nblk * nblk, 0);
+    for (int p = 0; p < ps.np; ++p) {
+        int i = pos[where[fl[p].x]], j = pos[where[fl[p].y]];
+        int code = 2 * p;
+        if (i < j) {
+            std::swap(i, j);
+            code += 1;
+        }
+        int& slot = prod[(size_t)i * ns_pad + j];
+        if (slot >= 0) return;  // the same pair both ways: the segment kernel
+        slot = code;
+        want[(size_t)(i / clk::kPairTile) * nblk + j / clk::kPairTile] = 1;
+    }
+    std::vector<int> tiles;
+    for (int bi = 0; bi < nblk; ++bi)
+        for (int bj = 0; bj <= bi; ++bj)
+            if (want[(size_t)bi * nblk + bj]) tiles.push_back(bi | (bj << 16));
+    const size_t per_atom = sizeof(cx<double>) * (size_t)ns_pad * (size_t)(c->n_orb | 1);
+    int A = 0;
+    for (int cand : {64, 32, 16, 8})
+        if (per_atom * cand <= 110 * 1024) {
+            A = cand;
+            break;
+        }
+    if (A == 0 && per_atom * 8 <= 227 * 1024) A = 8;
+    if (A == 0) return;
+    ps.tile_ok = true;
+    ps.ns_pad = ns_pad;
+    ps.n_tiles = (int)tiles.size();
+    ps.tile_atoms = A;
+    ps.tile_smem = per_atom * A;
+    ps.tile_threads = (int)std::min<long long>(256, ((long long)ps.n_tiles * A + 31) / 32 * 32);
+    ps.tile_blocks = (int)std::max<long long>(1, std::min<long long>((c->n_sorted + A - 1) / A, 148LL * 8));
+    ps.tile_states.upload(st.data(), st.size(), c->stream);
+    ps.tiles.upload(tiles.data(), tiles.size(), c->stream);
+    ps.tile_prod.upload(prod.data(), prod.size(), c->stream);
+}
 
 void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
     ps.np = (int)fl.size();
@@ -1368,9 +1494,11 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
         }
     ps.n_segs = (int)segs.size();
     ps.segs.upload(segs.data(), segs.size(), c->stream);
-    // register kernel (at most 8 used states): the used states in ascending order, and the
+    // register kernel (at most 12 used states): the used states in ascending order, and the
     // density row of each product (i, j), i >= j in that order (rows are conj(c_x) c_y, x >= y)
-    ps.reg_ok = !used.empty() && used.size() <= 8;
+    // (CL_NO_PAIR_REG12=1: at most 8, the 4 x 4-state tile kernel above that)
+    const size_t reg_max = std::getenv("CL_NO_PAIR_REG12") ? 8 : (size_t)clk::kPairRegStates;
+    ps.reg_ok = !used.empty() && used.size() <= reg_max;
     if (ps.reg_ok) {
         std::vector<int> order(used.size());
         std::iota(order.begin(), order.end(), 0);
@@ -1380,7 +1508,7 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
             pos[order[k]] = (int)k;
             ps.tri.states[k] = used[order[k]];
         }
-        for (size_t k = order.size(); k < 8; ++k) ps.tri.states[k] = used[order[0]];
+        for (size_t k = order.size(); k < (size_t)clk::kPairRegStates; ++k) ps.tri.states[k] = used[order[0]];
         for (int& v : ps.tri.prod) v = -1;
         for (int p = 0; p < ps.np; ++p) {
             const int i = pos[where[fl[p].x]], j = pos[where[fl[p].y]];
@@ -1390,6 +1518,7 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
         ps.grid_reg = (int)std::max<long long>(
             1, std::min<long long>((c->n_sorted + clk::kPairAtoms - 1) / clk::kPairAtoms, 148LL * 2 * 4));
     }
+    if (!ps.reg_ok && !used.empty() && !std::getenv("CL_NO_PAIR_TILE")) pair_tile_setup(c, fl, used, where, ps);
     ps.states.upload(used.data(), used.size(), c->stream);
     ps.n_used = (int)used.size();
     // two stages of `chunk` atoms, each up to 48 KB (about two blocks per SM)
@@ -1415,7 +1544,7 @@ void pair_setup(cl_ctx* c, const std::vector<int2>& fl, PairSetup& ps) {
     CL_CUDA(cudaStreamSynchronize(c->stream));
 }
 
-// f(std::integral_constant<int, n>) for 1 <= n <= 8 used states
+// f(std::integral_constant<int, n>) for 1 <= n <= 12 used states
 template <typename F>
 void with_states(int n, F&& f) {
     switch (n) {
@@ -1426,7 +1555,11 @@ void with_states(int n, F&& f) {
         case 5: f(std::integral_constant<int, 5>{}); break;
         case 6: f(std::integral_constant<int, 6>{}); break;
         case 7: f(std::integral_constant<int, 7>{}); break;
-        default: f(std::integral_constant<int, 8>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 9: f(std::integral_constant<int, 9>{}); break;
+        case 10: f(std::integral_constant<int, 10>{}); break;
+        case 11: f(std::integral_constant<int, 11>{}); break;
+        default: f(std::integral_constant<int, 12>{}); break;
     }
 }
 
@@ -1440,11 +1573,11 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
             constexpr int NS = decltype(ns)::value;
             const size_t smem = 2 * sizeof(cx<double>) * clk::pair_stage_elems(NS);
             ensure_smem(clk::k_pair_density_reg<NS, double>, smem);
-            clk::k_pair_density_reg<NS, double><<<ps.grid_reg, 256, smem, c->stream>>>(
+            clk::k_pair_density_reg<NS, double><<<ps.grid_reg, clk::kPairAtoms * clk::pair_parts(NS), smem, c->stream>>>(
                 c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
         };
         with_states(ps.n_used, go);
-    } else if (fp64_form(c)) {
+    } else if (fp64_form(c) && !ps.tile_ok) {
         ensure_smem(clk::k_pair_density<double>, ps.smem);
         clk::k_pair_density<double><<<ps.blocks, 256, ps.smem, c->stream>>>(
             c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
@@ -1455,11 +1588,23 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
             constexpr int NS = decltype(ns)::value;
             const size_t smem = 2 * sizeof(cx<double>) * clk::pair_stage_elems(NS);
             ensure_smem(clk::k_pair_density_reg<NS, float>, smem);
-            clk::k_pair_density_reg<NS, float><<<ps.grid_reg, 256, smem, c->stream>>>(
+            clk::k_pair_density_reg<NS, float><<<ps.grid_reg, clk::kPairAtoms * clk::pair_parts(NS), smem, c->stream>>>(
                 c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
         };
         with_states(ps.n_used, go);
-    } else {  // more than 8 states: the staged kernel (FP64 sums, rounded once)
+    } else if (ps.tile_ok) {  // more than 12 states: 4 x 4-state tiles (FP64 sums, rounded once)
+        const auto go = [&](auto tag) {
+            using RT = decltype(tag);
+            ensure_smem(clk::k_pair_density_tile<RT>, ps.tile_smem);
+            clk::k_pair_density_tile<RT><<<ps.tile_blocks, ps.tile_threads, ps.tile_smem, c->stream>>>(
+                c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tile_states.p, ps.ns_pad,
+                ps.tiles.p, ps.n_tiles, ps.tile_prod.p, ps.tile_atoms, static_cast<cx<RT>*>(rho));
+        };
+        if (fp64_form(c))
+            go(double{});
+        else
+            go(float{});
+    } else {  // the segment kernel (FP64 sums, rounded once)
         ensure_smem(clk::k_pair_density<float>, ps.smem);
         clk::k_pair_density<float><<<ps.blocks, 256, ps.smem, c->stream>>>(
             c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
@@ -1634,7 +1779,7 @@ int cl_calculate_grid(cl_ctx* c, const double* rho2, double out[2]) {
         DevBuf<int> ridx;
         int zero = 0;
         ridx.upload(&zero, 1, c->stream);
-        tc_reserve(c, 1, 1, c->M);
+        tc_reserve(c, 1, 1, c->M, false, false);
         gram(c, c->grid_V.p, false, c->M, 1, c->grid_rho2.p, false, c->M, ridx.p, 1, c->M, o4.p);
         double h[5];
         CL_CUDA(cudaMemcpyAsync(h, o4.p, sizeof h, cudaMemcpyDeviceToHost, c->stream));
@@ -1939,7 +2084,7 @@ void compute_impl(cl_ctx* c, int64_t n_int, const int16_t* spec, double* out, in
         grow(V, (size_t)nl * As);
         DevBuf<double>& o4 = c->req_o4;
         grow(o4, (size_t)4 * nl * nr + 1);
-        tc_reserve(c, nl, nr, As);
+        tc_reserve(c, nl, nr, As, v_fp32(c), rho_bytes(c) == sizeof(cx<float>));
         CL_CUDA(cudaEventRecord(c->ev[0], c->stream));
         pair_densities(c, fl, rho.p);
         CL_CUDA(cudaEventRecord(c->ev[1], c->stream));
@@ -2102,7 +2247,7 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     grow(V, (size_t)nl * As);
     DevBuf<double>& o4 = c->req_o4;
     grow(o4, (size_t)4 * nl * nr + 1);
-    tc_reserve(c, nl, nr, As);
+    tc_reserve(c, nl, nr, As, v_fp32(c), rho_bytes(c) == sizeof(cx<float>));
     CL_CUDA(cudaStreamSynchronize(c->stream));
     for (auto& g : groups) {
         upload_through(g->last_state);
@@ -2349,7 +2494,7 @@ int cl_request_create_shard(cl_ctx* c, int64_t n_int, const int16_t* spec, int s
         r->V.alloc((size_t)r->nl * As);
         r->o4.alloc((size_t)4 * r->nl * r->nr + 1);
         CL_CUDA(cudaMallocHost(&r->o4_host, sizeof(double) * (4 * (size_t)r->nl * r->nr + 1)));
-        tc_reserve(c, r->nl, r->nr, As);
+        tc_reserve(c, r->nl, r->nr, As, v_fp32(c), rho_bytes(c) == sizeof(cx<float>));
         CL_CUDA(cudaStreamSynchronize(c->stream));
         *out = r;
     });

@@ -125,6 +125,44 @@ __device__ __forceinline__ void dft8(cx<T>* v) {
     v[7] = e[3] - o3;
 }
 
+// 8-point DFT of (v[0..3], 0, 0, 0, 0): the zero half skipped (the zero-padded first stage of
+// an aperiodic transform).
+template <int S, typename T>
+__device__ __forceinline__ void dft8_half_in(cx<T>* v) {
+    const cx<T> e0 = v[0] + v[2], e2 = v[0] - v[2], is2 = mul_is<S>(v[2]);
+    const cx<T> e1 = v[0] + is2, e3 = v[0] - is2;
+    const cx<T> o0 = v[1] + v[3], o2 = v[1] - v[3], is3 = mul_is<S>(v[3]);
+    const cx<T> p1 = v[1] + is3, p3 = v[1] - is3;
+    const T r = T(CLK_SQRT1_2);
+    const cx<T> o1 = mk((p1.re - S * p1.im) * r, (p1.im + S * p1.re) * r);
+    const cx<T> o2w = mul_is<S>(o2);
+    const cx<T> o3 = mk((-p3.re - S * p3.im) * r, (-p3.im + S * p3.re) * r);
+    v[0] = e0 + o0;
+    v[4] = e0 - o0;
+    v[1] = e1 + o1;
+    v[5] = e1 - o1;
+    v[2] = e2 + o2w;
+    v[6] = e2 - o2w;
+    v[3] = e3 + o3;
+    v[7] = e3 - o3;
+}
+
+// Outputs 0..3 of the 8-point DFT of v[0..7] (the kept half of an aperiodic result).
+template <int S, typename T>
+__device__ __forceinline__ void dft8_half_out(cx<T>* v) {
+    cx<T> e[4] = {v[0], v[2], v[4], v[6]};
+    cx<T> o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<S>(e);
+    dft4<S>(o);
+    const T r = T(CLK_SQRT1_2);
+    const cx<T> o1 = mk((o[1].re - S * o[1].im) * r, (o[1].im + S * o[1].re) * r);
+    const cx<T> o3 = mk((-o[3].re - S * o[3].im) * r, (-o[3].im + S * o[3].re) * r);
+    v[0] = e[0] + o[0];
+    v[1] = e[1] + o1;
+    v[2] = e[2] + mul_is<S>(o[2]);
+    v[3] = e[3] + o3;
+}
+
 template <int N>
 struct WConst;
 // Twiddle constants exp(2 pi i m / N) of the composite register codelets, evaluated to

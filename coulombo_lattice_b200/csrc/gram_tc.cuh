@@ -378,5 +378,302 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Fused Gram for FP32 operands (the FP32 sub-lattice form: FP32 potentials and pair densities).
+// The split happens inside the kernel, so neither the hi/lo operands nor any padding reach HBM.
+// Sixteen warps, each with three jobs per k-tile of 32 atoms:
+//   copy    8-byte cp.async of the raw complex values of its densities into a ring of AHEAD+1
+//           raw slots, AHEAD tiles ahead: a lane takes 4 consecutive atoms of one density, 8
+//           lanes a density, a warp 4 densities (4w + 64j + lane/8: left densities of the
+//           block's A tile, then right densities of its B tile);
+//   convert round the lane's 4 values to TF32 hi and lo parts and store them with four 16-byte
+//           stores (re hi, im hi, re lo, im lo) into the MMA stage in the 128-byte-swizzled
+//           K-major layout the descriptors expect -- row r, atoms 4c..4c+3 at (r/8)*1024 +
+//           (r%8)*128 + ((c ^ (r%8))*16): 8 lanes fill one row without bank conflicts -- fence
+//           the stores to the async proxy and arrive on the stage's full barrier (then thread 0
+//           issues the tile's MMAs as in k_gram_tc, with N = the block's right rows rounded up
+//           to 16);
+//   drain   the previous k-tile's main products, tensor memory -> FP64 registers: lane quarter
+//           w % 4, accumulator columns 32 (w / 4) .. + 31.
+// Rows beyond the real ones are zeroed once at the start and never written again.  Each thread
+// reads back only the raw values it copied itself, so its own cp.async group wait is the only
+// ordering the raw ring needs.
+// ---------------------------------------------------------------------------------------
+struct FusedGram {
+    const float2* V;      // left densities: V[l * v_stride + atom]
+    long long v_stride;
+    const float2* rho;    // right densities: rho[(ridx ? ridx[r] : r) * r_stride + atom]
+    long long r_stride;
+    const int* ridx;
+    int nl, nr;
+    long long na;         // atoms
+    int kt_total, kt_per;
+    uint32_t stage_bytes;     // 2 * BM * 128 + 2 * nb_max * 128
+    uint32_t raw_slot_bytes;  // (left + right densities of a block, at most) * 32 * 8
+    double* out4;
+};
+
+constexpr int FUSED_WARPS = 16;
+constexpr int FUSED_THREADS = 32 * FUSED_WARPS;
+constexpr int FUSED_MMA_STAGES = 2;
+constexpr int FUSED_MAX_DENS = BM / 2 + BN / 2;  // densities a block converts per k-tile
+
+__host__ __device__ constexpr uint32_t fused_idesc(int nb) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(nb >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+// Bytes of dynamic shared memory: alignment slack, the MMA stages, the raw ring, the source
+// table and the barriers.
+__host__ __device__ constexpr size_t fused_smem_bytes(uint32_t stage_bytes, uint32_t raw_slot_bytes, int ahead) {
+    return 1024 + (size_t)FUSED_MMA_STAGES * stage_bytes + (size_t)(ahead + 1) * raw_slot_bytes +
+           sizeof(void*) * FUSED_MAX_DENS + 256;
+}
+
+// Byte offset of the 16-byte chunk c (atoms 4c..4c+3) of row r in a 128-byte-swizzled tile.
+__device__ __forceinline__ uint32_t sw128_chunk(int row, int c) {
+    return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((c ^ (row & 7)) << 4));
+}
+__device__ __forceinline__ void mma_tf32_n(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// grid = (ceil(2 nl / BM), ceil(2 nr / BN), splits); block z covers k-tiles
+// [z * kt_per, min(kt_total, (z + 1) * kt_per)), never empty.  out4 as for k_gram_tc.
+template <int AHEAD>
+__global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedGram g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - raw);
+    const uint32_t ring_off = FUSED_MMA_STAGES * g.stage_bytes;
+    const float2** src_tab = reinterpret_cast<const float2**>(gbase + ring_off + (AHEAD + 1) * g.raw_slot_bytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(src_tab + FUSED_MAX_DENS);
+    // bars: full[2], empty[2], acc_full[2], acc_empty[2], drain
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 9);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const auto bar = [&](int i) { return smem_u32(bars + i); };
+    constexpr int FULL = 0, EMPTY = 2, ACCF = 4, ACCE = 6, DRAIN = 8;
+    constexpr uint32_t A_PART = BM * 128;  // bytes of one TF32 part of the A tile
+    const uint32_t b_part = (g.stage_bytes - 2u * A_PART) / 2u;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int la0 = m0 / 2, rb0 = n0 / 2;
+    const int nA = min(BM / 2, g.nl - la0), nB = min(BN / 2, g.nr - rb0);
+    const int nd = nA + nB;
+    const int nb = max(16, (2 * nB + 15) / 16 * 16);  // MMA N: the block's right rows, rounded up
+    const uint32_t idesc = fused_idesc(nb);
+    const int kt0 = blockIdx.z * g.kt_per;
+    const int nt = min(g.kt_total, kt0 + g.kt_per) - kt0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < FUSED_MMA_STAGES; ++s) {
+            mbar_init(bar(FULL + s), FUSED_THREADS);
+            mbar_init(bar(EMPTY + s), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(bar(ACCF + b), 1);
+            mbar_init(bar(ACCE + b), FUSED_THREADS);
+        }
+        mbar_init(bar(DRAIN), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < nd; i += FUSED_THREADS) {
+        if (i < nA) {
+            src_tab[i] = g.V + (long long)(la0 + i) * g.v_stride;
+        } else {
+            const int r = rb0 + (i - nA);
+            src_tab[i] = g.rho + (long long)(g.ridx ? g.ridx[r] : r) * g.r_stride;
+        }
+    }
+    // zero both MMA stages once: rows beyond the real ones are never written again
+    for (uint32_t o = threadIdx.x * 16u; o < ring_off; o += FUSED_THREADS * 16u)
+        *reinterpret_cast<uint4*>(gbase + o) = make_uint4(0u, 0u, 0u, 0u);
+    fence_proxy_async();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int dsub = lane >> 3;       // density of the warp's four this lane converts
+    const int quad = lane & 7;        // atoms 4 quad .. 4 quad + 3 of the k-tile
+    const int q = warp & 3;           // tensor-memory lane quarter this warp may read
+    const int c0 = (warp >> 2) * 32;  // first accumulator column this warp drains
+    bool issued_any = false;          // thread 0: MMAs issued
+    // thread 0: the MMAs of k-tile t, once its stage is full and its accumulator drained
+    const auto mma_tile = [&](int t) -> bool {
+        const int s = t & 1, b = t & 1;
+        const uint32_t ph = (uint32_t)((t >> 1) & 1);
+        if (!mbar_wait(bar(ACCE + b), ph ^ 1u, abort_flag)) return false;
+        if (!mbar_wait(bar(FULL + s), ph, abort_flag)) return false;
+        fence_after();
+        const uint32_t st = base + (uint32_t)s * g.stage_bytes;
+        const uint32_t dm = tmem + (uint32_t)(b * BN);  // main products of this k-tile
+        const uint32_t dc = tmem + (uint32_t)(2 * BN);  // correction products, whole range
+#pragma unroll
+        for (int kk = 0; kk < BK / 8; ++kk) {
+            const uint64_t ahi = sw128_desc(st + kk * 32);
+            const uint64_t alo = sw128_desc(st + A_PART + kk * 32);
+            const uint64_t bhi = sw128_desc(st + 2 * A_PART + kk * 32);
+            const uint64_t blo = sw128_desc(st + 2 * A_PART + b_part + kk * 32);
+            mma_tf32_n(dm, ahi, bhi, idesc, kk > 0 ? 1u : 0u);
+            mma_tf32_n(dc, alo, bhi, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+            mma_tf32_n(dc, ahi, blo, idesc, 1u);
+        }
+        issued_any = true;
+        mma_commit(bar(EMPTY + s));  // the stage is free once these MMAs finish
+        mma_commit(bar(ACCF + b));   // k-tile complete in accumulator b
+        return true;
+    };
+    double acc[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+    const auto issue = [&](int t) {
+        const long long at0 = (long long)(kt0 + t) * BK + 4 * quad;
+        const uint32_t slot = base + ring_off + (uint32_t)(t % (AHEAD + 1)) * g.raw_slot_bytes + (uint32_t)quad * 32u;
+        for (int i = 4 * warp + dsub; i < nd; i += 4 * FUSED_WARPS) {
+            const float2* src = src_tab[i];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const bool in = at0 + e < g.na;
+                cp_async8(slot + (uint32_t)i * 256u + 8u * e, src + (in ? at0 + e : 0LL), in ? 8u : 0u);
+            }
+        }
+    };
+    // adds accumulator columns col + c0 .. + 31 of this warp's lanes to acc (after waiting for
+    // the MMAs that complete the barrier `mbar`, phase `ph`)
+    const auto drain = [&](uint32_t mbar, uint32_t ph, uint32_t col) -> bool {
+        bool got = mbar_wait(mbar, ph, abort_flag);
+        got = __all_sync(0xffffffffu, got);
+        if (!got) return false;
+        fence_after();
+        if (c0 < nb) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + col + (uint32_t)c0, v);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] += (double)v[i];
+        }
+        fence_before();
+        return true;
+    };
+#pragma unroll 1
+    for (int t = 0; t < AHEAD; ++t) {
+        if (t < nt) issue(t);
+        cp_async_commit();
+    }
+    bool ok = true;
+#pragma unroll 1
+    for (int t = 0; t < nt; ++t) {
+        if (t + AHEAD < nt) issue(t + AHEAD);
+        cp_async_commit();
+        cp_async_wait<AHEAD>();  // this thread's copies of k-tile t have landed
+        const int s = t & 1;
+        bool got = mbar_wait(bar(EMPTY + s), (uint32_t)(((t >> 1) & 1) ^ 1), abort_flag);
+        if (!__all_sync(0xffffffffu, got)) {
+            ok = false;
+            break;
+        }
+        unsigned char* stg = gbase + (size_t)s * g.stage_bytes;
+        const unsigned char* rs = gbase + ring_off + (size_t)(t % (AHEAD + 1)) * g.raw_slot_bytes + quad * 32;
+        for (int i = 4 * warp + dsub; i < nd; i += 4 * FUSED_WARPS) {
+            const float4 z0 = *reinterpret_cast<const float4*>(rs + i * 256);       // atoms 0, 1
+            const float4 z1 = *reinterpret_cast<const float4*>(rs + i * 256 + 16);  // atoms 2, 3
+            const float re[4] = {z0.x, z0.z, z1.x, z1.z}, im[4] = {z0.y, z0.w, z1.y, z1.w};
+            float rh[4], ih[4], rl[4], il[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                rh[e] = tf32_rn(re[e]);
+                ih[e] = tf32_rn(im[e]);
+                rl[e] = tf32_rn(re[e] - rh[e]);
+                il[e] = tf32_rn(im[e] - ih[e]);
+            }
+            const bool left = i < nA;
+            unsigned char* hi_p = left ? stg : stg + 2 * A_PART;
+            unsigned char* lo_p = hi_p + (left ? A_PART : b_part);
+            const int row = 2 * (left ? i : i - nA);
+            const uint32_t o0 = sw128_chunk(row, quad), o1 = sw128_chunk(row + 1, quad);
+            *reinterpret_cast<float4*>(hi_p + o0) = make_float4(rh[0], rh[1], rh[2], rh[3]);
+            *reinterpret_cast<float4*>(hi_p + o1) = make_float4(ih[0], ih[1], ih[2], ih[3]);
+            *reinterpret_cast<float4*>(lo_p + o0) = make_float4(rl[0], rl[1], rl[2], rl[3]);
+            *reinterpret_cast<float4*>(lo_p + o1) = make_float4(il[0], il[1], il[2], il[3]);
+        }
+        fence_proxy_async();  // the stores, seen by the tensor cores' async proxy
+        mbar_arrive(bar(FULL + s));
+        if (warp == 0) {
+            bool go = true;
+            if (lane == 0) go = mma_tile(t);
+            if (!__shfl_sync(0xffffffffu, go ? 1 : 0, 0)) {
+                ok = false;
+                break;
+            }
+        }
+        if (t > 0) {
+            const int tp = t - 1;
+            if (!drain(bar(ACCF + (tp & 1)), (uint32_t)((tp >> 1) & 1), (uint32_t)((tp & 1) * BN))) {
+                ok = false;
+                break;
+            }
+            mbar_arrive(bar(ACCE + (tp & 1)));
+        }
+    }
+    if (ok) {
+        const int tp = nt - 1;
+        ok = drain(bar(ACCF + (tp & 1)), (uint32_t)((tp >> 1) & 1), (uint32_t)((tp & 1) * BN));
+        // the correction accumulator is complete with the last k-tile's commit
+        if (ok) ok = drain(bar(ACCF + (tp & 1)), (uint32_t)((tp >> 1) & 1), (uint32_t)(2 * BN));
+    }
+    cp_async_wait_all();
+    if (threadIdx.x == 0 && *abort_flag && issued_any) {
+        mma_commit(bar(DRAIN));
+        mbar_drain(bar(DRAIN), 0);
+    }
+    if (ok) {
+        const int R = m0 + 32 * q + lane;
+        const int l = R >> 1, pa = R & 1;
+        if (l < g.nl) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int Cg = n0 + c0 + j;
+                const int r = Cg >> 1, pc = Cg & 1;
+                if (r < g.nr) {
+                    const int qi = (pa == pc) ? pa : 2 + pa;  // ac, bd, ad, bc
+                    atomicAdd(g.out4 + ((long long)l * g.nr + r) * 4 + qi, acc[j]);
+                }
+            }
+        }
+    }
+
+    fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag)
+        *reinterpret_cast<volatile int*>(g.out4 + (long long)4 * g.nl * g.nr) = 1;
+    if (warp == 0) {
+        __syncwarp();
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 }  // namespace tc
 }  // namespace clk

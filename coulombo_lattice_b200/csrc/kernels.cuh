@@ -241,29 +241,32 @@ __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restri
 }
 
 // ---------------------------------------------------------------------------------------
-// Pair densities for requests over at most 8 states, summed in FP64 and rounded once to the
+// Pair densities for requests over at most 12 states, summed in FP64 and rounded once to the
 // form's precision RT; products t = i (i + 1) / 2 + j of states i >= j (ascending order) go to
 // rows prod[t] of rho.
 // ---------------------------------------------------------------------------------------
+constexpr int kPairRegStates = 12;
 struct PairTri {
-    int states[8];  // used states in ascending order (coefficient rows)
-    int prod[36];   // density row of product (i, j), i >= j, at i (i + 1) / 2 + j; -1: not requested
+    int states[kPairRegStates];                             // used states, ascending (coefficient rows)
+    int prod[kPairRegStates * (kPairRegStates + 1) / 2];    // row of product (i, j), i >= j; -1: not requested
 };
 
-// Block = 256 threads over 64 atoms: the products are split into four parts (t mod 4), each
-// taken by two warps (the part is uniform over a warp: no predicated work; nine FP64 sums at most
-// per thread).  The coefficients are staged through shared memory four orbitals at a time: per
-// (state, atom) the 64 contiguous bytes of those orbitals are copied with 16-byte cp.async
-// (coalesced; the next slice is in flight while this one is used), at an 80-byte pitch per atom
-// so that threads on consecutive atoms read distinct banks.  Every coefficient leaves HBM once and
-// each part reads the slice from shared memory.  The barriers are in the kernel body, reached by
-// every thread; only the arithmetic is specialised per part.
-constexpr int kPairParts = 4;
-constexpr int kPairAtoms = 256 / kPairParts;  // atoms per block and step
-constexpr int kPairOrbSlice = 4;              // orbitals per stage
+// Block = 64 atoms x PARTS warp pairs: the products are split into PARTS parts (t mod PARTS),
+// each taken by the two warps of one part (the part is uniform over a warp: no predicated work;
+// at most 10 FP64 sums per thread: 4 parts up to 8 states, 8 parts up to 12).  The coefficients
+// are staged through shared memory four orbitals at a time: per (state, atom) the 64 contiguous
+// bytes of those orbitals are copied with 16-byte cp.async (coalesced; the next slice is in
+// flight while this one is used), at an 80-byte pitch per atom so that threads on consecutive
+// atoms read distinct banks.  Every coefficient leaves HBM once and each part reads the slice
+// from shared memory.  The barriers are in the kernel body, reached by every thread; only the
+// arithmetic is specialised per part.
+constexpr int kPairAtoms = 64;      // atoms per block and step
+constexpr int kPairOrbSlice = 4;    // orbitals per stage
 __host__ __device__ constexpr int pair_stage_elems(int ns) { return ns * kPairAtoms * (kPairOrbSlice + 1); }
+__host__ __device__ constexpr int pair_parts(int ns) { return ns <= 8 ? 4 : 8; }
+__host__ __device__ constexpr int pair_min_blocks(int ns) { return ns <= 8 ? 2 : 1; }  // <= 128 registers
 
-template <int NS, int H>
+template <int NS, int PARTS, int H>
 __device__ __forceinline__ void pair_accumulate(const cx<double>* __restrict__ st, int a, double* ar, double* ai) {
     constexpr int NT = NS * (NS + 1) / 2;
 #pragma unroll
@@ -276,31 +279,54 @@ __device__ __forceinline__ void pair_accumulate(const cx<double>* __restrict__ s
 #pragma unroll
             for (int j = 0; j <= i; ++j) {
                 const int t = i * (i + 1) / 2 + j;
-                if (t % kPairParts == H && t < NT) {  // compile-time after unrolling
-                    ar[t / kPairParts] += c[i].re * c[j].re + c[i].im * c[j].im;  // conj(c_i) c_j
-                    ai[t / kPairParts] += c[i].re * c[j].im - c[i].im * c[j].re;
+                if (t % PARTS == H && t < NT) {  // compile-time after unrolling
+                    ar[t / PARTS] += c[i].re * c[j].re + c[i].im * c[j].im;  // conj(c_i) c_j
+                    ai[t / PARTS] += c[i].re * c[j].im - c[i].im * c[j].re;
                 }
             }
     }
 }
 
-template <int NS, int H, typename RT>
+template <int NS, int PARTS, int H, typename RT>
 __device__ __forceinline__ void pair_store(const PairTri& tri, const double* ar, const double* ai, long long slot,
                                            long long n_sorted, cx<RT>* __restrict__ rho) {
-    constexpr int NT = NS * (NS + 1) / 2, NH = (NT - H + kPairParts - 1) / kPairParts;
+    constexpr int NT = NS * (NS + 1) / 2, NH = (NT - H + PARTS - 1) / PARTS;
 #pragma unroll
     for (int k = 0; k < NH; ++k) {
-        const int p = tri.prod[kPairParts * k + H];
+        const int p = tri.prod[PARTS * k + H];
         if (p >= 0) rho[(long long)p * n_sorted + slot] = narrow<RT>(mk(ar[k], ai[k]));
     }
 }
 
+// The part `part` of the thread, dispatched to the compile-time part H.
+template <int NS, int PARTS, int H = 0>
+__device__ __forceinline__ void pair_accumulate_part(int part, const cx<double>* __restrict__ st, int a, double* ar,
+                                                     double* ai) {
+    if constexpr (H < PARTS) {
+        if (part == H)
+            pair_accumulate<NS, PARTS, H>(st, a, ar, ai);
+        else
+            pair_accumulate_part<NS, PARTS, H + 1>(part, st, a, ar, ai);
+    }
+}
+template <int NS, int PARTS, typename RT, int H = 0>
+__device__ __forceinline__ void pair_store_part(int part, const PairTri& tri, const double* ar, const double* ai,
+                                                long long slot, long long n_sorted, cx<RT>* __restrict__ rho) {
+    if constexpr (H < PARTS) {
+        if (part == H)
+            pair_store<NS, PARTS, H, RT>(tri, ar, ai, slot, n_sorted, rho);
+        else
+            pair_store_part<NS, PARTS, RT, H + 1>(part, tri, ar, ai, slot, n_sorted, rho);
+    }
+}
+
 template <int NS, typename RT>
-__global__ void __launch_bounds__(256, 2) k_pair_density_reg(const cx<double>* __restrict__ coeff, long long n_atoms,
-                                                            int n_orb, const int* __restrict__ orig,
-                                                            long long n_sorted, const PairTri tri,
-                                                            cx<RT>* __restrict__ rho) {
-    constexpr int NT = NS * (NS + 1) / 2, NHM = (NT + kPairParts - 1) / kPairParts;
+__global__ void __launch_bounds__(kPairAtoms * pair_parts(NS), pair_min_blocks(NS))
+    k_pair_density_reg(const cx<double>* __restrict__ coeff, long long n_atoms, int n_orb,
+                       const int* __restrict__ orig, long long n_sorted, const PairTri tri,
+                       cx<RT>* __restrict__ rho) {
+    constexpr int PARTS = pair_parts(NS), THREADS = kPairAtoms * PARTS;
+    constexpr int NT = NS * (NS + 1) / 2, NHM = (NT + PARTS - 1) / PARTS;
     constexpr int SE = pair_stage_elems(NS);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<double>* sm = reinterpret_cast<cx<double>*>(smem_raw);
@@ -310,7 +336,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_density_reg(const cx<double>* _
     // the copies of one stage: NS states x 64 atoms x 4 orbitals, 16 bytes each
     const auto issue = [&](long long a0, int slice, cx<double>* st) {
         const int na = (int)min((long long)kPairAtoms, n_sorted - a0);
-        for (int e = threadIdx.x; e < NS * kPairAtoms * kPairOrbSlice; e += 256) {
+        for (int e = threadIdx.x; e < NS * kPairAtoms * kPairOrbSlice; e += THREADS) {
             const int o = e % kPairOrbSlice, r = e / kPairOrbSlice;
             const int at = r % kPairAtoms, i = r / kPairAtoms;
             const int orb = slice * kPairOrbSlice + o;
@@ -340,21 +366,97 @@ __global__ void __launch_bounds__(256, 2) k_pair_density_reg(const cx<double>* _
                 asm volatile("cp.async.wait_group 0;\n" ::);
             }
             __syncthreads();
-            const cx<double>* st = sm + stage * SE;
-            if (part == 0) pair_accumulate<NS, 0>(st, a, ar, ai);
-            else if (part == 1) pair_accumulate<NS, 1>(st, a, ar, ai);
-            else if (part == 2) pair_accumulate<NS, 2>(st, a, ar, ai);
-            else pair_accumulate<NS, 3>(st, a, ar, ai);
+            pair_accumulate_part<NS, PARTS>(part, sm + stage * SE, a, ar, ai);
             __syncthreads();  // the stage is refilled two slices on
             stage ^= 1;
         }
         const long long slot = a0 + a;
-        if (slot < n_sorted) {
-            if (part == 0) pair_store<NS, 0, RT>(tri, ar, ai, slot, n_sorted, rho);
-            else if (part == 1) pair_store<NS, 1, RT>(tri, ar, ai, slot, n_sorted, rho);
-            else if (part == 2) pair_store<NS, 2, RT>(tri, ar, ai, slot, n_sorted, rho);
-            else pair_store<NS, 3, RT>(tri, ar, ai, slot, n_sorted, rho);
+        if (slot < n_sorted) pair_store_part<NS, PARTS, RT>(part, tri, ar, ai, slot, n_sorted, rho);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Pair densities for requests over more than 8 states, in tiles of 4 x 4 states.  The used
+// states, ascending and padded to a multiple of 4 (padding rows are zero), form blocks of 4;
+// tile (bi, bj), bi >= bj, holds the products conj(c_i) c_j, i = 4 bi + u, j = 4 bj + v, of
+// which prod[i * ns_pad + j] names the density row (2 p, or 2 p + 1 where the row is the
+// conjugate, conj(c_j) c_i; -1: not requested).  Only tiles with a requested product are
+// listed.  A block stages every orbital of its A atoms for every used state in shared memory
+// ([state][atom][orbital], odd atom pitch: consecutive atoms on distinct banks; each
+// coefficient leaves HBM once), then each thread takes (tile, atom) work items: per orbital
+// 8 coefficient loads feed 16 complex FP64 products (the FP64 pipe, not shared memory, bounds
+// it), and the sums are rounded once to RT on the store.
+// ---------------------------------------------------------------------------------------
+constexpr int kPairTile = 4;
+
+template <typename RT>
+__global__ void __launch_bounds__(256, 2) k_pair_density_tile(const cx<double>* __restrict__ coeff,
+                                                             long long n_atoms, int n_orb,
+                                                             const int* __restrict__ orig, long long n_sorted,
+                                                             const int* __restrict__ states, int ns_pad,
+                                                             const int* __restrict__ tiles, int n_tiles,
+                                                             const int* __restrict__ prod, int A,
+                                                             cx<RT>* __restrict__ rho) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<double>* sm = reinterpret_cast<cx<double>*>(smem_raw);
+    const int P = n_orb | 1;
+    const int items = n_tiles * A;
+    const long long AP = (long long)A * P;
+    for (long long a0 = (long long)blockIdx.x * A; a0 < n_sorted; a0 += (long long)gridDim.x * A) {
+        const int na = (int)min((long long)A, n_sorted - a0);
+        for (int e = threadIdx.x; e < ns_pad * A * n_orb; e += blockDim.x) {
+            const int o = e % n_orb, r = e / n_orb;
+            const int at = r % A, i = r / A;
+            cx<double>* dst = sm + (i * A + at) * P + o;
+            const int st = states[i];
+            if (st >= 0 && at < na)
+                pd_cp_async16(dst, coeff + ((long long)st * n_atoms + orig[a0 + at]) * n_orb + o);
+            else
+                *dst = mk(0.0, 0.0);
         }
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncthreads();
+        for (int w = threadIdx.x; w < items; w += blockDim.x) {
+            const int t = w / A, a = w - t * A;
+            const int code = tiles[t];
+            const int bi = code & 0xffff, bj = code >> 16;
+            const cx<double>* L = sm + (long long)(kPairTile * bi) * AP + (long long)a * P;
+            const cx<double>* R = sm + (long long)(kPairTile * bj) * AP + (long long)a * P;
+            double ar[kPairTile * kPairTile], ai[kPairTile * kPairTile];
+#pragma unroll
+            for (int k = 0; k < kPairTile * kPairTile; ++k) ar[k] = ai[k] = 0.0;
+#pragma unroll 1
+            for (int o = 0; o < n_orb; ++o) {
+                cx<double> l[kPairTile], r[kPairTile];
+#pragma unroll
+                for (int u = 0; u < kPairTile; ++u) {
+                    l[u] = L[u * AP + o];
+                    r[u] = R[u * AP + o];
+                }
+#pragma unroll
+                for (int u = 0; u < kPairTile; ++u)
+#pragma unroll
+                    for (int v = 0; v < kPairTile; ++v) {
+                        ar[u * kPairTile + v] += l[u].re * r[v].re + l[u].im * r[v].im;  // conj(c_i) c_j
+                        ai[u * kPairTile + v] += l[u].re * r[v].im - l[u].im * r[v].re;
+                    }
+            }
+            if (a < na) {
+                const long long slot = a0 + a;
+#pragma unroll
+                for (int u = 0; u < kPairTile; ++u)
+#pragma unroll
+                    for (int v = 0; v < kPairTile; ++v) {
+                        const int pc = prod[(kPairTile * bi + u) * ns_pad + kPairTile * bj + v];
+                        if (pc >= 0) {
+                            const double im = (pc & 1) ? -ai[u * kPairTile + v] : ai[u * kPairTile + v];
+                            rho[(long long)(pc >> 1) * n_sorted + slot] = narrow<RT>(mk(ar[u * kPairTile + v], im));
+                        }
+                    }
+            }
+        }
+        __syncthreads();  // the stage is refilled for the next atoms
     }
 }
 

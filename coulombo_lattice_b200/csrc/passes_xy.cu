@@ -42,7 +42,7 @@ bool xyfwd(cudaStream_t s, const cx<T>* rho, long long rho_stride, const int* ro
         using Tag = decltype(tag);
         constexpr int TH = decltype(threads)::value, MB = decltype(minb)::value;
         auto kern = clk::k_xyfwd_plane<T, Tag::r1, Tag::r2, TH, MB>;
-        const size_t smem = clk::PlaneSmem<T, Tag::r1, Tag::r2, TH, true>::bytes;
+        const size_t smem = clk::PlaneSmem<T, Tag::r1, Tag::r2, TH, true, MB>::bytes;
         set_smem(kern, smem);
         kern<<<dim3((unsigned)nz, plane_groups(nz, cnt, MB)), TH, smem, s>>>(rho, rho_stride, row_ptr, cell, buf, M,
                                                                              tw, rp, cnt);

@@ -99,8 +99,10 @@ struct PlaneLayout {
 };
 
 // Shared memory of the plane kernels: the plane, the twiddles W_N^(t j) laid out [t][j], the atom phases (forward),
-// the atom masks and the row and item tables.
-template <typename T, int R1, int R2, int THREADS, bool FWD>
+// the atom masks and the row and item tables; then (forward, one block an SM, where it holds
+// more atoms than the register slots) the staging of a plane's atom values for the next
+// density, KS of them, and their plane positions.
+template <typename T, int R1, int R2, int THREADS, bool FWD, int MINB = 1>
 struct PlaneSmem {
     using L = PlaneLayout<T, R1, R2>;
     static constexpr int KA = 4;                   // atoms a thread keeps (slots) across densities
@@ -108,8 +110,23 @@ struct PlaneSmem {
     static constexpr int AW = (NI + 3) / 4;        // words of the byte masks amask
     static constexpr size_t elems = (size_t)L::N * L::LDP + L::N + (FWD ? (size_t)KA * THREADS : 0);
     static constexpr size_t shorts = 4 * (size_t)L::N + 2 + NI;  // prl, lst, tmask, items
-    static constexpr size_t bytes = sizeof(cx<T>) * elems + 4 * (size_t)AW + 2 * shorts;
+    static constexpr size_t base_bytes = sizeof(cx<T>) * elems + 4 * (size_t)AW + 2 * shorts;
+    static constexpr size_t stage_off = (base_bytes + 15) / 16 * 16;
+    static constexpr long long ks_fit =
+        (FWD && MINB == 1) ? ((227LL * 1024 - (long long)stage_off) / (long long)(sizeof(cx<T>) + 4)) / 256 * 256 : 0;
+    static constexpr int KS = ks_fit > (long long)KA * THREADS ? (int)(ks_fit < 8192 ? ks_fit : 8192) : 0;
+    static constexpr size_t bytes = KS ? stage_off + (size_t)KS * (sizeof(cx<T>) + 4) : base_bytes;
 };
+
+// Asynchronous copy of one complex value (8 or 16 bytes) from HBM to shared memory.
+template <typename T>
+__device__ __forceinline__ void cp_async_cx(cx<T>* dst, const cx<T>* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    if constexpr (sizeof(cx<T>) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
 
 // Row tables of the block's plane (rp = the plane's slice of the row CSR): the physical rows
 // (pr = y, or dig(y) for digit-order rows) of the rows with atoms, paired class 0 with class 1
@@ -260,12 +277,14 @@ __global__ void __launch_bounds__(THREADS, MINB)
                   const int* __restrict__ cell, cx<T>* __restrict__ out, long long out_stride,
                   const cx<T>* __restrict__ tw_g, RoundPhase rp, int np) {
     using L = PlaneLayout<T, R1, R2>;
-    using Sm = PlaneSmem<T, R1, R2, THREADS, true>;
+    using Sm = PlaneSmem<T, R1, R2, THREADS, true, MINB>;
     static_assert(R1 <= 8 && R2 <= 16 && L::N <= 128, "plane stages serve 16 lanes a row (phase A) and 8 (phase B)");
     static_assert(L::kConflictFree, "plane layout has bank conflicts");
-    constexpr int N = L::N, KA = Sm::KA, NW = (N + 31) / 32;
+    constexpr int N = L::N, KA = Sm::KA, NW = (N + 31) / 32, KS = Sm::KS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const PlaneTables<T, R1, R2, THREADS, true> tb(smem_raw);
+    cx<T>* const stg = reinterpret_cast<cx<T>*>(smem_raw + Sm::stage_off);  // KS atom values
+    int* const slt = reinterpret_cast<int*>(stg + KS);                      // their plane positions
     cx<T>* const plane = tb.plane;
     const cx<T>* const tw = tb.tw;
     __shared__ unsigned live_mask[4];
@@ -295,6 +314,23 @@ __global__ void __launch_bounds__(THREADS, MINB)
             tb.phs[k * THREADS + tid] = narrow<T>(round_phase(rp, x, y, z));
         }
     }
+    // planes with more atoms than the register slots: the next density's atom values are copied
+    // into shared memory (cp.async, each thread the atoms it scatters) while this one is
+    // transformed
+    const bool staged = KS > 0 && !pre && (a1 - a0) <= KS;
+    const bool has_phase = (rp.kx | rp.ky | rp.kz) != 0;
+    if (staged) {
+        for (int i = tid; i < a1 - a0; i += THREADS) {
+            const int c = cell[a0 + i];
+            const int row = c / N, x = c - row * N, y = row - r0;
+            slt[i] = L::rowbase(y) + L::pos(x);
+        }
+    }
+    const auto stage_issue = [&](int p) {
+        const cx<T>* src = rho + (long long)p * rho_stride + a0;
+        for (int i = tid; i < a1 - a0; i += THREADS) cp_async_cx(stg + i, src + i);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
     const int per = (np + gridDim.y - 1) / gridDim.y;
     const int p_begin = blockIdx.y * per, p_end = min(np, p_begin + per);
     cx<T> rv[KA], rn[KA];
@@ -304,6 +340,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
         for (int k = 0; k < KA; ++k) v[k] = slot[k] >= 0 ? src[k * THREADS] : mk(T(0), T(0));
     };
     if (pre && p_begin < p_end) load(p_begin, rv);
+    if (staged && p_begin < p_end) stage_issue(p_begin);
     __syncthreads();
     // The plane is never cleared: every read below takes only points written for the current
     // density (atom points, masked by amask / tmask / the live rows) and zero for the rest.
@@ -313,6 +350,17 @@ __global__ void __launch_bounds__(THREADS, MINB)
             for (int k = 0; k < KA; ++k)
                 if (slot[k] >= 0) plane[slot[k]] = cmulc(rv[k], tb.phs[k * THREADS + tid]);
             if (p + 1 < p_end) load(p + 1, rn);
+        } else if (staged) {
+            asm volatile("cp.async.wait_all;\n" ::: "memory");  // this thread's copies of density p
+            for (int i = tid; i < a1 - a0; i += THREADS) {
+                cx<T> v = stg[i];
+                if (has_phase) {
+                    const int c = cell[a0 + i];
+                    const int row = c / N, x = c - row * N, y = row - r0;
+                    v = narrow<T>(cmulc(widen(v), round_phase(rp, x, y, z)));
+                }
+                plane[slt[i]] = v;
+            }
         } else {
             const cx<T>* rp_ = rho + (long long)p * rho_stride;
             for (int i = a0 + tid; i < a1; i += THREADS) {
@@ -322,6 +370,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
         }
         __syncthreads();
+        if (staged && p + 1 < p_end) stage_issue(p + 1);  // every value of density p is scattered
         // x, phase A: the items (row, t) with atoms, their atom points only
         for (int i = tid; i < n_items; i += THREADS) {
             const int code = tb.items[i];

@@ -299,7 +299,10 @@ __global__ void __launch_bounds__(kSlMaxClasses * L * ColShape<R1, R2>::P, 1)
                 cx<T> w[R1];
 #pragma unroll
                 for (int j = 0; j < R1; ++j) w[j] = j < HALF ? v[a][j] : mk(T(0), T(0));
-                dft<R1, -1>(w);
+                if constexpr (R1 == 8)
+                    dft8_half_in<-1>(w);
+                else
+                    dft<R1, -1>(w);
 #pragma unroll
                 for (int r = 0; r < R1; ++r) s0[(q * R1 + r) * LP0 + line] = w[r];
             }
@@ -403,7 +406,10 @@ __global__ void __launch_bounds__(kSlMaxClasses * L * ColShape<R1, R2>::P, 1)
                 for (int r = 0; r < R1; ++r) w[r] = s0[(q + r * R2) * LP0 + line];
 #pragma unroll
                 for (int r = 1; r < R1; ++r) w[r] = cmulc(w[r], tw[r * q]);
-                dft<R1, +1>(w);
+                if constexpr (R1 == 8)
+                    dft8_half_out<+1>(w);  // outputs r < 4 only
+                else
+                    dft<R1, +1>(w);
                 if (valid) {
 #pragma unroll
                     for (int r = 0; r < HALF; ++r) dst[(long long)(q + R2 * r) * nxy] = w[r];

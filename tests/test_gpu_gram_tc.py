@@ -1,6 +1,7 @@
-"""The split-precision tensor-core Gram of the FP32 form (TF32 hi/lo operands, tcgen05 MMAs,
-FP64 accumulation across 64-atom chunks) against the FP64 Gram on the same potentials and
-against the oracle."""
+"""The split-precision tensor-core Gram of the FP32 forms (TF32 hi/lo operands, tcgen05 MMAs,
+FP64 accumulation across 32-atom k-tiles) against the FP64 Gram on the same potentials and
+against the oracle; and the fused Gram of the FP32 sub-lattice form (split inside the kernel)
+against the separate split pass."""
 import numpy as np
 import pytest
 
@@ -13,12 +14,12 @@ pytestmark = pytest.mark.gpu
 STEP = (synth.A_ZB / 4,) * 3
 
 
-def _run(d, specs, holes, env=None, monkeypatch=None, profile=False):
+def _run(d, specs, holes, env=None, monkeypatch=None, profile=False, mode=cl.MODE_FP32_ROUNDS):
     if env:
         for k, v in env.items():
             monkeypatch.setenv(k, v)
     try:
-        with cl.CoulombCalculator(d["dims"], STEP, cl.MODE_FP32_ROUNDS) as cc:
+        with cl.CoulombCalculator(d["dims"], STEP, mode) as cc:
             cc.initialize(dielectric=10.89)
             cc.set_states(d["states"], d["cells_idx"], holes)
             if profile:
@@ -119,3 +120,47 @@ def test_profile_recorded_inside_graph():
     for k, (ms, n, nbytes) in prof.items():
         assert n == 3 * eager[k][1] and ms > 0
         assert nbytes == pytest.approx(3 * eager[k][2])
+
+
+SL32 = cl.MODE_FP32_SUBLATTICE
+
+
+def _fused_vs_split(d, specs, holes, monkeypatch):
+    # CL_TC_FUSED: the fused Gram also where the operands span several tiles
+    got, prof = _run(d, specs, holes, env={"CL_TC_FUSED": "1"}, monkeypatch=monkeypatch, profile=True, mode=SL32)
+    assert "gram_split" not in prof and prof["gram"][1] >= 1
+    ref, prof_s = _run(d, specs, holes, env={"CL_TC_SPLIT": "1"}, monkeypatch=monkeypatch, profile=True, mode=SL32)
+    assert "gram_split" in prof_s
+    # the same TF32 parts and the same MMAs: only the order of the FP64 additions differs
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    return got
+
+
+def test_fused_gram_matches_split_pass_and_oracle(monkeypatch):
+    d = synth.build("c1")
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    got = _fused_vs_split(d, specs, 2, monkeypatch)
+    want = _oracle(d, specs)
+    lim = np.maximum(1e-6 * np.abs(want), 1e-9)
+    assert np.all(np.abs(got - want) <= lim), (np.abs(got - want) / lim).max()
+
+
+@pytest.mark.parametrize("cells", [(2, 2, 2), (3, 2, 5), (1, 1, 1)])
+def test_fused_gram_ragged_and_tiny_atom_ranges(cells, monkeypatch):
+    """64, 240 and 8 atoms: a partial last k-tile, and a block of one k-tile."""
+    d = synth.build("c1", cells=cells)
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    got = _fused_vs_split(d, specs, 2, monkeypatch)
+    want = _oracle(d, specs)
+    lim = np.maximum(1e-6 * np.abs(want), 1e-9)
+    assert np.all(np.abs(got - want) <= lim), (np.abs(got - want) / lim).max()
+
+
+@pytest.mark.parametrize("n_states", [5, 9, 12])
+def test_fused_gram_right_tile_widths_and_several_tiles(n_states, monkeypatch):
+    """15, 45 and 78 right densities: MMA widths 32, 96, and 128 + 32 over two right tiles (and
+    two left tiles at 12 states), each block converting its own tiles' densities."""
+    d = synth.build("c2", cells=(4, 5, 4))
+    d["states"] = d["states"][:n_states, :, :8]
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", n_states, n_states // 2)][::5]
+    _fused_vs_split(d, specs, n_states // 2, monkeypatch)

@@ -59,7 +59,9 @@ def test_plane_passes_on_zincblende_atoms(mode, cells, monkeypatch):
                          ids=["fp32-96", "fp64-96", "fp32-128", "fp32-64", "fp64-64"])
 def test_plane_passes_on_scattered_atoms(mode, n, monkeypatch):
     """Atoms on random distinct cells: live rows of both classes in every plane, unpaired rows,
-    and a first plane holding more atoms (2,100) than a block keeps in registers."""
+    and a first plane holding more atoms (2,100) than a block keeps in registers (copied ahead
+    through shared memory where the plane kernel has room, read directly otherwise); the grid
+    API below has planes with more atoms than that room."""
     d = synth.build("c1", cells=(n // 4, n // 4, 2))
     n_atoms = d["states"].shape[1]
     rng = np.random.default_rng(n)
