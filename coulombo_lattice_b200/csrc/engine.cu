@@ -23,6 +23,7 @@
 #include "host/status.hpp"
 #include "kernels.cuh"
 #include "passes.hpp"
+#include "gram_dmma.cuh"
 #include "gram_tc.cuh"
 #include "sublattice.cuh"
 
@@ -286,6 +287,7 @@ struct cl_ctx {
     long long n_atoms = 0, n_sorted = 0;
     DevBuf<cx<double>> coeff;
     DevBuf<int> cell_sorted, orig_sorted, row_ptr;
+    DevBuf<cx<double>> coeff_stage;  // two states of caller coefficients, input atom order
     long long live_rows = 0;           // rows (y, z) holding at least one atom
     std::vector<long long> atom_slot;  // input atom -> sorted (deduplicated) slot
     std::vector<int64_t> cells_seen;   // the cells of the last load (an identical list skips the sort)
@@ -1200,10 +1202,26 @@ bool fused_gram(bool v_f32, bool rho_f32, int nl, int nr) {
     return 2 * nl <= clk::tc::BM && 2 * nr <= clk::tc::BN;
 }
 
+// Reductions of the FP32 forms over fewer than 65,536 atoms (CL_TC_MIN_ATOMS) are summed in
+// FP64: the FP64 tensor-core Gram (k_gram_dmma) on FP32 potentials and densities, k_gram on FP64
+// potentials.  The TF32x3 Gram's error is ~2^-23 of each product, random in sign, so relative to
+// the sum of the terms' magnitudes it falls as 1/sqrt(atoms): at 2M atoms it is far below the
+// FP32 gate even where the terms cancel 1000:1, while on a box of a hundred atoms it can reach
+// the 1e-9 eV floor on integrals that small.  Below the threshold the FP64 Gram costs little.
+long long tc_min_atoms() {
+    const char* e = std::getenv("CL_TC_MIN_ATOMS");
+    return e ? std::atoll(e) : 65536LL;
+}
+bool small_gram(const cl_ctx* c, long long n_atoms) {
+    return !fp64_form(c) && n_atoms < tc_min_atoms() && !std::getenv("CL_TC_FUSED") && !std::getenv("CL_TC_SPLIT");
+}
+
 // Operand buffer for (nl, nr, n_atoms): whole atom range when it fits in a quarter of the free
 // device memory (at most 8 GiB), else chunks of the atom range.  Called outside any capture.
 void tc_reserve(cl_ctx* c, int nl, int nr, long long n_atoms, bool v_f32, bool rho_f32) {
-    if (!use_tc_gram(c) || nl <= 0 || nr <= 0 || n_atoms <= 0 || fused_gram(v_f32, rho_f32, nl, nr)) return;
+    if (!use_tc_gram(c) || nl <= 0 || nr <= 0 || n_atoms <= 0 || fused_gram(v_f32, rho_f32, nl, nr) ||
+        small_gram(c, n_atoms))
+        return;
     const int rowsA = 2 * nl, rowsB = 2 * nr;
     const long long per_atom = tc_bytes_per_atom(rowsA, rowsB);
     const long long full = (n_atoms + clk::tc::BK - 1) / clk::tc::BK * clk::tc::BK;
@@ -1235,6 +1253,40 @@ int gram_splits(int tiles, int kt_total) {
         }
     }
     return best_s;
+}
+
+// The FP64 tensor-core Gram on FP32 operands over the whole atom range (see k_gram_dmma).
+void gram_dmma(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, const cx<float>* rho, long long r_stride,
+               const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
+    using namespace clk::dm;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        CL_CUDA(cudaFuncSetAttribute(k_gram_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    });
+    const int tilesA = (2 * nl + TILE - 1) / TILE, tilesB = (2 * nr + TILE - 1) / TILE;
+    const int nA4 = (std::min(TILE / 2, nl) + 3) & ~3, nB4 = (std::min(TILE / 2, nr) + 3) & ~3;
+    GramArgs g{};
+    g.V = reinterpret_cast<const float2*>(V);
+    g.v_stride = v_stride;
+    g.rho = reinterpret_cast<const float2*>(rho);
+    g.r_stride = r_stride;
+    g.ridx = ridx_dev;
+    g.nl = nl;
+    g.nr = nr;
+    g.na = n_atoms;
+    g.nd_max = nA4 + nB4;
+    g.out4 = out4_dev;
+    const int chunks = (int)std::min<long long>((n_atoms + KC - 1) / KC, 1LL << 30);
+    const int splits0 = gram_splits(tilesA * tilesB, chunks);
+    const long long per_chunks = (chunks + splits0 - 1) / splits0;
+    g.atoms_per_split = per_chunks * KC;
+    const int splits = (int)((n_atoms + g.atoms_per_split - 1) / g.atoms_per_split);
+    const size_t smem = smem_bytes(g.nd_max);
+    if (smem > 227 * 1024) cl::fail(CL_ERR_UNSUPPORTED, "FP64 Gram needs %zu bytes of shared memory", smem);
+    cudaEvent_t e = prof_begin(c);
+    k_gram_dmma<<<dim3(tilesA, tilesB, splits), THREADS, smem, c->stream>>>(g);
+    CL_LAUNCHED();
+    prof_end(c, e, CL_KCLASS_GRAM, (double)n_atoms * (nl + nr) * (double)sizeof(cx<float>));
 }
 
 // The fused Gram on FP32 operands over the whole atom range (see k_gram_tc_fused).
@@ -1348,7 +1400,13 @@ void check_gram_slot(double slot) {
 void gram(cl_ctx* c, const void* V_any, bool v_f32, long long v_stride, int nl, const void* rho_any, bool rho_f32,
           long long r_stride, const int* ridx_dev, int nr, long long n_atoms, double* out4_dev) {
     CL_CUDA(cudaMemsetAsync(out4_dev, 0, sizeof(double) * (4 * (size_t)nl * nr + 1), c->stream));
-    if (use_tc_gram(c)) {
+    const bool small = small_gram(c, n_atoms);
+    if (small && v_f32 && rho_f32) {
+        gram_dmma(c, static_cast<const cx<float>*>(V_any), v_stride, nl, static_cast<const cx<float>*>(rho_any),
+                  r_stride, ridx_dev, nr, n_atoms, out4_dev);
+        return;
+    }
+    if (use_tc_gram(c) && !small) {
         gram_tc(c, V_any, v_f32, v_stride, nl, rho_any, rho_f32, r_stride, ridx_dev, nr, n_atoms, out4_dev);
         return;
     }
@@ -1574,13 +1632,13 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
             const size_t smem = 2 * sizeof(cx<double>) * clk::pair_stage_elems(NS);
             ensure_smem(clk::k_pair_density_reg<NS, double>, smem);
             clk::k_pair_density_reg<NS, double><<<ps.grid_reg, clk::kPairAtoms * clk::pair_parts(NS), smem, c->stream>>>(
-                c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
+                c->coeff.p, c->n_sorted, c->n_orb, nullptr, c->n_sorted, ps.tri, out);
         };
         with_states(ps.n_used, go);
     } else if (fp64_form(c) && !ps.tile_ok) {
         ensure_smem(clk::k_pair_density<double>, ps.smem);
         clk::k_pair_density<double><<<ps.blocks, 256, ps.smem, c->stream>>>(
-            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
+            c->coeff.p, c->n_sorted, c->n_orb, nullptr, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<double>*>(rho));
     } else if (ps.reg_ok) {
         cx<float>* out = static_cast<cx<float>*>(rho);
@@ -1589,7 +1647,7 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
             const size_t smem = 2 * sizeof(cx<double>) * clk::pair_stage_elems(NS);
             ensure_smem(clk::k_pair_density_reg<NS, float>, smem);
             clk::k_pair_density_reg<NS, float><<<ps.grid_reg, clk::kPairAtoms * clk::pair_parts(NS), smem, c->stream>>>(
-                c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tri, out);
+                c->coeff.p, c->n_sorted, c->n_orb, nullptr, c->n_sorted, ps.tri, out);
         };
         with_states(ps.n_used, go);
     } else if (ps.tile_ok) {  // more than 12 states: 4 x 4-state tiles (FP64 sums, rounded once)
@@ -1597,7 +1655,7 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
             using RT = decltype(tag);
             ensure_smem(clk::k_pair_density_tile<RT>, ps.tile_smem);
             clk::k_pair_density_tile<RT><<<ps.tile_blocks, ps.tile_threads, ps.tile_smem, c->stream>>>(
-                c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.tile_states.p, ps.ns_pad,
+                c->coeff.p, c->n_sorted, c->n_orb, nullptr, c->n_sorted, ps.tile_states.p, ps.ns_pad,
                 ps.tiles.p, ps.n_tiles, ps.tile_prod.p, ps.tile_atoms, static_cast<cx<RT>*>(rho));
         };
         if (fp64_form(c))
@@ -1607,12 +1665,12 @@ void pair_launch(cl_ctx* c, const PairSetup& ps, void* rho) {
     } else {  // the segment kernel (FP64 sums, rounded once)
         ensure_smem(clk::k_pair_density<float>, ps.smem);
         clk::k_pair_density<float><<<ps.blocks, 256, ps.smem, c->stream>>>(
-            c->coeff.p, c->n_atoms, c->n_orb, c->orig_sorted.p, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
+            c->coeff.p, c->n_sorted, c->n_orb, nullptr, c->n_sorted, ps.segs.p, ps.n_segs, ps.states.p,
             ps.n_used, ps.chunk, static_cast<cx<float>*>(rho));
     }
     CL_LAUNCHED();
     prof_end(c, e, CL_KCLASS_DENSITY,
-             (double)ps.n_used * c->n_atoms * c->n_orb * 16.0 + (double)ps.np * c->n_sorted * rho_bytes(c));
+             (double)ps.n_used * c->n_sorted * c->n_orb * 16.0 + (double)ps.np * c->n_sorted * rho_bytes(c));
 }
 
 void pair_densities(cl_ctx* c, const std::vector<int2>& fl, void* rho) {
@@ -1964,6 +2022,25 @@ void load_cells(cl_ctx* c, int64_t n_atoms, const int64_t* cells) {
     c->cells_seen.assign(cells, cells + n_atoms);
 }
 
+// Uploads state s of the caller's coefficients ([state][atom][orb], input atom order) through
+// a staging slot and stores it in the cell-sorted atom order the pair-density kernels read
+// (k_gather_atoms): consecutive slots of a block are then contiguous rows in HBM.  Both on
+// `stream`, so slot s & 1 is free again once the gather of state s - 2 has run.
+void upload_state_sorted(cl_ctx* c, int s, const double* coeff, cudaStream_t stream) {
+    const size_t per_in = (size_t)c->n_atoms * c->n_orb, per_s = (size_t)c->n_sorted * c->n_orb;
+    cx<double>* slot = c->coeff_stage.p + (size_t)(s & 1) * per_in;
+    CL_CUDA(cudaMemcpyAsync(slot, coeff + 2 * (size_t)s * per_in, sizeof(cx<double>) * per_in, cudaMemcpyHostToDevice,
+                            stream));
+    const int blocks = (int)std::max<long long>(1, std::min<long long>(((long long)per_s + 255) / 256, 148LL * 16));
+    clk::k_gather_atoms<<<blocks, 256, 0, stream>>>(slot, c->orig_sorted.p, c->n_sorted, c->n_orb,
+                                                    c->coeff.p + (size_t)s * per_s);
+    CL_LAUNCHED();
+}
+void reserve_coeff(cl_ctx* c, int n_states) {
+    grow(c->coeff, (size_t)n_states * c->n_sorted * c->n_orb);
+    grow(c->coeff_stage, 2 * (size_t)c->n_atoms * c->n_orb);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1978,7 +2055,8 @@ int cl_set_states(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, int n_o
         c->n_holes = n_holes;
         c->n_orb = n_orb;
         c->n_atoms = n_atoms;
-        c->coeff.upload(reinterpret_cast<const cx<double>*>(coeff), (size_t)n_states * n_atoms * n_orb, c->stream);
+        reserve_coeff(c, n_states);
+        for (int s = 0; s < n_states; ++s) upload_state_sorted(c, s, coeff, c->stream);
         CL_CUDA(cudaStreamSynchronize(c->stream));
     });
 }
@@ -2125,8 +2203,7 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     c->n_holes = n_holes;
     c->n_orb = n_orb;
     c->n_atoms = n_atoms;
-    const size_t per_state = (size_t)n_atoms * n_orb;
-    grow(c->coeff, (size_t)n_states * per_state);
+    reserve_coeff(c, n_states);
     std::memset(c->timings, 0, sizeof c->timings);
     if (!c->copy_stream) CL_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     while ((int)c->state_ev.size() < n_states) {
@@ -2135,8 +2212,7 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
         c->state_ev.push_back(e);
     }
     if (n_int == 0) {
-        CL_CUDA(cudaMemcpyAsync(c->coeff.p, coeff, sizeof(cx<double>) * n_states * per_state, cudaMemcpyHostToDevice,
-                                c->stream));
+        for (int s = 0; s < n_states; ++s) upload_state_sorted(c, s, coeff, c->stream);
         CL_CUDA(cudaStreamSynchronize(c->stream));
         return;
     }
@@ -2167,8 +2243,7 @@ void compute_states_impl(cl_ctx* c, int n_states, int n_holes, int64_t n_atoms, 
     int uploaded = 0;
     const auto upload_through = [&](int last) {
         for (; uploaded <= last && uploaded < n_states; ++uploaded) {
-            CL_CUDA(cudaMemcpyAsync(c->coeff.p + uploaded * per_state, coeff + 2 * uploaded * per_state,
-                                    sizeof(cx<double>) * per_state, cudaMemcpyHostToDevice, c->copy_stream));
+            upload_state_sorted(c, uploaded, coeff, c->copy_stream);
             CL_CUDA(cudaEventRecord(c->state_ev[uploaded], c->copy_stream));
         }
     };

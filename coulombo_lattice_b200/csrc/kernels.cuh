@@ -147,8 +147,27 @@ __global__ void k_khat(const double* __restrict__ ghat, int nx, int ny, int nz, 
 
 // ---------------------------------------------------------------------------------------
 // Pair densities at atoms: rho_p(a) = sum_o conj(c_fl[a][o]) c_fr[a][o]  (Product.cpp:16-30).
-// coeff is [state][atom][orb] in input atom order; orig maps sorted -> input atom.
+// coeff is [state][atom][orb] with n_atoms atoms a state; the atom of sorted slot i is
+// orig[i], or i itself when orig is null (coefficients already in sorted order: the library
+// stores them so, see k_gather_atoms).
 // ---------------------------------------------------------------------------------------
+__device__ __forceinline__ long long atom_of(const int* __restrict__ orig, long long i) {
+    return orig ? (long long)orig[i] : i;
+}
+
+// dst[i][o] = src[orig[i]][o] for the n_sorted slots and n_orb orbitals of one state: the
+// coefficients of a state in the cell-sorted order of the atoms (consecutive threads on
+// consecutive orbitals: whole 16-byte values, rows of n_orb contiguous on both sides).
+static __global__ void __launch_bounds__(256) k_gather_atoms(const cx<double>* __restrict__ src,
+                                                     const int* __restrict__ orig, long long n_sorted, int n_orb,
+                                                     cx<double>* __restrict__ dst) {
+    const long long n = n_sorted * n_orb;
+    for (long long e = blockIdx.x * 256LL + threadIdx.x; e < n; e += (long long)gridDim.x * 256) {
+        const long long i = e / n_orb;
+        const int o = (int)(e - i * n_orb);
+        dst[e] = src[(long long)orig[i] * n_orb + o];
+    }
+}
 __device__ __forceinline__ void pd_cp_async16(void* smem_dst, const void* gmem_src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
                      static_cast<unsigned>(__cvta_generic_to_shared(smem_dst))),
@@ -188,7 +207,7 @@ __global__ void __launch_bounds__(256) k_pair_density(const cx<double>* __restri
         const int ca = (int)min((long long)chunk, n_sorted - i0);
         for (int row = warp; row < n_used * ca; row += nwarps) {
             const int su = row / ca, a = row - su * ca;
-            const cx<double>* src = coeff + ((long long)states[su] * n_atoms + orig[i0 + a]) * n_orb;
+            const cx<double>* src = coeff + ((long long)states[su] * n_atoms + atom_of(orig, i0 + a)) * n_orb;
             cx<double>* dst = sc + (su * chunk + a) * os;
             for (int k = lane; k < n_orb; k += 32) pd_cp_async16(dst + k, src + k);
         }
@@ -342,7 +361,7 @@ __global__ void __launch_bounds__(kPairAtoms * pair_parts(NS), pair_min_blocks(N
             const int orb = slice * kPairOrbSlice + o;
             cx<double>* dst = st + (i * kPairAtoms + at) * (kPairOrbSlice + 1) + o;
             if (at < na && orb < n_orb)
-                pd_cp_async16(dst, coeff + ((long long)tri.states[i] * n_atoms + orig[a0 + at]) * n_orb + orb);
+                pd_cp_async16(dst, coeff + ((long long)tri.states[i] * n_atoms + atom_of(orig, a0 + at)) * n_orb + orb);
             else
                 *dst = mk(0.0, 0.0);
         }
@@ -410,7 +429,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_density_tile(const cx<double>* 
             cx<double>* dst = sm + (i * A + at) * P + o;
             const int st = states[i];
             if (st >= 0 && at < na)
-                pd_cp_async16(dst, coeff + ((long long)st * n_atoms + orig[a0 + at]) * n_orb + o);
+                pd_cp_async16(dst, coeff + ((long long)st * n_atoms + atom_of(orig, a0 + at)) * n_orb + o);
             else
                 *dst = mk(0.0, 0.0);
         }

@@ -14,6 +14,13 @@ pytestmark = pytest.mark.gpu
 STEP = (synth.A_ZB / 4,) * 3
 
 
+@pytest.fixture(autouse=True)
+def _tf32_gram_at_any_size(monkeypatch):
+    """The FP32 forms sum the reductions of boxes under 65,536 atoms in FP64; these small test
+    boxes take the TF32x3 Gram unless a test removes this."""
+    monkeypatch.setenv("CL_TC_MIN_ATOMS", "0")
+
+
 def _run(d, specs, holes, env=None, monkeypatch=None, profile=False, mode=cl.MODE_FP32_ROUNDS):
     if env:
         for k, v in env.items():
@@ -164,3 +171,35 @@ def test_fused_gram_right_tile_widths_and_several_tiles(n_states, monkeypatch):
     d["states"] = d["states"][:n_states, :, :8]
     specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", n_states, n_states // 2)][::5]
     _fused_vs_split(d, specs, n_states // 2, monkeypatch)
+
+
+def _dmma_vs_tf32(d, specs, holes, monkeypatch):
+    """The FP64 tensor-core Gram (the FP32 sub-lattice form's Gram under 65,536 atoms) against
+    the TF32x3 Gram on the same potentials and against the oracle."""
+    monkeypatch.delenv("CL_TC_MIN_ATOMS", raising=False)
+    got, prof = _run(d, specs, holes, profile=True, mode=SL32)
+    assert "gram_split" not in prof and prof["gram"][1] >= 1
+    tf32, _ = _run(d, specs, holes, env={"CL_TC_FUSED": "1"}, monkeypatch=monkeypatch, mode=SL32)
+    want = _oracle(d, specs)
+    lim = np.maximum(1e-6 * np.abs(want), 1e-9)
+    assert np.all(np.abs(got - want) <= lim), (np.abs(got - want) / lim).max()
+    # TF32x3 sums carry ~2^-22 per product; FP64 sums carry none of it
+    assert np.all(np.abs(got - tf32) <= lim)
+    return got
+
+
+@pytest.mark.parametrize("cells", [(4, 4, 4), (3, 2, 5), (1, 1, 1)])
+def test_fp64_tensor_core_gram(cells, monkeypatch):
+    """1,024, 240 and 8 atoms: several chunks, a partial last chunk, one chunk of one block."""
+    d = synth.build("c1", cells=cells)
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+    _dmma_vs_tf32(d, specs, 2, monkeypatch)
+
+
+def test_fp64_tensor_core_gram_two_tiles_each_side(monkeypatch):
+    """12 states: 78 densities a side, 156 Gram rows: 2 x 2 blocks of 128 x 128, the second
+    of each side partial (14 densities, zero rows beyond)."""
+    d = synth.build("c2", cells=(4, 5, 4))
+    d["states"] = d["states"][:, :, :8]
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 12, 6)][::5]
+    _dmma_vs_tf32(d, specs, 6, monkeypatch)
