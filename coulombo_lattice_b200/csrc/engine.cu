@@ -1297,6 +1297,7 @@ void gram_tc_fused(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, co
     std::call_once(once, [] {
         CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     });
     const int tilesA = (2 * nl + BM - 1) / BM, tilesB = (2 * nr + BN - 1) / BN;
     const int nA = std::min(BM / 2, nl), nB = std::min(BN / 2, nr);
@@ -1317,12 +1318,16 @@ void gram_tc_fused(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, co
     const int splits0 = gram_splits(tilesA * tilesB, g.kt_total);
     g.kt_per = (g.kt_total + splits0 - 1) / splits0;
     const int splits = (g.kt_total + g.kt_per - 1) / g.kt_per;
+    // the deepest copy ring that fits: 5 k-tiles ahead (6 slots) at the 2.1M-atom box's 72 densities
+    const size_t smem5 = fused_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 5);
     const size_t smem3 = fused_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 3);
     const size_t smem2 = fused_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 2);
     if (smem2 > 227 * 1024) cl::fail(CL_ERR_UNSUPPORTED, "fused Gram needs %zu bytes of shared memory", smem2);
     cudaEvent_t e = prof_begin(c);
     const dim3 grid(tilesA, tilesB, splits);
-    if (smem3 <= 227 * 1024)
+    if (smem5 <= 227 * 1024)
+        k_gram_tc_fused<5><<<grid, FUSED_THREADS, smem5, c->stream>>>(g);
+    else if (smem3 <= 227 * 1024)
         k_gram_tc_fused<3><<<grid, FUSED_THREADS, smem3, c->stream>>>(g);
     else
         k_gram_tc_fused<2><<<grid, FUSED_THREADS, smem2, c->stream>>>(g);

@@ -385,7 +385,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 //   copy    8-byte cp.async of the raw complex values of its densities into a ring of AHEAD+1
 //           raw slots, AHEAD tiles ahead: a lane takes 4 consecutive atoms of one density, 8
 //           lanes a density, a warp 4 densities (4w + 64j + lane/8: left densities of the
-//           block's A tile, then right densities of its B tile);
+//           block's A tile, then right densities of its B tile); a density's 256-byte raw row
+//           holds each lane's first two atoms in its first half and the other two in its second;
 //   convert round the lane's 4 values to TF32 hi and lo parts and store them with four 16-byte
 //           stores (re hi, im hi, re lo, im lo) into the MMA stage in the 128-byte-swizzled
 //           K-major layout the descriptors expect -- row r, atoms 4c..4c+3 at (r/8)*1024 +
@@ -551,13 +552,16 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedG
     for (int i = 0; i < 32; ++i) acc[i] = 0.0;
     const auto issue = [&](int t) {
         const long long at0 = (long long)(kt0 + t) * BK + 4 * quad;
-        const uint32_t slot = base + ring_off + (uint32_t)(t % (AHEAD + 1)) * g.raw_slot_bytes + (uint32_t)quad * 32u;
+        // raw density row (256 B): atoms 4q, 4q+1 at 16 q, atoms 4q+2, 4q+3 at 128 + 16 q, so that
+        // the 8 lanes of a density read two contiguous 128-byte halves
+        const uint32_t slot = base + ring_off + (uint32_t)(t % (AHEAD + 1)) * g.raw_slot_bytes + (uint32_t)quad * 16u;
         for (int i = 4 * warp + dsub; i < nd; i += 4 * FUSED_WARPS) {
             const float2* src = src_tab[i];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const bool in = at0 + e < g.na;
-                cp_async8(slot + (uint32_t)i * 256u + 8u * e, src + (in ? at0 + e : 0LL), in ? 8u : 0u);
+                cp_async8(slot + (uint32_t)i * 256u + 128u * (e >> 1) + 8u * (e & 1), src + (in ? at0 + e : 0LL),
+                          in ? 8u : 0u);
             }
         }
     };
@@ -595,10 +599,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedG
             break;
         }
         unsigned char* stg = gbase + (size_t)s * g.stage_bytes;
-        const unsigned char* rs = gbase + ring_off + (size_t)(t % (AHEAD + 1)) * g.raw_slot_bytes + quad * 32;
+        const unsigned char* rs = gbase + ring_off + (size_t)(t % (AHEAD + 1)) * g.raw_slot_bytes + quad * 16;
         for (int i = 4 * warp + dsub; i < nd; i += 4 * FUSED_WARPS) {
             const float4 z0 = *reinterpret_cast<const float4*>(rs + i * 256);       // atoms 0, 1
-            const float4 z1 = *reinterpret_cast<const float4*>(rs + i * 256 + 16);  // atoms 2, 3
+            const float4 z1 = *reinterpret_cast<const float4*>(rs + i * 256 + 128);  // atoms 2, 3
             const float re[4] = {z0.x, z0.z, z1.x, z1.z}, im[4] = {z0.y, z0.w, z1.y, z1.w};
             float rh[4], ih[4], rl[4], il[4];
 #pragma unroll
