@@ -1008,6 +1008,9 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, v
     const bool reg_y = register_passes_enabled() && clp::split_variants(ny) > 0;
     const int skip_empty = (reg_x && reg_y && !std::getenv("CL_NO_ROW_SKIP")) ? 1 : 0;
     const bool plane_ok = reg_x && reg_y && clp::plane_supported(fp32, nx, ny);
+    // 128 x 128 FP32 class planes: the quadrant forward plane pass (two blocks an SM);
+    // CL_NO_QPLANE=1 keeps the general one
+    const bool qplane = clp::quadrant_supported(fp32, nx, ny) && !std::getenv("CL_NO_QPLANE");
     // no phase in any pass: the rounds' phase tables are never read with kappa = 0
     const clk::RoundPhase rp0{c->ax[0].phase.p, c->ax[1].phase.p, c->ax[2].phase.p, 0, 0, 0};
     cx<T>* out0 = via_tr ? tr : static_cast<cx<T>*>(V_any);
@@ -1055,7 +1058,10 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, v
         const cx<T>* rho_c = rho + (long long)p0 * rho_stride;
         cx<T>* out_c = via_tr ? tr : static_cast<cx<T>*>(V_any) + (long long)p0 * v_stride;
         cudaEvent_t e = prof_begin(c);
-        if (xy_fwd) {
+        if (qplane) {
+            clp::qfwd(c->stream, reinterpret_cast<const cx<float>*>(rho_c), rho_stride, row_ptr, cell,
+                      reinterpret_cast<cx<float>*>(buf), vM, reinterpret_cast<const cx<float>*>(twx), nz, cnt);
+        } else if (xy_fwd) {
             clp::xyfwd<T>(c->stream, rho_c, rho_stride, row_ptr, cell, buf, vM, twx, rp0, nx, ny, nz, cnt);
         } else if (!(reg_x && clp::xfwd<T>(c->stream, v_xf, rho_c, rho_stride, row_ptr, cell, buf, vM, twx, rp0, nx,
                                             ny, nrows, cnt, skip_empty))) {
@@ -1064,9 +1070,9 @@ void run_sublattice(cl_ctx* c, const cx<T>* rho, long long rho_stride, int np, v
                                                                  xt.ld, cnt);
         }
         CL_LAUNCHED();
-        prof_end(c, e, CL_KCLASS_XFWD, cnt * (atoms * (double)sizeof(cx<T>) + (xy_fwd ? 1.0 : live) * gbytes) +
-                                           atoms * 4.0);
-        if (!xy_fwd) {
+        prof_end(c, e, CL_KCLASS_XFWD,
+                 cnt * (atoms * (double)sizeof(cx<T>) + (xy_fwd || qplane ? 1.0 : live) * gbytes) + atoms * 4.0);
+        if (!xy_fwd && !qplane) {
             e = prof_begin(c);
             if (!(reg_y && clp::ycol<-1, T>(c->stream, v_yf, buf, vM, twy, nx, ny, nz, cnt,
                                              skip_empty ? row_ptr : nullptr)))

@@ -73,6 +73,11 @@ bool xinv(cudaStream_t s, Variant v, cx<T>* buf, long long M, const cx<T>* tw, c
 // transformed along x and y and every plane is stored; inverse: planes are transformed back
 // along y and x and the round's values at the atoms are written to out.
 bool plane_supported(bool fp32, int nx, int ny);
+// Quadrant forward plane pass (plane_q.cuh): FP32 128 x 128 sub-lattice planes, atoms in
+// [0, 64)^2.
+bool quadrant_supported(bool fp32, int nx, int ny);
+bool qfwd(cudaStream_t s, const cx<float>* rho, long long rho_stride, const int* row_ptr, const int* cell,
+          cx<float>* buf, long long M, const cx<float>* tw, int nz, int cnt);
 template <typename T>
 bool xyfwd(cudaStream_t s, const cx<T>* rho, long long rho_stride, const int* row_ptr, const int* cell, cx<T>* buf,
            long long M, const cx<T>* tw, const clk::RoundPhase& rp, int nx, int ny, int nz, int cnt);

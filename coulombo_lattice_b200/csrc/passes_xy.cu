@@ -2,6 +2,7 @@
 #include <algorithm>
 
 #include "passes_impl.cuh"
+#include "plane_q.cuh"
 #include "plane_rf.cuh"
 
 namespace clp {
@@ -61,6 +62,16 @@ bool xyinv(cudaStream_t s, cx<T>* buf, long long M, const cx<T>* tw, const int* 
         kern<<<dim3((unsigned)nz, plane_groups(nz, cnt, MB)), TH, smem, s>>>(buf, M, tw, row_ptr, cell, out,
                                                                              o_stride, cnt);
     });
+}
+
+bool quadrant_supported(bool fp32, int nx, int ny) { return fp32 && nx == clk::qp::N && ny == clk::qp::N; }
+
+bool qfwd(cudaStream_t s, const cx<float>* rho, long long rho_stride, const int* row_ptr, const int* cell,
+          cx<float>* buf, long long M, const cx<float>* tw, int nz, int cnt) {
+    set_smem(clk::qp::k_qfwd, clk::qp::SMEM);
+    clk::qp::k_qfwd<<<dim3((unsigned)nz, plane_groups(nz, cnt, 2)), clk::qp::THREADS, clk::qp::SMEM, s>>>(
+        rho, rho_stride, row_ptr, cell, buf, M, tw, cnt);
+    return true;
 }
 
 template bool xyfwd<float>(cudaStream_t, const cx<float>*, long long, const int*, const int*, cx<float>*, long long,

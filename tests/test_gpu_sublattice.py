@@ -189,3 +189,39 @@ def test_round_split_is_refused():
             cc.compute_rounds(specs, 0x0F)
         full = cc.compute_rounds(specs, 0xFF)
         assert np.allclose(full, cc.compute(specs), rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("drop", [0.0, 0.1])
+def test_quadrant_plane_passes(drop, monkeypatch):
+    """128 x 128 class planes (a 64 x 64 x 2-cell box): the FP32 quadrant forward plane pass
+    against the general one (CL_NO_QPLANE=1) and the oracle; with every quadrant point an atom,
+    and with a tenth of the atoms removed (planes that must be cleared between densities)."""
+    cells = (64, 64, 2)
+    lat = synth.zincblende_lattice(cells)
+    if drop:
+        rng = np.random.default_rng(77)
+        lat = lat[rng.random(lat.shape[0]) >= drop]
+    dims = synth.grid_of(cells)
+    st, cc_ = _structure(lat, dims, n_states=4, n_orb=2, seed=13)
+    step = (synth.A_ZB / 4,) * 3
+    specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", 4, 2)]
+
+    def run(no_q):
+        if no_q:
+            monkeypatch.setenv("CL_NO_QPLANE", "1")
+        try:
+            with cl.CoulombCalculator(dims, step, cl.MODE_FP32_SUBLATTICE) as cc:
+                cc.initialize(dielectric=EPS)
+                cc.set_states(st, cc_, 2)
+                info = cc.form_info()
+                return np.asarray(cc.compute(specs)), info
+        finally:
+            monkeypatch.delenv("CL_NO_QPLANE", raising=False)
+
+    got, info = run(False)
+    assert info["sublattice"] and info["lengths"][:2] == (128, 128)
+    ref, _ = run(True)
+    want = np.array(H.compute_integrals(list(st), cc_, dims, step, specs, dielectric=EPS))
+    err, lim = gate(got, want, cl.MODE_FP32_SUBLATTICE)
+    assert np.all(err <= lim), (err / lim).max()
+    assert np.all(np.abs(got - ref) <= 0.25 * lim)
