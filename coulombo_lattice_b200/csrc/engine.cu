@@ -1283,7 +1283,9 @@ void gram_dmma(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, const 
     g.nd_max = nA4 + nB4;
     g.out4 = out4_dev;
     const int chunks = (int)std::min<long long>((n_atoms + KC - 1) / KC, 1LL << 30);
-    const int splits0 = gram_splits(tilesA * tilesB, chunks);
+    // small boxes: enough atom splits to occupy every SM (at least 2 chunks a block)
+    const int splits0 = std::max(gram_splits(tilesA * tilesB, chunks),
+                                 std::min(chunks / 2, (148 + tilesA * tilesB - 1) / (tilesA * tilesB)));
     const long long per_chunks = (chunks + splits0 - 1) / splits0;
     g.atoms_per_split = per_chunks * KC;
     const int splits = (int)((n_atoms + g.atoms_per_split - 1) / g.atoms_per_split);
