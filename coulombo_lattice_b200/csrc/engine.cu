@@ -1306,6 +1306,9 @@ void gram_tc_fused(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, co
         CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         CL_CUDA(cudaFuncSetAttribute(k_gram_tc_fused<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CL_CUDA(cudaFuncSetAttribute(k_gram_tc_ws<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CL_CUDA(cudaFuncSetAttribute(k_gram_tc_ws<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CL_CUDA(cudaFuncSetAttribute(k_gram_tc_ws<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     });
     const int tilesA = (2 * nl + BM - 1) / BM, tilesB = (2 * nr + BN - 1) / BN;
     const int nA = std::min(BM / 2, nl), nB = std::min(BN / 2, nr);
@@ -1333,7 +1336,16 @@ void gram_tc_fused(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, co
     if (smem2 > 227 * 1024) cl::fail(CL_ERR_UNSUPPORTED, "fused Gram needs %zu bytes of shared memory", smem2);
     cudaEvent_t e = prof_begin(c);
     const dim3 grid(tilesA, tilesB, splits);
-    if (smem5 <= 227 * 1024)
+    // up to 40 right densities a block (N <= 80): the warp-specialised kernel; CL_TC_NO_WS=1
+    // keeps the kernel whose warps take every role in turn
+    const bool ws = nb <= WS_MAX_NB && !std::getenv("CL_TC_NO_WS");
+    if (ws && smem5 <= 227 * 1024)
+        k_gram_tc_ws<5><<<grid, WS_THREADS, smem5, c->stream>>>(g);
+    else if (ws && smem3 <= 227 * 1024)
+        k_gram_tc_ws<3><<<grid, WS_THREADS, smem3, c->stream>>>(g);
+    else if (ws)
+        k_gram_tc_ws<2><<<grid, WS_THREADS, smem2, c->stream>>>(g);
+    else if (smem5 <= 227 * 1024)
         k_gram_tc_fused<5><<<grid, FUSED_THREADS, smem5, c->stream>>>(g);
     else if (smem3 <= 227 * 1024)
         k_gram_tc_fused<3><<<grid, FUSED_THREADS, smem3, c->stream>>>(g);

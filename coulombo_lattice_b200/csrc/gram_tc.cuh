@@ -679,5 +679,274 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedG
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// The fused Gram with its roles in separate warps (at most 40 right densities a block: N <= 80),
+// so that the conversion of k-tile t + 1, the MMAs of k-tile t and the drain of k-tile t - 1
+// run at the same time instead of one after another in every warp:
+//   warps 0-6    copy their items' raw values AHEAD k-tiles ahead with 8-byte cp.async (each
+//                thread reads back only its own copies) and convert them: item (density i,
+//                atom pair c) -> TF32 hi and lo of re and im, 8-byte stores into the
+//                128-byte-swizzled K-major stage; then arrive on the stage's full barrier;
+//   warp 7       lane 0 issues the tile's 12 MMAs once the stage is full and its accumulator
+//                buffer drained (three main buffers in tensor memory, the correction in a
+//                fourth), and commits them to the stage's empty and the buffer's full barrier;
+//   warps 8-15   drain: warp w reads lane quarter w % 4, columns [h DC, h DC + DC) for h =
+//                (w - 8) / 4, DC = N / 2, adding them to FP64 registers; the correction
+//                accumulator once after the last k-tile.
+// TF32 rounding to nearest (ties away from zero, as cvt.rna.tf32.f32 for finite values) is done
+// on the integer pipe: add half the weight of the 13 dropped mantissa bits, clear them.
+// ---------------------------------------------------------------------------------------
+constexpr int WS_CONV_WARPS = 7;
+constexpr int WS_MMA_WARP = 7;
+constexpr int WS_DRAIN_WARP0 = 8;
+constexpr int WS_DRAIN_WARPS = 8;
+constexpr int WS_THREADS = 32 * (WS_DRAIN_WARP0 + WS_DRAIN_WARPS);
+constexpr int WS_NACC = 3;         // main accumulator buffers (128 columns apart)
+constexpr int WS_MAX_NB = 80;      // MMA N: at most 40 right densities
+constexpr int WS_MAX_DC = WS_MAX_NB / 2;
+
+__device__ __forceinline__ uint32_t tf32_rna_bits(uint32_t b) { return (b + 0x1000u) & 0xFFFFE000u; }
+
+// 8 consecutive FP32 accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr)
+                 : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <int AHEAD>
+__global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - raw);
+    const uint32_t ring_off = FUSED_MMA_STAGES * g.stage_bytes;
+    const float2** src_tab = reinterpret_cast<const float2**>(gbase + ring_off + (AHEAD + 1) * g.raw_slot_bytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(src_tab + FUSED_MAX_DENS);
+    // bars: full[2], empty[2], acc_full[3], acc_empty[3], drain
+    constexpr int FULL = 0, EMPTY = 2, ACCF = 4, ACCE = 4 + WS_NACC, DRAIN = 4 + 2 * WS_NACC;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + DRAIN + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const auto bar = [&](int i) { return smem_u32(bars + i); };
+    constexpr uint32_t A_PART = BM * 128;
+    const uint32_t b_part = (g.stage_bytes - 2u * A_PART) / 2u;
+    constexpr int CONV_THREADS = 32 * WS_CONV_WARPS, DRAIN_THREADS = 32 * WS_DRAIN_WARPS;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int la0 = m0 / 2, rb0 = n0 / 2;
+    const int nA = min(BM / 2, g.nl - la0), nB = min(BN / 2, g.nr - rb0);
+    const int nd = nA + nB;
+    const int nb = max(16, (2 * nB + 15) / 16 * 16);
+    const uint32_t idesc = fused_idesc(nb);
+    const int kt0 = blockIdx.z * g.kt_per;
+    const int nt = min(g.kt_total, kt0 + g.kt_per) - kt0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < FUSED_MMA_STAGES; ++s) {
+            mbar_init(bar(FULL + s), CONV_THREADS);
+            mbar_init(bar(EMPTY + s), 1);
+        }
+        for (int b = 0; b < WS_NACC; ++b) {
+            mbar_init(bar(ACCF + b), 1);
+            mbar_init(bar(ACCE + b), DRAIN_THREADS);
+        }
+        mbar_init(bar(DRAIN), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < nd; i += WS_THREADS) {
+        if (i < nA) {
+            src_tab[i] = g.V + (long long)(la0 + i) * g.v_stride;
+        } else {
+            const int r = rb0 + (i - nA);
+            src_tab[i] = g.rho + (long long)(g.ridx ? g.ridx[r] : r) * g.r_stride;
+        }
+    }
+    // zero both MMA stages once: rows beyond the real ones are never written again
+    for (uint32_t o = threadIdx.x * 16u; o < ring_off; o += WS_THREADS * 16u)
+        *reinterpret_cast<uint4*>(gbase + o) = make_uint4(0u, 0u, 0u, 0u);
+    fence_proxy_async();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+
+    if (warp < WS_CONV_WARPS) {
+        // ---- converters: item it = (density it / 16, atoms 2 (it % 16), +1)
+        const int items = nd * (BK / 2);
+        const auto issue = [&](int t) {
+            const long long at0 = (long long)(kt0 + t) * BK;
+            const uint32_t slot = base + ring_off + (uint32_t)(t % (AHEAD + 1)) * g.raw_slot_bytes;
+            for (int it = threadIdx.x; it < items; it += CONV_THREADS) {
+                const int i = it >> 4, c = it & 15;
+                const float2* src = src_tab[i];
+                const long long a = at0 + 2 * c;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const bool in = a + e < g.na;
+                    cp_async8(slot + (uint32_t)it * 16u + 8u * e, src + (in ? a + e : 0LL), in ? 8u : 0u);
+                }
+            }
+        };
+#pragma unroll 1
+        for (int t = 0; t < AHEAD; ++t) {
+            if (t < nt) issue(t);
+            cp_async_commit();
+        }
+#pragma unroll 1
+        for (int t = 0; t < nt; ++t) {
+            if (t + AHEAD < nt) issue(t + AHEAD);
+            cp_async_commit();
+            cp_async_wait<AHEAD>();  // this thread's copies of k-tile t have landed
+            const int s = t & 1;
+            const bool got = mbar_wait(bar(EMPTY + s), (uint32_t)(((t >> 1) & 1) ^ 1), abort_flag);
+            if (!__all_sync(0xffffffffu, got)) {
+                ok = false;
+                break;
+            }
+            unsigned char* stg = gbase + (size_t)s * g.stage_bytes;
+            const unsigned char* rs = gbase + ring_off + (size_t)(t % (AHEAD + 1)) * g.raw_slot_bytes;
+            for (int it = threadIdx.x; it < items; it += CONV_THREADS) {
+                const int i = it >> 4, c = it & 15;
+                const uint4 z = *reinterpret_cast<const uint4*>(rs + it * 16);  // re0, im0, re1, im1
+                const uint32_t h0 = tf32_rna_bits(z.x), h1 = tf32_rna_bits(z.y), h2 = tf32_rna_bits(z.z),
+                               h3 = tf32_rna_bits(z.w);
+                const uint32_t l0 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.x) - __uint_as_float(h0)));
+                const uint32_t l1 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.y) - __uint_as_float(h1)));
+                const uint32_t l2 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.z) - __uint_as_float(h2)));
+                const uint32_t l3 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.w) - __uint_as_float(h3)));
+                const bool left = i < nA;
+                unsigned char* hi_p = left ? stg : stg + 2 * A_PART;
+                unsigned char* lo_p = hi_p + (left ? A_PART : b_part);
+                const int row = 2 * (left ? i : i - nA);
+                // atoms 2c, 2c + 1: half (c & 1) of the 16-byte chunk c / 2 of each row
+                const uint32_t o0 = sw128_chunk(row, c >> 1) + 8u * (c & 1);
+                const uint32_t o1 = sw128_chunk(row + 1, c >> 1) + 8u * (c & 1);
+                *reinterpret_cast<uint2*>(hi_p + o0) = make_uint2(h0, h2);
+                *reinterpret_cast<uint2*>(hi_p + o1) = make_uint2(h1, h3);
+                *reinterpret_cast<uint2*>(lo_p + o0) = make_uint2(l0, l2);
+                *reinterpret_cast<uint2*>(lo_p + o1) = make_uint2(l1, l3);
+            }
+            fence_proxy_async();  // the stores, seen by the tensor cores' async proxy
+            mbar_arrive(bar(FULL + s));
+        }
+        cp_async_wait_all();
+    } else if (warp == WS_MMA_WARP) {
+        // ---- MMA issuer
+        bool issued_any = false;
+        if (lane == 0) {
+#pragma unroll 1
+            for (int t = 0; t < nt; ++t) {
+                const int s = t & 1, b = t % WS_NACC;
+                if (!mbar_wait(bar(ACCE + b), (uint32_t)(((t / WS_NACC) & 1) ^ 1), abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                if (!mbar_wait(bar(FULL + s), (uint32_t)((t >> 1) & 1), abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                const uint32_t st = base + (uint32_t)s * g.stage_bytes;
+                const uint32_t dm = tmem + (uint32_t)(b * BN);
+                const uint32_t dc = tmem + (uint32_t)(WS_NACC * BN);
+#pragma unroll
+                for (int kk = 0; kk < BK / 8; ++kk) {
+                    const uint64_t ahi = sw128_desc(st + kk * 32);
+                    const uint64_t alo = sw128_desc(st + A_PART + kk * 32);
+                    const uint64_t bhi = sw128_desc(st + 2 * A_PART + kk * 32);
+                    const uint64_t blo = sw128_desc(st + 2 * A_PART + b_part + kk * 32);
+                    mma_tf32_n(dm, ahi, bhi, idesc, kk > 0 ? 1u : 0u);
+                    mma_tf32_n(dc, alo, bhi, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+                    mma_tf32_n(dc, ahi, blo, idesc, 1u);
+                }
+                issued_any = true;
+                mma_commit(bar(EMPTY + s));
+                mma_commit(bar(ACCF + b));
+            }
+            // every MMA issued has completed before the teardown frees tensor memory
+            if (issued_any) {
+                mma_commit(bar(DRAIN));
+                mbar_drain(bar(DRAIN), 0);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- drain warps
+        const int q = warp & 3;
+        const int dc = nb / 2;                                // columns a drain warp takes
+        const int col0 = ((warp - WS_DRAIN_WARP0) >> 2) * dc;
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * q) << 16);
+        double acc[WS_MAX_DC];
+#pragma unroll
+        for (int i = 0; i < WS_MAX_DC; ++i) acc[i] = 0.0;
+        const auto add_cols = [&](uint32_t col) {
+#pragma unroll
+            for (int j = 0; j < WS_MAX_DC / 8; ++j) {
+                if (8 * j < dc) {
+                    float v[8];
+                    tmem_ld8(lane_base + col + (uint32_t)(col0 + 8 * j), v);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[8 * j + i] += (double)v[i];
+                }
+            }
+        };
+#pragma unroll 1
+        for (int t = 0; t < nt; ++t) {
+            const int b = t % WS_NACC;
+            const bool got = mbar_wait(bar(ACCF + b), (uint32_t)((t / WS_NACC) & 1), abort_flag);
+            if (!__all_sync(0xffffffffu, got)) {
+                ok = false;
+                break;
+            }
+            fence_after();
+            add_cols((uint32_t)(b * BN));
+            fence_before();
+            mbar_arrive(bar(ACCE + b));
+        }
+        if (ok) {
+            // the correction accumulator is complete with the last k-tile's commit
+            fence_after();
+            add_cols((uint32_t)(WS_NACC * BN));
+            const int R = m0 + 32 * q + lane;
+            const int l = R >> 1, pa = R & 1;
+            if (l < g.nl) {
+#pragma unroll
+                for (int j = 0; j < WS_MAX_DC; ++j) {
+                    const int Cg = n0 + col0 + j;
+                    const int r = Cg >> 1, pc = Cg & 1;
+                    if (j < dc && r < g.nr) {
+                        const int qi = (pa == pc) ? pa : 2 + pa;  // ac, bd, ad, bc
+                        atomicAdd(g.out4 + ((long long)l * g.nr + r) * 4 + qi, acc[j]);
+                    }
+                }
+            }
+        }
+    }
+
+    fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag)
+        *reinterpret_cast<volatile int*>(g.out4 + (long long)4 * g.nl * g.nr) = 1;
+    if (warp == 0) {
+        __syncwarp();
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 }  // namespace tc
 }  // namespace clk

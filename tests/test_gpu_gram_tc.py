@@ -140,6 +140,10 @@ def _fused_vs_split(d, specs, holes, monkeypatch):
     assert "gram_split" in prof_s
     # the same TF32 parts and the same MMAs: only the order of the FP64 additions differs
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    # up to 40 right densities the warp-specialised kernel runs (TF32 rounding on the integer
+    # pipe); CL_TC_NO_WS=1 takes the kernel whose warps take every role (cvt.rna.tf32)
+    one, _ = _run(d, specs, holes, env={"CL_TC_FUSED": "1", "CL_TC_NO_WS": "1"}, monkeypatch=monkeypatch, mode=SL32)
+    assert np.abs(got - one).max() <= 1e-12 * np.abs(one).max()
     return got
 
 
@@ -163,10 +167,11 @@ def test_fused_gram_ragged_and_tiny_atom_ranges(cells, monkeypatch):
     assert np.all(np.abs(got - want) <= lim), (np.abs(got - want) / lim).max()
 
 
-@pytest.mark.parametrize("n_states", [5, 9, 12])
+@pytest.mark.parametrize("n_states", [5, 8, 9, 12])
 def test_fused_gram_right_tile_widths_and_several_tiles(n_states, monkeypatch):
-    """15, 45 and 78 right densities: MMA widths 32, 96, and 128 + 32 over two right tiles (and
-    two left tiles at 12 states), each block converting its own tiles' densities."""
+    """15, 36, 45 and 78 right densities: MMA widths 32, 80 (the widest of the warp-specialised
+    kernel), 96, and 128 + 32 over two right tiles (and two left tiles at 12 states), each block
+    converting its own tiles' densities."""
     d = synth.build("c2", cells=(4, 5, 4))
     d["states"] = d["states"][:n_states, :, :8]
     specs = [tuple(int(v) for v in s) for s in cl.enumerate_integrals("****", n_states, n_states // 2)][::5]
