@@ -1326,6 +1326,11 @@ void gram_tc_fused(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, co
     g.kt_total = (int)((n_atoms + BK - 1) / BK);
     g.stage_bytes = (uint32_t)(2 * BM * 128 + 2 * nb * 128);
     g.raw_slot_bytes = (uint32_t)((nA + nB) * BK * 8);
+    // CL_TC_COPY8=1: 8-byte copies even where the rows allow 16 (zinc-blende boxes always do)
+    g.aligned16 = (reinterpret_cast<uintptr_t>(V) % 16 == 0 && reinterpret_cast<uintptr_t>(rho) % 16 == 0 &&
+                   v_stride % 2 == 0 && r_stride % 2 == 0 && !std::getenv("CL_TC_COPY8"))
+                      ? 1
+                      : 0;
     const int splits0 = gram_splits(tilesA * tilesB, g.kt_total);
     g.kt_per = (g.kt_total + splits0 - 1) / splits0;
     const int splits = (g.kt_total + g.kt_per - 1) / g.kt_per;

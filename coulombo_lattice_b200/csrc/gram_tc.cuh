@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(bar(ACCF + b), 1);
-            mbar_init(bar(ACCE + b), 32 * EPI_WARPS);
+            mbar_init(bar(ACCE + b), EPI_WARPS);  // one arrival a warp, after __syncwarp
         }
         mbar_init(bar(DRAIN), 1);
         *abort_flag = 0;
@@ -336,7 +336,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
             for (int i = 0; i < 32; ++i) acc[32 + i] += (double)v[i];
             fence_before();
-            mbar_arrive(bar(ACCE + b));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar(ACCE + b));
         }
         if (ok) {
             // the correction accumulator is complete with the last chunk's commit
@@ -412,6 +413,7 @@ struct FusedGram {
     uint32_t stage_bytes;     // 2 * BM * 128 + 2 * nb_max * 128
     uint32_t raw_slot_bytes;  // (left + right densities of a block, at most) * 32 * 8
     double* out4;
+    int aligned16;            // every density row starts on a 16-byte boundary (16-byte copies)
 };
 
 constexpr int FUSED_WARPS = 16;
@@ -443,6 +445,10 @@ __device__ __forceinline__ void mma_tf32_n(uint32_t d, uint64_t a, uint64_t b, u
 }
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, uint32_t src_bytes) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+// 16 bytes, of which the first src_bytes (0, 8 or 16) are read and the rest zero-filled.
+__device__ __forceinline__ void cp_async16z(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -483,12 +489,12 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedG
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < FUSED_MMA_STAGES; ++s) {
-            mbar_init(bar(FULL + s), FUSED_THREADS);
+            mbar_init(bar(FULL + s), FUSED_WARPS);  // one arrival a warp, after __syncwarp
             mbar_init(bar(EMPTY + s), 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(bar(ACCF + b), 1);
-            mbar_init(bar(ACCE + b), FUSED_THREADS);
+            mbar_init(bar(ACCE + b), FUSED_WARPS);
         }
         mbar_init(bar(DRAIN), 1);
         *abort_flag = 0;
@@ -623,7 +629,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedG
             *reinterpret_cast<float4*>(lo_p + o1) = make_float4(il[0], il[1], il[2], il[3]);
         }
         fence_proxy_async();  // the stores, seen by the tensor cores' async proxy
-        mbar_arrive(bar(FULL + s));
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar(FULL + s));
         if (warp == 0) {
             bool go = true;
             if (lane == 0) go = mma_tile(t);
@@ -638,7 +645,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedG
                 ok = false;
                 break;
             }
-            mbar_arrive(bar(ACCE + (tp & 1)));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar(ACCE + (tp & 1)));
         }
     }
     if (ok) {
@@ -704,6 +712,8 @@ constexpr int WS_THREADS = 32 * (WS_DRAIN_WARP0 + WS_DRAIN_WARPS);
 constexpr int WS_NACC = 3;         // main accumulator buffers (128 columns apart)
 constexpr int WS_MAX_NB = 80;      // MMA N: at most 40 right densities
 constexpr int WS_MAX_DC = WS_MAX_NB / 2;
+// items of 4 atoms a converter thread takes: 64 left + 40 right densities, 8 items each
+constexpr int WS_ITEMS = ((BM / 2 + WS_MAX_NB / 2) * (BK / 4) + 32 * WS_CONV_WARPS - 1) / (32 * WS_CONV_WARPS);
 
 __device__ __forceinline__ uint32_t tf32_rna_bits(uint32_t b) { return (b + 0x1000u) & 0xFFFFE000u; }
 
@@ -735,7 +745,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
     const auto bar = [&](int i) { return smem_u32(bars + i); };
     constexpr uint32_t A_PART = BM * 128;
     const uint32_t b_part = (g.stage_bytes - 2u * A_PART) / 2u;
-    constexpr int CONV_THREADS = 32 * WS_CONV_WARPS, DRAIN_THREADS = 32 * WS_DRAIN_WARPS;
+    constexpr int CONV_THREADS = 32 * WS_CONV_WARPS;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
@@ -748,13 +758,15 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
     const int nt = min(g.kt_total, kt0 + g.kt_per) - kt0;
 
     if (threadIdx.x == 0) {
+        // one arrival a warp (after __syncwarp): full by the converter warps, drained by the
+        // drain warps
         for (int s = 0; s < FUSED_MMA_STAGES; ++s) {
-            mbar_init(bar(FULL + s), CONV_THREADS);
+            mbar_init(bar(FULL + s), WS_CONV_WARPS);
             mbar_init(bar(EMPTY + s), 1);
         }
         for (int b = 0; b < WS_NACC; ++b) {
             mbar_init(bar(ACCF + b), 1);
-            mbar_init(bar(ACCE + b), DRAIN_THREADS);
+            mbar_init(bar(ACCE + b), WS_DRAIN_WARPS);
         }
         mbar_init(bar(DRAIN), 1);
         *abort_flag = 0;
@@ -785,19 +797,51 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
     bool ok = true;
 
     if (warp < WS_CONV_WARPS) {
-        // ---- converters: item it = (density it / 16, atoms 2 (it % 16), +1)
-        const int items = nd * (BK / 2);
+        // ---- converters: item it = (density it / 8, atoms 4 (it % 8) .. + 3); the raw slot holds
+        // atoms 4q, 4q + 1 of item it at 16 it and atoms 4q + 2, 4q + 3 at half + 16 it, so that
+        // consecutive threads copy and read contiguous 16-byte pieces.  A thread's items, their
+        // sources and their places in the stage are the same for every k-tile.
+        const int items = nd * (BK / 4);
+        const uint32_t half = (uint32_t)items * 16u;
+        const float2* isrc[WS_ITEMS];
+        uint32_t ihi[WS_ITEMS][2], ilo[WS_ITEMS][2];
+#pragma unroll
+        for (int k = 0; k < WS_ITEMS; ++k) {
+            const int it = threadIdx.x + k * CONV_THREADS;
+            const int i = min(it, items - 1) >> 3, qd = it & 7;
+            const bool left = i < nA;
+            const int row = 2 * (left ? i : i - nA);
+            const uint32_t hi0 = left ? 0u : 2u * A_PART, lo0 = hi0 + (left ? A_PART : b_part);
+            isrc[k] = src_tab[i] + 4 * qd;
+            ihi[k][0] = hi0 + sw128_chunk(row, qd);
+            ihi[k][1] = hi0 + sw128_chunk(row + 1, qd);
+            ilo[k][0] = lo0 + sw128_chunk(row, qd);
+            ilo[k][1] = lo0 + sw128_chunk(row + 1, qd);
+        }
         const auto issue = [&](int t) {
             const long long at0 = (long long)(kt0 + t) * BK;
             const uint32_t slot = base + ring_off + (uint32_t)(t % (AHEAD + 1)) * g.raw_slot_bytes;
-            for (int it = threadIdx.x; it < items; it += CONV_THREADS) {
-                const int i = it >> 4, c = it & 15;
-                const float2* src = src_tab[i];
-                const long long a = at0 + 2 * c;
 #pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const bool in = a + e < g.na;
-                    cp_async8(slot + (uint32_t)it * 16u + 8u * e, src + (in ? a + e : 0LL), in ? 8u : 0u);
+            for (int k = 0; k < WS_ITEMS; ++k) {
+                const int it = threadIdx.x + k * CONV_THREADS;
+                if (it < items) {
+                    const long long a = at0 + 4 * (it & 7);  // first atom of the item
+                    const uint32_t d0 = slot + (uint32_t)it * 16u;
+                    if (g.aligned16) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const long long left_atoms = g.na - (a + 2 * h);
+                            const uint32_t nbytes = left_atoms >= 2 ? 16u : (left_atoms == 1 ? 8u : 0u);
+                            cp_async16z(d0 + h * half, isrc[k] + (nbytes ? at0 + 2 * h : -4LL * (it & 7)), nbytes);
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const bool in = a + e < g.na;
+                            cp_async8(d0 + (e >> 1) * half + 8u * (e & 1), isrc[k] + (in ? at0 + e : -4LL * (it & 7)),
+                                      in ? 8u : 0u);
+                        }
+                    }
                 }
             }
         };
@@ -819,29 +863,30 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
             }
             unsigned char* stg = gbase + (size_t)s * g.stage_bytes;
             const unsigned char* rs = gbase + ring_off + (size_t)(t % (AHEAD + 1)) * g.raw_slot_bytes;
-            for (int it = threadIdx.x; it < items; it += CONV_THREADS) {
-                const int i = it >> 4, c = it & 15;
-                const uint4 z = *reinterpret_cast<const uint4*>(rs + it * 16);  // re0, im0, re1, im1
-                const uint32_t h0 = tf32_rna_bits(z.x), h1 = tf32_rna_bits(z.y), h2 = tf32_rna_bits(z.z),
-                               h3 = tf32_rna_bits(z.w);
-                const uint32_t l0 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.x) - __uint_as_float(h0)));
-                const uint32_t l1 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.y) - __uint_as_float(h1)));
-                const uint32_t l2 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.z) - __uint_as_float(h2)));
-                const uint32_t l3 = tf32_rna_bits(__float_as_uint(__uint_as_float(z.w) - __uint_as_float(h3)));
-                const bool left = i < nA;
-                unsigned char* hi_p = left ? stg : stg + 2 * A_PART;
-                unsigned char* lo_p = hi_p + (left ? A_PART : b_part);
-                const int row = 2 * (left ? i : i - nA);
-                // atoms 2c, 2c + 1: half (c & 1) of the 16-byte chunk c / 2 of each row
-                const uint32_t o0 = sw128_chunk(row, c >> 1) + 8u * (c & 1);
-                const uint32_t o1 = sw128_chunk(row + 1, c >> 1) + 8u * (c & 1);
-                *reinterpret_cast<uint2*>(hi_p + o0) = make_uint2(h0, h2);
-                *reinterpret_cast<uint2*>(hi_p + o1) = make_uint2(h1, h3);
-                *reinterpret_cast<uint2*>(lo_p + o0) = make_uint2(l0, l2);
-                *reinterpret_cast<uint2*>(lo_p + o1) = make_uint2(l1, l3);
+#pragma unroll
+            for (int k = 0; k < WS_ITEMS; ++k) {
+                const int it = threadIdx.x + k * CONV_THREADS;
+                if (it < items) {
+                    const uint4 z0 = *reinterpret_cast<const uint4*>(rs + it * 16);         // re0 im0 re1 im1
+                    const uint4 z1 = *reinterpret_cast<const uint4*>(rs + half + it * 16);  // re2 im2 re3 im3
+                    const uint32_t re[4] = {z0.x, z0.z, z1.x, z1.z}, im[4] = {z0.y, z0.w, z1.y, z1.w};
+                    uint32_t rh[4], ih[4], rl[4], il[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        rh[e] = tf32_rna_bits(re[e]);
+                        ih[e] = tf32_rna_bits(im[e]);
+                        rl[e] = tf32_rna_bits(__float_as_uint(__uint_as_float(re[e]) - __uint_as_float(rh[e])));
+                        il[e] = tf32_rna_bits(__float_as_uint(__uint_as_float(im[e]) - __uint_as_float(ih[e])));
+                    }
+                    *reinterpret_cast<uint4*>(stg + ihi[k][0]) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                    *reinterpret_cast<uint4*>(stg + ihi[k][1]) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                    *reinterpret_cast<uint4*>(stg + ilo[k][0]) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                    *reinterpret_cast<uint4*>(stg + ilo[k][1]) = make_uint4(il[0], il[1], il[2], il[3]);
+                }
             }
             fence_proxy_async();  // the stores, seen by the tensor cores' async proxy
-            mbar_arrive(bar(FULL + s));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar(FULL + s));
         }
         cp_async_wait_all();
     } else if (warp == WS_MMA_WARP) {
@@ -915,7 +960,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
             fence_after();
             add_cols((uint32_t)(b * BN));
             fence_before();
-            mbar_arrive(bar(ACCE + b));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar(ACCE + b));
         }
         if (ok) {
             // the correction accumulator is complete with the last k-tile's commit

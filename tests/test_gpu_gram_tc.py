@@ -144,6 +144,9 @@ def _fused_vs_split(d, specs, holes, monkeypatch):
     # pipe); CL_TC_NO_WS=1 takes the kernel whose warps take every role (cvt.rna.tf32)
     one, _ = _run(d, specs, holes, env={"CL_TC_FUSED": "1", "CL_TC_NO_WS": "1"}, monkeypatch=monkeypatch, mode=SL32)
     assert np.abs(got - one).max() <= 1e-12 * np.abs(one).max()
+    # CL_TC_COPY8=1: the 8-byte copies of rows that do not start on a 16-byte boundary
+    c8, _ = _run(d, specs, holes, env={"CL_TC_FUSED": "1", "CL_TC_COPY8": "1"}, monkeypatch=monkeypatch, mode=SL32)
+    assert np.abs(got - c8).max() <= 1e-12 * np.abs(one).max()
     return got
 
 
