@@ -1344,12 +1344,16 @@ void gram_tc_fused(cl_ctx* c, const cx<float>* V, long long v_stride, int nl, co
     // up to 40 right densities a block (N <= 80): the warp-specialised kernel; CL_TC_NO_WS=1
     // keeps the kernel whose warps take every role in turn
     const bool ws = nb <= WS_MAX_NB && !std::getenv("CL_TC_NO_WS");
-    if (ws && smem5 <= 227 * 1024)
-        k_gram_tc_ws<5><<<grid, WS_THREADS, smem5, c->stream>>>(g);
-    else if (ws && smem3 <= 227 * 1024)
-        k_gram_tc_ws<3><<<grid, WS_THREADS, smem3, c->stream>>>(g);
+    const size_t ws5 = ws_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 5);
+    const size_t ws3 = ws_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 3);
+    const size_t ws2 = ws_smem_bytes(g.stage_bytes, g.raw_slot_bytes, 2);
+    if (ws && ws2 > 227 * 1024) cl::fail(CL_ERR_UNSUPPORTED, "fused Gram needs %zu bytes of shared memory", ws2);
+    if (ws && ws5 <= 227 * 1024)
+        k_gram_tc_ws<5><<<grid, WS_THREADS, ws5, c->stream>>>(g);
+    else if (ws && ws3 <= 227 * 1024)
+        k_gram_tc_ws<3><<<grid, WS_THREADS, ws3, c->stream>>>(g);
     else if (ws)
-        k_gram_tc_ws<2><<<grid, WS_THREADS, smem2, c->stream>>>(g);
+        k_gram_tc_ws<2><<<grid, WS_THREADS, ws2, c->stream>>>(g);
     else if (smem5 <= 227 * 1024)
         k_gram_tc_fused<5><<<grid, FUSED_THREADS, smem5, c->stream>>>(g);
     else if (smem3 <= 227 * 1024)

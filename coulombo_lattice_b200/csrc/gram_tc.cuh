@@ -710,10 +710,16 @@ constexpr int WS_DRAIN_WARP0 = 8;
 constexpr int WS_DRAIN_WARPS = 8;
 constexpr int WS_THREADS = 32 * (WS_DRAIN_WARP0 + WS_DRAIN_WARPS);
 constexpr int WS_NACC = 3;         // main accumulator buffers (128 columns apart)
+constexpr int WS_STAGES = 2;       // MMA operand stages in shared memory
 constexpr int WS_MAX_NB = 80;      // MMA N: at most 40 right densities
 constexpr int WS_MAX_DC = WS_MAX_NB / 2;
 // items of 4 atoms a converter thread takes: 64 left + 40 right densities, 8 items each
 constexpr int WS_ITEMS = ((BM / 2 + WS_MAX_NB / 2) * (BK / 4) + 32 * WS_CONV_WARPS - 1) / (32 * WS_CONV_WARPS);
+
+__host__ __device__ constexpr size_t ws_smem_bytes(uint32_t stage_bytes, uint32_t raw_slot_bytes, int ahead) {
+    return 1024 + (size_t)WS_STAGES * stage_bytes + (size_t)(ahead + 1) * raw_slot_bytes +
+           sizeof(void*) * FUSED_MAX_DENS + 256;
+}
 
 __device__ __forceinline__ uint32_t tf32_rna_bits(uint32_t b) { return (b + 0x1000u) & 0xFFFFE000u; }
 
@@ -729,17 +735,35 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Issues the load of 8 consecutive FP32 accumulator columns of this thread's lane (no wait).
+__device__ __forceinline__ void tmem_ld8_issue(uint32_t taddr, uint32_t* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr)
+                 : "memory");
+}
+// Waits for this thread's tensor-memory loads; the 16 destination registers pass through the
+// wait, so that no use of them is scheduled before it.
+__device__ __forceinline__ void tmem_wait_ld16(uint32_t* r) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :
+                 : "memory");
+}
+
 template <int AHEAD>
 __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     unsigned char* gbase = smem_raw + (base - raw);
-    const uint32_t ring_off = FUSED_MMA_STAGES * g.stage_bytes;
+    const uint32_t ring_off = WS_STAGES * g.stage_bytes;
     const float2** src_tab = reinterpret_cast<const float2**>(gbase + ring_off + (AHEAD + 1) * g.raw_slot_bytes);
     uint64_t* bars = reinterpret_cast<uint64_t*>(src_tab + FUSED_MAX_DENS);
-    // bars: full[2], empty[2], acc_full[3], acc_empty[3], drain
-    constexpr int FULL = 0, EMPTY = 2, ACCF = 4, ACCE = 4 + WS_NACC, DRAIN = 4 + 2 * WS_NACC;
+    // bars: full[WS_STAGES], empty[WS_STAGES], acc_full[WS_NACC], acc_empty[WS_NACC], drain
+    constexpr int FULL = 0, EMPTY = WS_STAGES, ACCF = 2 * WS_STAGES, ACCE = ACCF + WS_NACC, DRAIN = ACCE + WS_NACC;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + DRAIN + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     const auto bar = [&](int i) { return smem_u32(bars + i); };
@@ -760,7 +784,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
     if (threadIdx.x == 0) {
         // one arrival a warp (after __syncwarp): full by the converter warps, drained by the
         // drain warps
-        for (int s = 0; s < FUSED_MMA_STAGES; ++s) {
+        for (int s = 0; s < WS_STAGES; ++s) {
             mbar_init(bar(FULL + s), WS_CONV_WARPS);
             mbar_init(bar(EMPTY + s), 1);
         }
@@ -855,8 +879,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
             if (t + AHEAD < nt) issue(t + AHEAD);
             cp_async_commit();
             cp_async_wait<AHEAD>();  // this thread's copies of k-tile t have landed
-            const int s = t & 1;
-            const bool got = mbar_wait(bar(EMPTY + s), (uint32_t)(((t >> 1) & 1) ^ 1), abort_flag);
+            const int s = t % WS_STAGES;
+            const bool got = mbar_wait(bar(EMPTY + s), (uint32_t)(((t / WS_STAGES) & 1) ^ 1), abort_flag);
             if (!__all_sync(0xffffffffu, got)) {
                 ok = false;
                 break;
@@ -895,12 +919,12 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
         if (lane == 0) {
 #pragma unroll 1
             for (int t = 0; t < nt; ++t) {
-                const int s = t & 1, b = t % WS_NACC;
+                const int s = t % WS_STAGES, b = t % WS_NACC;
                 if (!mbar_wait(bar(ACCE + b), (uint32_t)(((t / WS_NACC) & 1) ^ 1), abort_flag)) {
                     ok = false;
                     break;
                 }
-                if (!mbar_wait(bar(FULL + s), (uint32_t)((t >> 1) & 1), abort_flag)) {
+                if (!mbar_wait(bar(FULL + s), (uint32_t)((t / WS_STAGES) & 1), abort_flag)) {
                     ok = false;
                     break;
                 }
@@ -949,19 +973,44 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_gram_tc_ws(const FusedGram g)
                 }
             }
         };
+        // two k-tiles' main products (buffers at columns c0 and c1): their FP32 sum, rounded to
+        // nearest once (unbiased, 2^-24 of the pair against the TF32x3 parts' 2^-22 of each
+        // product), goes into the FP64 sums -- half the conversions and waits of one by one
+        const auto add_pair = [&](uint32_t c0, uint32_t c1) {
+#pragma unroll
+            for (int j = 0; j < WS_MAX_DC / 8; ++j) {
+                if (8 * j < dc) {
+                    uint32_t r[16];
+                    tmem_ld8_issue(lane_base + c0 + (uint32_t)(col0 + 8 * j), r);
+                    tmem_ld8_issue(lane_base + c1 + (uint32_t)(col0 + 8 * j), r + 8);
+                    tmem_wait_ld16(r);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        acc[8 * j + i] += (double)(__uint_as_float(r[i]) + __uint_as_float(r[8 + i]));
+                }
+            }
+        };
 #pragma unroll 1
-        for (int t = 0; t < nt; ++t) {
-            const int b = t % WS_NACC;
-            const bool got = mbar_wait(bar(ACCF + b), (uint32_t)((t / WS_NACC) & 1), abort_flag);
+        for (int t = 0; t < nt; t += 2) {
+            const bool pair = t + 1 < nt;
+            const int b0 = t % WS_NACC, b1 = (t + 1) % WS_NACC;
+            bool got = mbar_wait(bar(ACCF + b0), (uint32_t)((t / WS_NACC) & 1), abort_flag);
+            if (got && pair) got = mbar_wait(bar(ACCF + b1), (uint32_t)(((t + 1) / WS_NACC) & 1), abort_flag);
             if (!__all_sync(0xffffffffu, got)) {
                 ok = false;
                 break;
             }
             fence_after();
-            add_cols((uint32_t)(b * BN));
+            if (pair)
+                add_pair((uint32_t)(b0 * BN), (uint32_t)(b1 * BN));
+            else
+                add_cols((uint32_t)(b0 * BN));
             fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(bar(ACCE + b));
+            if (lane == 0) {
+                mbar_arrive(bar(ACCE + b0));
+                if (pair) mbar_arrive(bar(ACCE + b1));
+            }
         }
         if (ok) {
             // the correction accumulator is complete with the last k-tile's commit

@@ -138,12 +138,19 @@ def _fused_vs_split(d, specs, holes, monkeypatch):
     assert "gram_split" not in prof and prof["gram"][1] >= 1
     ref, prof_s = _run(d, specs, holes, env={"CL_TC_SPLIT": "1"}, monkeypatch=monkeypatch, profile=True, mode=SL32)
     assert "gram_split" in prof_s
-    # the same TF32 parts and the same MMAs: only the order of the FP64 additions differs
-    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
-    # up to 40 right densities the warp-specialised kernel runs (TF32 rounding on the integer
-    # pipe); CL_TC_NO_WS=1 takes the kernel whose warps take every role (cvt.rna.tf32)
+    # CL_TC_NO_WS=1: the fused kernel whose warps take every role -- the same TF32 parts
+    # (cvt.rna.tf32) and the same MMAs as the split pass, each k-tile drained into FP64: only the
+    # order of the FP64 additions differs
     one, _ = _run(d, specs, holes, env={"CL_TC_FUSED": "1", "CL_TC_NO_WS": "1"}, monkeypatch=monkeypatch, mode=SL32)
-    assert np.abs(got - one).max() <= 1e-12 * np.abs(one).max()
+    assert np.abs(one - ref).max() <= 1e-12 * np.abs(ref).max()
+    # up to 40 right densities the warp-specialised kernel runs: TF32 rounding on the integer
+    # pipe, k-tiles drained in pairs summed once in FP32 (round to nearest: at most 2^-24 of the
+    # pair's magnitude, a quarter of the TF32x3 parts' 2^-22 of each product), and bit-for-bit
+    # the same parts (equal sums) where a block holds a single k-tile
+    lim = np.maximum(1e-6 * np.abs(ref), 1e-9)
+    assert np.all(np.abs(got - ref) <= 0.25 * lim), (np.abs(got - ref) / lim).max()
+    if d["pos"].shape[0] <= 32:
+        assert np.abs(got - one).max() <= 1e-12 * np.abs(one).max()
     # CL_TC_COPY8=1: the 8-byte copies of rows that do not start on a 16-byte boundary
     c8, _ = _run(d, specs, holes, env={"CL_TC_FUSED": "1", "CL_TC_COPY8": "1"}, monkeypatch=monkeypatch, mode=SL32)
     assert np.abs(got - c8).max() <= 1e-12 * np.abs(one).max()
