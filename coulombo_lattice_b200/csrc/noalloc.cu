@@ -11,17 +11,14 @@
 // The scratch: g_fft_scratch below, three tables (x, y, z) of at most kMaxAxis complex
 // doubles each, 192 KiB in total.  It is a file-scope __device__ array, so every GPU that
 // loads the library holds it until the process exits.  In host code its name is only a
-// host-side stand-in; the device address is obtained once per device with
-// cudaGetSymbolAddress, on the first call made with that device current.  The address is
-// kept for the life of the process: after a
-// cudaDeviceReset the module is loaded again and the array may move, so a process that resets
-// a device must not call this entry point on it afterwards.  Every call rewrites all table
+// host-side stand-in; every call looks the device address up with cudaGetSymbolAddress on the
+// current device (no allocation, no stream work), so a device reset that reloads the module
+// and moves the array leaves no stale address behind.  Every call rewrites all table
 // entries it reads, so nothing has to start at zero; but all calls share the one array, so
 // calls that overlap on the GPU (e.g. from threads using per-thread default streams) race on
 // it.
 #include <algorithm>
 #include <cstdint>
-#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -32,12 +29,9 @@
 namespace {
 
 constexpr int kMaxAxis = 4096;
-constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) clk::cx<double> g_fft_scratch[3 * kMaxAxis];
 
-std::mutex g_setup_mutex;
-clk::cx<double>* g_scratch_addr[kMaxDevices] = {};
 
 #define NA_CUDA(call)                                                                          \
     do {                                                                                       \
@@ -47,18 +41,11 @@ clk::cx<double>* g_scratch_addr[kMaxDevices] = {};
                      __LINE__, cudaGetErrorString(err_));                                      \
     } while (0)
 
-// Device address of the scratch array on the current device (set up on first use).
+// Device address of the scratch array on the current device.
 clk::cx<double>* scratch_on_current_device() {
-    int dev = 0;
-    NA_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) cl::fail(CL_ERR_UNSUPPORTED, "device ordinal %d is out of range", dev);
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        NA_CUDA(cudaGetSymbolAddress(&p, g_fft_scratch));
-        g_scratch_addr[dev] = static_cast<clk::cx<double>*>(p);
-    }
-    return g_scratch_addr[dev];
+    void* p = nullptr;
+    NA_CUDA(cudaGetSymbolAddress(&p, g_fft_scratch));
+    return static_cast<clk::cx<double>*>(p);
 }
 
 // tw[t] = exp(-2 pi i t / n)

@@ -238,10 +238,9 @@ int cl_fft3d(int nx, int ny, int nz, int batch, int sign, int fp32, double* data
  * 16-byte aligned, transformed in place on the legacy default stream; the call returns
  * after the transform has finished.  It allocates nothing: the twiddle tables live in a
  * fixed 192 KiB array inside the library (held by every GPU that loads it until exit), so
- * each axis is limited to 4096 points and longer axes are rejected.  The first call on a
- * device looks up that array's device address, which is kept until the process exits, so do
- * not call this again on a device after cudaDeviceReset.  All calls share the array: calls
- * that overlap on the GPU race. */
+ * each axis is limited to 4096 points and longer axes are rejected.  Every call looks up
+ * that array's device address on the current device, so a device reset leaves no stale
+ * address.  All calls share the array: calls that overlap on the GPU race. */
 int cl_fft3d_noalloc(int nx, int ny, int nz, int batch, int sign, double* data);
 
 /* ---------------------------------------------------------------------------------------
