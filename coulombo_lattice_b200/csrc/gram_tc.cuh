@@ -691,16 +691,19 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_gram_tc_fused(const FusedG
 // The fused Gram with its roles in separate warps (at most 40 right densities a block: N <= 80),
 // so that the conversion of k-tile t + 1, the MMAs of k-tile t and the drain of k-tile t - 1
 // run at the same time instead of one after another in every warp:
-//   warps 0-6    copy their items' raw values AHEAD k-tiles ahead with 8-byte cp.async (each
-//                thread reads back only its own copies) and convert them: item (density i,
-//                atom pair c) -> TF32 hi and lo of re and im, 8-byte stores into the
-//                128-byte-swizzled K-major stage; then arrive on the stage's full barrier;
+//   warps 0-6    copy their items' raw values AHEAD k-tiles ahead with cp.async (16 bytes on
+//                rows that start on a 16-byte boundary, else 8; each thread reads back only its
+//                own copies) and convert them: item (density i, atoms 4q .. 4q + 3) -> TF32 hi
+//                and lo of re and im, four 16-byte stores into the 128-byte-swizzled K-major
+//                stage; then one arrival a warp on the stage's full barrier;
 //   warp 7       lane 0 issues the tile's 12 MMAs once the stage is full and its accumulator
 //                buffer drained (three main buffers in tensor memory, the correction in a
 //                fourth), and commits them to the stage's empty and the buffer's full barrier;
 //   warps 8-15   drain: warp w reads lane quarter w % 4, columns [h DC, h DC + DC) for h =
-//                (w - 8) / 4, DC = N / 2, adding them to FP64 registers; the correction
-//                accumulator once after the last k-tile.
+//                (w - 8) / 4, DC = N / 2, two k-tiles at a time: the two FP32 values of a
+//                column summed once (round to nearest, unbiased, at most 2^-24 of the pair
+//                against the TF32 parts' 2^-22 of each product) and added to FP64 registers;
+//                the correction accumulator once after the last k-tile.
 // TF32 rounding to nearest (ties away from zero, as cvt.rna.tf32.f32 for finite values) is done
 // on the integer pipe: add half the weight of the 13 dropped mantissa bits, clear them.
 // ---------------------------------------------------------------------------------------
